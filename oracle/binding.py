@@ -82,6 +82,8 @@ def lib():
         L.oracle_solve.restype = C.c_int
         L.oracle_precondition.argtypes = [_P(OracleProblem), C.c_int, _f64p, _f64p, _f64p]
         L.oracle_precondition.restype = C.c_int
+        L.oracle_evaluate.argtypes = [_P(OracleProblem), _f64p, _f64p, _f64p]
+        L.oracle_evaluate.restype = C.c_int
         _lib = L
     return _lib
 
@@ -178,3 +180,22 @@ def precondition(prob, rescaling=3):
     if rc != 0:
         raise ValueError(f"oracle_precondition rc={rc}")
     return Dr, Dl, val
+
+
+EVAL_KEYS = ("primal_res", "dual_res", "rel_gap", "primal_res_gpu_form", "pobj", "dobj",
+             "primal_abs_inf", "dual_abs_inf")
+
+
+def evaluate(prob, x, y):
+    """Score a final point with the shared FP64 evaluator (README-form criteria)."""
+    keep = _Keep()
+    P = _problem_struct(prob, keep)
+    out = np.zeros(8)
+    xv = np.ascontiguousarray(x, dtype=np.float64)
+    yv = np.ascontiguousarray(y, dtype=np.float64)
+    rc = lib().oracle_evaluate(C.byref(P), _f(xv), _f(yv), _f(out))
+    if rc != 0:
+        raise ValueError(f"oracle_evaluate rc={rc}")
+    d = dict(zip(EVAL_KEYS, out.tolist()))
+    d["max_rel"] = max(d["primal_res"], d["dual_res"], d["rel_gap"])
+    return d

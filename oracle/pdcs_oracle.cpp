@@ -1355,6 +1355,46 @@ int oracle_precondition(const oracle_problem* p, int rescaling, double* Dr, doub
   return 0;
 }
 
+// Shared FP64 evaluator of a final point (x, y) in the original scale.
+// out[0] primal residual, README form: ||r - P(r)||_inf / (1 + max(||h||, ||Gx||, ||P(r)||)), r = Gx - h
+// out[1] dual residual: ||lam - P(lam)||_inf / (1 + max(||c||, ||G'y||)), lam = c - G'y
+// out[2] relative gap |c'x - dobj| / (1 + max(|c'x|, |dobj|)), dobj = h'y + l'lam+ + u'lam-
+// out[3] primal residual with the GPU code's denominator (||P(lam)|| instead of ||P(r)||)
+// out[4] c'x, out[5] dobj, out[6] ||r - P(r)||_inf, out[7] ||lam - P(lam)||_inf
+// (README.md:70-90; rpdhg_alg_gpu_gen_scaling.jl:126-183)
+int oracle_evaluate(const oracle_problem* p, const double* x, const double* y, double* out) {
+  Problem P;
+  int rc = build_problem(p, 0, P);
+  if (rc) return rc;
+  int64_t n = p->n, m = p->m;
+  Vec xv(x, x + n), yv(y, y + m), gx(m), aty(n), r(m), pr(m), lam(n), pl(n);
+  spmv(P.Graw, xv.data(), gx.data());
+  spmv(P.Gtraw, yv.data(), aty.data());
+  for (int64_t i = 0; i < m; ++i) r[i] = gx[i] - P.hraw[i];
+  pr = r;
+  project_all(P.conb, pr.data(), nullptr, nullptr, nullptr);
+  for (int64_t j = 0; j < n; ++j) lam[j] = P.craw[j] - aty[j];
+  pl = lam;
+  project_all(P.slackb, pl.data(), nullptr, P.lam_l.data(), P.lam_u.data());
+  double rinf = 0, linf = 0;
+  for (int64_t i = 0; i < m; ++i) rinf = std::max(rinf, std::fabs(pr[i] - r[i]));
+  for (int64_t j = 0; j < n; ++j) linf = std::max(linf, std::fabs(pl[j] - lam[j]));
+  double pobj = dot(xv, P.craw), dobj = dot(yv, P.hraw);
+  for (int64_t j = 0; j < P.nb; ++j)
+    dobj += P.bl_fin[j] * std::max(0.0, lam[j]) + P.bu_fin[j] * std::min(0.0, lam[j]);
+  double hinf = nrminf(P.hraw), gxinf = nrminf(gx), prinf = nrminf(pr), cinf = nrminf(P.craw);
+  double atyinf = nrminf(aty), plinf = nrminf(pl);
+  out[0] = rinf / (1.0 + std::max(hinf, std::max(gxinf, prinf)));
+  out[1] = linf / (1.0 + std::max(cinf, atyinf));
+  out[2] = std::fabs(pobj - dobj) / (1.0 + std::max(std::fabs(pobj), std::fabs(dobj)));
+  out[3] = rinf / (1.0 + std::max(plinf, std::max(hinf, gxinf)));
+  out[4] = pobj;
+  out[5] = dobj;
+  out[6] = rinf;
+  out[7] = linf;
+  return 0;
+}
+
 int oracle_solve(const oracle_problem* p, const oracle_options* opt, oracle_result* res) {
 #ifdef _OPENMP
   if (opt->threads > 0) omp_set_num_threads(opt->threads);

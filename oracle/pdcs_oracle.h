@@ -99,6 +99,8 @@ int oracle_project_block(int kind, double* v, int64_t len, const double* S,
 /* Euclidean projection onto the exponential cone scaled by D (D o K_exp). */
 void oracle_proj_exp_scaled(double* v, const double* D);
 int oracle_solve(const oracle_problem* p, const oracle_options* o, oracle_result* r);
+/* Shared KKT evaluator of a final point in the original scale (8 outputs, see the .cpp). */
+int oracle_evaluate(const oracle_problem* p, const double* x, const double* y, double* out);
 /* Apply the Ruiz(10)+Pock-Chambolle(1) preconditioner and return the scaling
  * vectors (Dr: n, Dl: m) and the scaled CSR values (nnz). */
 int oracle_precondition(const oracle_problem* p, int rescaling, double* Dr, double* Dl,

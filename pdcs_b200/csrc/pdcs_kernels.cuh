@@ -1,0 +1,469 @@
+// pdcs_kernels.cuh -- kernels of the PDHG hot path (FP64).
+//
+// One PDHG attempt (rpdhg_alg_gpu_gen_scaling.jl:680-765) runs as
+//   spmv(G^T, y_lag)          -> aty                 [1 matrix pass]
+//   update_project<Primal>    x = P_X(x_lag + tau*dec*(aty - c)), sum |dx|^2
+//   spmv2(G, x, x_lag)        -> gx, gxl             [1 matrix pass, 2 gathers]
+//   update_project<Dual>      y = P_Y(y_lag - sigma*dec*(2gx - gxl - h)),
+//                             sum |dy|^2, sum dy*(gx - gxl)   (= dx' G' dy)
+//   control                   eta_bar test, accept / retry, next step sizes
+//   reflect                   aggressive extrapolation + eta-weighted averages
+// The reference's third SpMV (G' dy, :712) is replaced by the identity
+// dx' G' dy = dy' (G x - G x_lag), which the second pass provides for free.
+#pragma once
+#include "pdcs_device.cuh"
+
+namespace pdcs {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+enum AccKind : int32_t { ACC_SUM = 0, ACC_MAX = 1 };
+
+// ---------------------------------------------------------------------------
+// Device-resident solver state (one per solve).
+// ---------------------------------------------------------------------------
+enum HaltReason : int32_t {
+  HALT_NONE = 0,
+  HALT_CHECK = 1,          // attempt with iter % check_freq == 0: host runs the exit check
+  HALT_RESTART_CHECK = 2,  // accepted step with iter % restart_freq == 0
+  HALT_ARTIFICIAL = 3,     // inner >= beta_artificial * iter (or forced restart)
+  HALT_LIMIT = 4,          // attempt limit reached
+};
+
+struct PdhgState {
+  double eta, eta_p, eta_bar, omega, dec, dec_next, extra, eta_cum;
+  double tau, sigma;   // params.tau / params.sigma of the last attempt
+  double ps, ds;       // primal / dual step of the current attempt (tau*dec, sigma*dec)
+  double refl_tmp, refl_inv, refl_eta, refl_cum, refl_extra;
+  double sum_dx2, sum_dy2, sum_dgdy;
+  long long iter, iter_stepsize, inner, reject_count;
+  long long check_freq, restart_freq, attempt_limit;
+  int32_t active, do_reflect, halt_reason, accepted;
+  int32_t force_restart, restart_enabled, pad0, pad1;
+};
+
+// Shared by the control kernel and the host (after a checkpoint):
+// the bookkeeping after an accepted step (:752-753 return, then the main
+// loop :854-866 and the next call's entry :667, :676).
+__host__ __device__ inline void post_accept(PdhgState& st, bool force) {
+  double eta_acc = st.eta > 1e-30 ? st.eta : 1e-30;
+  st.inner += 1;
+  double di = (double)st.inner;
+  st.refl_tmp = (di + 1.0) / (di + 2.0);
+  st.refl_inv = 1.0 / (di + 2.0);
+  st.refl_eta = eta_acc;
+  st.refl_cum = st.eta_cum;
+  st.refl_extra = st.extra;
+  st.eta_cum += eta_acc;
+  st.do_reflect = 1;
+  // next step call
+  st.dec = st.dec_next;
+  st.eta = st.eta_p > 1e-6 ? st.eta_p : 1e-6;
+  st.reject_count = 0;
+  st.ps = (st.eta / st.omega) * st.dec;
+  st.ds = (st.eta * st.omega) * st.dec;
+  bool artificial = ((double)st.inner >= (double)st.iter * 0.223 && st.iter > 10000) || (force && st.inner > 100);
+  bool restart_due = st.restart_enabled && st.restart_freq > 0 && (st.iter % st.restart_freq == 0);
+  if (artificial) {
+    st.halt_reason = HALT_ARTIFICIAL;
+    st.active = 0;
+  } else if (restart_due) {
+    st.halt_reason = HALT_RESTART_CHECK;
+    st.active = 0;
+  }
+}
+
+__host__ __device__ inline void after_reject(PdhgState& st) {
+  st.eta = st.eta_p;
+  st.reject_count += 1;
+  st.ps = (st.eta / st.omega) * st.dec;
+  st.ds = (st.eta * st.omega) * st.dec;
+}
+
+// ---------------------------------------------------------------------------
+// CSR SpMV with rows binned by length.  Bin b < 6 holds rows handled by a
+// group of g = 2^b lanes (rows of up to ~4g nonzeros); bin 6 holds long rows,
+// one CTA each.  One launch covers all bins: CTA ranges [cta0[b], cta0[b+1]).
+// ---------------------------------------------------------------------------
+constexpr int kBins = 7;
+
+struct CsrDev {
+  int64_t m, n, nnz;
+  const int32_t* rp;
+  const int32_t* ci;
+  const double* v;
+  const int32_t* perm;       // rows ordered by bin
+  int64_t bin_off[kBins + 1];
+  int32_t cta0[kBins + 1];   // first CTA of each bin, cta0[kBins] = grid size
+};
+
+template <int NV>
+__global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const double* __restrict__ x0,
+                                                              const double* __restrict__ x1,
+                                                              double* __restrict__ y0, double* __restrict__ y1,
+                                                              const int32_t* __restrict__ active) {
+  if (active && !*active) return;
+  const int cta = blockIdx.x;
+  int bin = 0;
+#pragma unroll
+  for (int b = 1; b < kBins; ++b)
+    if (cta >= A.cta0[b]) bin = b;
+  const int64_t r0 = A.bin_off[bin], r1 = A.bin_off[bin + 1];
+  const int ncta = A.cta0[bin + 1] - A.cta0[bin];
+  const int lcta = cta - A.cta0[bin];
+  if (bin < kBins - 1) {
+    const int g = 1 << bin;
+    const int lane_g = threadIdx.x & (g - 1);
+    const int64_t rows_per_cta = kThreads / g;
+    // the loop bound is uniform across the warp (all lanes reach the shuffles)
+    const int64_t warp_first = r0 + (int64_t)lcta * rows_per_cta + (threadIdx.x >> 5) * (32 / g);
+    for (int64_t qb = warp_first; qb < r1; qb += (int64_t)ncta * rows_per_cta) {
+      const int64_t q = qb + (threadIdx.x & 31) / g;
+      const bool valid = q < r1;
+      const int32_t row = valid ? A.perm[q] : 0;
+      const int32_t kb = valid ? A.rp[row] : 0, ke = valid ? A.rp[row + 1] : 0;
+      double s0 = 0.0, s1 = 0.0;
+      for (int32_t k = kb + lane_g; k < ke; k += g) {
+        const double a = A.v[k];
+        const int32_t col = A.ci[k];
+        s0 = fma(a, x0[col], s0);
+        if (NV == 2) s1 = fma(a, x1[col], s1);
+      }
+      for (int o = g >> 1; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(kFull, s0, o, g);
+        if (NV == 2) s1 += __shfl_down_sync(kFull, s1, o, g);
+      }
+      if (valid && lane_g == 0) {
+        y0[row] = s0;
+        if (NV == 2) y1[row] = s1;
+      }
+    }
+  } else {
+    __shared__ double red0[kWarps], red1[kWarps];
+    for (int64_t q = r0 + lcta; q < r1; q += ncta) {
+      const int32_t row = A.perm[q];
+      const int32_t kb = A.rp[row], ke = A.rp[row + 1];
+      double s0 = 0.0, s1 = 0.0;
+      for (int32_t k = kb + threadIdx.x; k < ke; k += kThreads) {
+        const double a = A.v[k];
+        const int32_t col = A.ci[k];
+        s0 = fma(a, x0[col], s0);
+        if (NV == 2) s1 = fma(a, x1[col], s1);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(kFull, s0, o);
+        if (NV == 2) s1 += __shfl_down_sync(kFull, s1, o);
+      }
+      const int w = threadIdx.x >> 5;
+      if ((threadIdx.x & 31) == 0) {
+        red0[w] = s0;
+        red1[w] = s1;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int i = 0; i < kWarps; ++i) {
+          t0 += red0[i];
+          t1 += red1[i];
+        }
+        y0[row] = t0;
+        if (NV == 2) y1[row] = t1;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Block structure of one vector for projections.
+// ---------------------------------------------------------------------------
+struct ConeTable {
+  int64_t len;
+  int32_t nseg;
+  int32_t seg_kind[3];
+  int64_t seg_start[3], seg_len[3];
+  const double* lo;  // BOX bounds (global index)
+  const double* hi;
+  int64_t nwc;               // SOC / RSOC blocks (one warp each)
+  const int64_t* wc_start;
+  const int32_t* wc_len;
+  const int8_t* wc_kind;     // PK_SOC or PK_RSOC
+  int64_t exp_base, exp_count;   // contiguous triples
+  int32_t exp_kind;              // PK_EXP or PK_DEXP
+  int64_t dexp_base, dexp_count;
+  int32_t dexp_kind;
+  const double* S;           // scaling (NULL: unscaled)
+  int64_t elem_total;        // sum of seg_len
+  int32_t ctaA, ctaB, ctaC;  // CTAs for elementwise / warp cones / exp cones
+};
+
+__device__ __forceinline__ double elem_proj(int32_t kind, double z, int64_t j, const ConeTable& T) {
+  switch (kind) {
+    case PK_ZERO: return 0.0;
+    case PK_NONNEG: return fmax(z, 0.0);
+    case PK_BOX: return fmin(fmax(z, T.lo[j]), T.hi[j]);
+    default: return z;
+  }
+}
+
+template <int N>
+__device__ inline void block_reduce_store(double (&acc)[N], const int32_t* kinds, double* partials, int nblocks) {
+  __shared__ double sh[N][kWarps];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double v = acc[k];
+    if (kinds[k] == ACC_MAX) {
+      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(kFull, v, o));
+    } else {
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    }
+    if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < N) {
+    int k = threadIdx.x;
+    double v = sh[k][0];
+    for (int w = 1; w < kWarps; ++w) v = (kinds[k] == ACC_MAX) ? fmax(v, sh[k][w]) : v + sh[k][w];
+    partials[(int64_t)k * nblocks + blockIdx.x] = v;
+  }
+}
+
+// Generic update + projection.  Op supplies:
+//   NACC, kinds[] (ACC_SUM / ACC_MAX), double* out (result / scratch, length T.len),
+//   load(): read scalars; z(j): value before projection; fin(j, z, p, acc): consume.
+template <class Op>
+__global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTable T, double* partials,
+                                                                 const int32_t* active) {
+  if (active && !*active) return;
+  op.load();
+  double acc[Op::NACC];
+#pragma unroll
+  for (int k = 0; k < Op::NACC; ++k) acc[k] = 0.0;
+  const int b = blockIdx.x;
+  const int nblocks = gridDim.x;
+  if (b < T.ctaA) {
+    const int64_t stride = (int64_t)T.ctaA * kThreads;
+    for (int s = 0; s < T.nseg; ++s) {
+      const int64_t j0 = T.seg_start[s], j1 = j0 + T.seg_len[s];
+      const int32_t kind = T.seg_kind[s];
+      for (int64_t j = j0 + (int64_t)b * kThreads + threadIdx.x; j < j1; j += stride) {
+        double z = op.z(j);
+        double p = elem_proj(kind, z, j, T);
+        op.fin(j, z, p, acc);
+      }
+    }
+  } else if (b < T.ctaA + T.ctaB) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wstride = (int64_t)T.ctaB * kWarps;
+    for (int64_t k = (int64_t)(b - T.ctaA) * kWarps + (threadIdx.x >> 5); k < T.nwc; k += wstride) {
+      const int64_t st = T.wc_start[k];
+      const int32_t d = T.wc_len[k];
+      const bool rsoc = T.wc_kind[k] == PK_RSOC;
+      const double* S = T.S ? T.S + st : nullptr;
+      const double r2 = 0.7071067811865476;
+      if (d <= 32) {
+        double z = (lane < d) ? op.z(st + lane) : 0.0;
+        double v = z;
+        double w = 1.0;
+        if (S && lane < d) {
+          if (rsoc) w = (lane >= 2) ? sqrt(S[0] * S[1]) / S[lane] : 1.0;
+          else w = (lane >= 1) ? S[0] / S[lane] : 1.0;
+        }
+        bool weighted = __any_sync(kFull, w != 1.0);
+        if (rsoc) {
+          double p0 = __shfl_sync(kFull, v, 0), q0 = __shfl_sync(kFull, v, 1);
+          if (lane == 0) v = (p0 + q0) * r2;
+          if (lane == 1) v = (p0 - q0) * r2;
+        }
+        warp_soc_reg(v, w, d, weighted);
+        if (rsoc) {
+          double a0 = __shfl_sync(kFull, v, 0), b0 = __shfl_sync(kFull, v, 1);
+          if (lane == 0) v = (a0 + b0) * r2;
+          if (lane == 1) v = (a0 - b0) * r2;
+        }
+        if (lane < d) op.fin(st + lane, z, v, acc);
+      } else {
+        double* p = op.out + st;
+        for (int64_t i = lane; i < d; i += 32) p[i] = op.z(st + i);
+        __syncwarp();
+        bool weighted = false;
+        if (S) {
+          double g = rsoc ? sqrt(S[0] * S[1]) : S[0];
+          bool any = false;
+          for (int64_t i = (rsoc ? 2 : 1) + lane; i < d; i += 32) any |= (g / S[i] != 1.0);
+          weighted = __any_sync(kFull, any);
+        }
+        if (rsoc) {
+          if (lane == 0) {
+            double p0 = p[0], q0 = p[1];
+            p[0] = (p0 + q0) * r2;
+            p[1] = (p0 - q0) * r2;
+          }
+          __syncwarp();
+          double g = S ? sqrt(S[0] * S[1]) : 1.0;
+          warp_soc_mem(p, d, [&](int64_t i) { return (i == 1 || !S) ? 1.0 : g / S[i]; }, weighted);
+          __syncwarp();
+          if (lane == 0) {
+            double a0 = p[0], b0 = p[1];
+            p[0] = (a0 + b0) * r2;
+            p[1] = (a0 - b0) * r2;
+          }
+        } else {
+          warp_soc_mem(p, d, [&](int64_t i) { return S ? S[0] / S[i] : 1.0; }, weighted);
+        }
+        __syncwarp();
+        for (int64_t i = lane; i < d; i += 32) {
+          double pi = p[i];
+          op.fin(st + i, op.z(st + i), pi, acc);
+        }
+        __syncwarp();
+      }
+    }
+  } else {
+    const int64_t tstride = (int64_t)T.ctaC * kThreads;
+    const int64_t total = T.exp_count + T.dexp_count;
+    for (int64_t k = (int64_t)(b - T.ctaA - T.ctaB) * kThreads + threadIdx.x; k < total; k += tstride) {
+      const bool first = k < T.exp_count;
+      const int64_t j = first ? T.exp_base + 3 * k : T.dexp_base + 3 * (k - T.exp_count);
+      const int32_t kind = first ? T.exp_kind : T.dexp_kind;
+      double z0 = op.z(j), z1 = op.z(j + 1), z2 = op.z(j + 2);
+      double r = z0, s = z1, t = z2;
+      double S0 = 1.0, S1 = 1.0, S2 = 1.0;
+      if (T.S) {
+        S0 = T.S[j];
+        S1 = T.S[j + 1];
+        S2 = T.S[j + 2];
+      }
+      if (kind == PK_EXP) proj_exp_scaled_dev(r, s, t, S0, S1, S2);
+      else proj_dexp_scaled_dev(r, s, t, S0, S1, S2);
+      op.fin(j, z0, r, acc);
+      op.fin(j + 1, z1, s, acc);
+      op.fin(j + 2, z2, t, acc);
+    }
+  }
+  block_reduce_store<Op::NACC>(acc, Op::kinds(), partials, nblocks);
+}
+
+// ---------------------------------------------------------------------------
+// Ops
+// ---------------------------------------------------------------------------
+__device__ __constant__ int32_t kSum1[1] = {ACC_SUM};
+__device__ __constant__ int32_t kSum2[2] = {ACC_SUM, ACC_SUM};
+__device__ __constant__ int32_t kSum3[3] = {ACC_SUM, ACC_SUM, ACC_SUM};
+__device__ __constant__ int32_t kResid7[7] = {ACC_SUM, ACC_MAX, ACC_MAX, ACC_SUM, ACC_MAX, ACC_SUM, ACC_SUM};
+
+// x = P(x_lag + ps (aty - c)); acc: sum (x - x_lag)^2
+struct OpPrimalStep {
+  static constexpr int NACC = 1;
+  __device__ static const int32_t* kinds() { return kSum1; }
+  const double* xl;
+  const double* aty;
+  const double* c;
+  double* out;
+  const PdhgState* st;
+  double ps;
+  __device__ void load() { ps = st->ps; }
+  __device__ double z(int64_t j) const { return xl[j] + ps * (aty[j] - c[j]); }
+  __device__ void fin(int64_t j, double, double p, double* acc) const {
+    out[j] = p;
+    double d = p - xl[j];
+    acc[0] = fma(d, d, acc[0]);
+  }
+};
+
+// y = P(y_lag - ds (2 gx - gxl - h)); acc: sum (y - y_lag)^2, sum (y - y_lag)(gx - gxl)
+struct OpDualStep {
+  static constexpr int NACC = 2;
+  __device__ static const int32_t* kinds() { return kSum2; }
+  const double* yl;
+  const double* gx;
+  const double* gxl;
+  const double* h;
+  double* out;
+  const PdhgState* st;
+  double ds;
+  __device__ void load() { ds = st->ds; }
+  __device__ double z(int64_t i) const { return yl[i] - ds * ((2.0 * gx[i] - gxl[i]) - h[i]); }
+  __device__ void fin(int64_t i, double, double p, double* acc) const {
+    out[i] = p;
+    double d = p - yl[i];
+    acc[0] = fma(d, d, acc[0]);
+    acc[1] = fma(d, gx[i] - gxl[i], acc[1]);
+  }
+};
+
+// out = P(base + alpha dir); acc: [0] sum (out - base)^2, [1] sum dir*(out - base),
+// [2] sum (out - base)*(g1 - g0) when g1 != NULL (restart binary search, Mnorm)
+struct OpAxpyProj {
+  static constexpr int NACC = 3;
+  __device__ static const int32_t* kinds() { return kSum3; }
+  const double* base;
+  const double* dir;
+  double alpha;
+  double* out;
+  const double* g1;
+  const double* g0;
+  __device__ void load() {}
+  __device__ double z(int64_t j) const { return base[j] + alpha * dir[j]; }
+  __device__ void fin(int64_t j, double, double p, double* acc) const {
+    out[j] = p;
+    double d = p - base[j];
+    acc[0] = fma(d, d, acc[0]);
+    acc[1] = fma(dir[j], d, acc[1]);
+    if (g1) acc[2] = fma(d, g1[j] - g0[j], acc[2]);
+  }
+};
+
+// Residual of a vector against its projection: z = a*u + b*w - c*q (any of
+// u, w, q may be NULL, scaled elementwise by su / sw when given); p = P(z).
+// acc: [0] sum (p-z)^2, [1] max |p-z|, [2] max |p|, [3] sum |p|,
+//      [4] max |a*u*su|, [5] sum |a*u*su|, [6] box dual objective contribution
+struct OpResidual {
+  static constexpr int NACC = 7;
+  __device__ static const int32_t* kinds() { return kResid7; }
+  const double* u;
+  const double* su;
+  double a;
+  const double* w;
+  double b;
+  const double* q;
+  double* out;
+  // dual-objective term of the box block: sum bl_fin * max(z, 0) + bu_fin * min(z, 0) over j < nbox
+  const double* bl_fin;
+  const double* bu_fin;
+  int64_t nbox;
+  __device__ void load() {}
+  __device__ double uterm(int64_t j) const { return u ? a * u[j] * (su ? su[j] : 1.0) : 0.0; }
+  __device__ double z(int64_t j) const {
+    double v = uterm(j);
+    if (w) v += b * w[j];
+    if (q) v -= q[j];
+    return v;
+  }
+  __device__ void fin(int64_t j, double z, double p, double* acc) const {
+    if (out) out[j] = p;
+    double d = p - z;
+    acc[0] = fma(d, d, acc[0]);
+    acc[1] = fmax(acc[1], fabs(d));
+    acc[2] = fmax(acc[2], fabs(p));
+    acc[3] += fabs(p);
+    double ut = fabs(uterm(j));
+    acc[4] = fmax(acc[4], ut);
+    acc[5] += ut;
+    if (j < nbox) acc[6] += bl_fin[j] * fmax(z, 0.0) + bu_fin[j] * fmin(z, 0.0);
+  }
+};
+
+// Dot products / norms of up to 4 vectors in one pass (deterministic).
+struct DotSpec {
+  const double* a[4];
+  const double* b[4];   // second operand (DK_DOT: NULL means a itself; DK_DIFF2: required)
+  const double* sa[4];  // optional elementwise divisor of a
+  int32_t kind[4];      // DotKind
+  int32_t count;
+  int64_t len;
+};
+
+}  // namespace pdcs

@@ -1,0 +1,1496 @@
+// pdcs_solver.cu -- B200-native restarted, diagonally preconditioned,
+// adaptive-step PDHG for PDCS conic programs, behind the C ABI of pdcs.h.
+//
+// Host control mirrors the reference's aggressive main loop
+// (src/pdcs_gpu/rpdhg_alg_gpu_gen_scaling.jl:770-895).  The inner loop runs on
+// the device: PDHG attempts are captured in CUDA graphs and the accept/retry
+// decision, step sizes and the reflected averaging are computed by kernels on a
+// device-resident state, so the host only intervenes at the reference's
+// checkpoints (iter % check_terminate_freq, restart checks, artificial restarts).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/pdcs.h"
+#include "pdcs_kernels.cuh"
+
+namespace pdcs {
+
+// ===========================================================================
+// Kernels with a single instantiation
+// ===========================================================================
+
+__global__ void finalize_partials_kernel2(const double* __restrict__ partials, int nblocks, int nacc,
+                                          uint32_t maxmask, double* __restrict__ out) {
+  const int k = blockIdx.x;
+  if (k >= nacc) return;
+  const bool mx = (maxmask >> k) & 1u;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+    double p = partials[(int64_t)k * nblocks + i];
+    v = mx ? fmax(v, p) : v + p;
+  }
+  __shared__ double sh[kThreads];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = kThreads / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] = mx ? fmax(sh[threadIdx.x], sh[threadIdx.x + s]) : sh[threadIdx.x] + sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[k] = sh[0];
+}
+
+// DotSpec kinds
+enum DotKind : int32_t { DK_DOT = 0, DK_MAXABS = 1, DK_SUMABS = 2, DK_DIFF2 = 3 };
+
+__global__ void __launch_bounds__(kThreads) dots_kernel(DotSpec spec, double* partials) {
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < spec.len; i += stride) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (k >= spec.count) break;
+      double a = spec.a[k][i];
+      if (spec.sa[k]) a /= spec.sa[k][i];
+      switch (spec.kind[k]) {
+        case DK_DOT: acc[k] = fma(a, spec.b[k] ? spec.b[k][i] : a, acc[k]); break;
+        case DK_MAXABS: acc[k] = fmax(acc[k], fabs(a)); break;
+        case DK_SUMABS: acc[k] += fabs(a); break;
+        case DK_DIFF2: { double d = a - spec.b[k][i]; acc[k] = fma(d, d, acc[k]); } break;
+      }
+    }
+  }
+  __shared__ double sh[4][kWarps];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double v = acc[k];
+    const bool mx = spec.kind[k] == DK_MAXABS;
+    for (int o = 16; o > 0; o >>= 1) v = mx ? fmax(v, __shfl_down_sync(kFull, v, o)) : v + __shfl_down_sync(kFull, v, o);
+    if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int k = threadIdx.x;
+    const bool mx = spec.kind[k] == DK_MAXABS;
+    double v = sh[k][0];
+    for (int w = 1; w < kWarps; ++w) v = mx ? fmax(v, sh[k][w]) : v + sh[k][w];
+    partials[(int64_t)k * gridDim.x + blockIdx.x] = v;
+  }
+}
+
+__global__ void control_kernel(PdhgState* st, const double* __restrict__ px, int nbx, const double* __restrict__ py,
+                               int nby) {
+  if (!st->active) {
+    if (threadIdx.x == 0) st->do_reflect = 0;
+    return;
+  }
+  __shared__ double sh[3][kThreads];
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int i = threadIdx.x; i < nbx; i += kThreads) a += px[i];
+  for (int i = threadIdx.x; i < nby; i += kThreads) {
+    b += py[i];
+    c += py[nby + i];
+  }
+  sh[0][threadIdx.x] = a;
+  sh[1][threadIdx.x] = b;
+  sh[2][threadIdx.x] = c;
+  __syncthreads();
+  for (int s = kThreads / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + s];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + s];
+      sh[2][threadIdx.x] += sh[2][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  PdhgState s = *st;
+  s.sum_dx2 = sh[0][0];
+  s.sum_dy2 = sh[1][0];
+  s.sum_dgdy = sh[2][0];
+  s.do_reflect = 0;
+  // eta_bar and eta' (rpdhg_alg_gpu_gen_scaling.jl:711-715)
+  double num = s.omega * s.sum_dx2 + s.sum_dy2 / s.omega;
+  double den = 2.0 * fabs(s.sum_dgdy);
+  s.eta_bar = num / (den + 1e-20);
+  s.iter += 1;
+  s.iter_stepsize += 1;
+  double k1 = (double)(s.iter_stepsize + 1);
+  s.eta_p = fmin((1.0 - pow(k1, -0.3)) * s.eta_bar, (1.0 + pow(k1, -0.6)) * s.eta);
+  s.tau = s.eta / s.omega;
+  s.sigma = s.eta * s.omega;
+  s.accepted = (s.eta <= s.eta_bar) ? 1 : 0;
+  if (s.check_freq > 0 && s.iter % s.check_freq == 0) {
+    s.halt_reason = HALT_CHECK;  // the host runs the exit check, then decides
+    s.active = 0;
+  } else if (s.attempt_limit > 0 && s.iter >= s.attempt_limit) {
+    s.halt_reason = HALT_LIMIT;
+    s.active = 0;
+  } else if (s.accepted) {
+    post_accept(s, false);
+  } else {
+    after_reject(s);
+    if (s.reject_count > 1000000) {
+      s.eta = s.eta_p;  // the forced return hands back the last eta (:757-764)
+      post_accept(s, true);
+    }
+  }
+  *st = s;
+}
+
+__global__ void __launch_bounds__(kThreads) reflect_kernel(PdhgState* st, double* __restrict__ x,
+                                                           double* __restrict__ xl, double* __restrict__ xm,
+                                                           int64_t n, double* __restrict__ y, double* __restrict__ yl,
+                                                           double* __restrict__ ym, int64_t m) {
+  if (!st->do_reflect) return;
+  const double tmp = st->refl_tmp, inv = st->refl_inv, e = st->refl_extra, eta = st->refl_eta, cum = st->refl_cum;
+  const double wsum = cum + eta;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t L = n > m ? n : m;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < L; i += stride) {
+    if (i < n) {
+      double xv = x[i];
+      double xn = tmp * ((1.0 + e) * xv - e * xl[i]) + inv * xv;
+      xm[i] = (xm[i] * cum + xn * eta) / wsum;
+      x[i] = xn;
+      xl[i] = xn;
+    }
+    if (i < m) {
+      double yv = y[i];
+      double yn = tmp * ((1.0 + e) * yv - e * yl[i]) + inv * yv;
+      ym[i] = (ym[i] * cum + yn * eta) / wsum;
+      y[i] = yn;
+      yl[i] = yn;
+    }
+  }
+}
+
+// y = A x with rows in natural order and one lane-group size (pdcs_spmv_csr)
+__global__ void __launch_bounds__(kThreads) spmv_identity_kernel(CsrDev A, int bin, const double* __restrict__ x,
+                                                                 double* __restrict__ y) {
+  const int g = 1 << bin;
+  const int lane_g = threadIdx.x & (g - 1);
+  const int64_t rows_per_cta = kThreads / g;
+  const int64_t warp_first = (int64_t)blockIdx.x * rows_per_cta + (threadIdx.x >> 5) * (32 / g);
+  for (int64_t qb = warp_first; qb < A.m; qb += (int64_t)gridDim.x * rows_per_cta) {
+    const int64_t row = qb + (threadIdx.x & 31) / g;
+    const bool valid = row < A.m;
+    const int32_t kb = valid ? A.rp[row] : 0, ke = valid ? A.rp[row + 1] : 0;
+    double s0 = 0.0;
+    for (int32_t k = kb + lane_g; k < ke; k += g) s0 = fma(A.v[k], x[A.ci[k]], s0);
+    for (int o = g >> 1; o > 0; o >>= 1) s0 += __shfl_down_sync(kFull, s0, o, g);
+    if (valid && lane_g == 0) y[row] = s0;
+  }
+}
+
+// out = a*u + b*v (u, v may alias out)
+__global__ void axpby_kernel(double* out, double a, const double* u, double b, const double* v, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    out[i] = a * u[i] + (v ? b * v[i] : 0.0);
+}
+// out = u / d
+__global__ void div_kernel(double* out, const double* u, const double* d, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = u[i] / d[i];
+}
+
+// standalone projection entry (pdcs_block_proj): one block per CTA-warp
+__global__ void __launch_bounds__(kThreads) block_proj_kernel(double* arr, const double* bl, const double* bu,
+                                                              const double* S, const int64_t* head,
+                                                              const int64_t* ns, int64_t nblk,
+                                                              const int64_t* code) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  const int64_t wstride = ((int64_t)gridDim.x * kThreads) >> 5;
+  const double r2 = 0.7071067811865476;
+  for (int64_t b = wid; b < nblk; b += wstride) {
+    const int64_t st = head[b], d = ns[b];
+    const int64_t c = code[b];
+    double* p = arr + st;
+    switch (c) {
+      case 0: case 1: break;
+      case 2: for (int64_t i = lane; i < d; i += 32) p[i] = 0.0; break;
+      case 3: case 4: for (int64_t i = lane; i < d; i += 32) p[i] = fmax(p[i], 0.0); break;
+      case 17: case 18: case 19:
+        for (int64_t i = lane; i < d; i += 32) p[i] = fmin(fmax(p[i], bl[st + i]), bu[st + i]);
+        break;
+      case 5: case 7: case 20: case 21:
+        warp_soc_mem(p, d, [](int64_t) { return 1.0; }, false);
+        break;
+      case 6: case 22: {
+        const double* Sb = S + st;
+        warp_soc_mem(p, d, [&](int64_t i) { return Sb[0] / Sb[i]; }, true);
+      } break;
+      case 8: case 10: case 23: case 24: case 9: case 25: {
+        const bool sc = (c == 9 || c == 25);
+        const double* Sb = sc ? S + st : nullptr;
+        if (d >= 3) {
+          if (lane == 0) {
+            double p0 = p[0], q0 = p[1];
+            p[0] = (p0 + q0) * r2;
+            p[1] = (p0 - q0) * r2;
+          }
+          __syncwarp();
+          double g = sc ? sqrt(Sb[0] * Sb[1]) : 1.0;
+          warp_soc_mem(p, d, [&](int64_t i) { return (i == 1 || !sc) ? 1.0 : g / Sb[i]; }, sc);
+          __syncwarp();
+          if (lane == 0) {
+            double a0 = p[0], b0 = p[1];
+            p[0] = (a0 + b0) * r2;
+            p[1] = (a0 - b0) * r2;
+          }
+        } else {
+          for (int64_t i = lane; i < d; i += 32) p[i] = fmax(p[i], 0.0);
+        }
+      } break;
+      case 11: case 16: case 28: case 12: case 29:
+        if (lane == 0 && d == 3) {
+          double Sr = 1.0, Ss = 1.0, St = 1.0;
+          if (c == 12 || c == 29) { Sr = S[st]; Ss = S[st + 1]; St = S[st + 2]; }
+          proj_dexp_scaled_dev(p[0], p[1], p[2], Sr, Ss, St);
+        }
+        break;
+      case 13: case 14: case 26: case 15: case 27:
+        if (lane == 0 && d == 3) {
+          double Sr = 1.0, Ss = 1.0, St = 1.0;
+          if (c == 15 || c == 27) { Sr = S[st]; Ss = S[st + 1]; St = S[st + 2]; }
+          proj_exp_scaled_dev(p[0], p[1], p[2], Sr, Ss, St);
+        }
+        break;
+      default: break;
+    }
+    __syncwarp();
+  }
+}
+
+// ===========================================================================
+// Host side
+// ===========================================================================
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+#define PDCS_CUDA(call)                                                                         \
+  do {                                                                                          \
+    cudaError_t e__ = (call);                                                                   \
+    if (e__ != cudaSuccess)                                                                     \
+      throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e__));                    \
+  } while (0)
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Arena {
+  std::vector<void*> ptrs;
+  template <class T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    PDCS_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  ~Arena() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+};
+
+struct HostCsr {
+  int64_t m = 0, n = 0;
+  std::vector<int32_t> rp, ci;
+  std::vector<double> v;
+};
+
+static HostCsr transpose(const HostCsr& A) {
+  HostCsr T;
+  T.m = A.n;
+  T.n = A.m;
+  T.rp.assign(A.n + 1, 0);
+  const int64_t nnz = A.rp[A.m];
+  T.ci.resize(nnz);
+  T.v.resize(nnz);
+  for (int64_t k = 0; k < nnz; ++k) T.rp[A.ci[k] + 1]++;
+  for (int64_t j = 0; j < A.n; ++j) T.rp[j + 1] += T.rp[j];
+  std::vector<int32_t> pos(T.rp.begin(), T.rp.end() - 1);
+  for (int64_t i = 0; i < A.m; ++i)
+    for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      int32_t q = pos[A.ci[k]]++;
+      T.ci[q] = (int32_t)i;
+      T.v[q] = A.v[k];
+    }
+  return T;
+}
+
+struct Converge {
+  double pobj = 1e30, dobj = 1e30, abs_gap = 1e30, rel_gap = 1e30;
+  double linf_rel_p = 1e30, linf_rel_d = 1e30, l2_rel_p = 1e30, l2_rel_d = 1e30;
+  double linf_abs_p = 1e30, linf_abs_d = 1e30, l2_abs_p = 1e30, l2_abs_d = 1e30;
+  int status = PDCS_EXIT_CONTINUE;
+};
+
+struct Infea {
+  double max_primal_ray_inf = 1e30, primal_ray_obj = 1e30, max_dual_ray_inf = 1e30, dual_ray_obj = 1e30;
+  double primal_ray_norm = 0, dual_ray_norm = 0;
+  std::vector<double> ptrend, dtrend;
+  int status = PDCS_EXIT_CONTINUE;
+};
+
+class Solver {
+ public:
+  Solver(const pdcs_problem* p, const pdcs_options* o) : P(*p), O(*o) {}
+  ~Solver() {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    if (host_state_) cudaFreeHost(host_state_);
+    if (host_red_) cudaFreeHost(host_red_);
+    if (own_stream_) cudaStreamDestroy(s_);
+  }
+  int run(pdcs_result* res);
+
+ private:
+  pdcs_problem P;
+  pdcs_options O;
+  Arena A;
+  cudaStream_t s_ = nullptr;
+  bool own_stream_ = false;
+  int64_t n_ = 0, m_ = 0, nb_ = 0, nnz_ = 0;
+  // device data
+  CsrDev G_{}, Gt_{};
+  double *c_s = nullptr, *c_raw = nullptr, *h_s = nullptr, *h_raw = nullptr, *Dr = nullptr, *Dl = nullptr;
+  double *bl_s = nullptr, *bu_s = nullptr, *lam_l = nullptr, *lam_u = nullptr, *bl_fin = nullptr, *bu_fin = nullptr;
+  double *x = nullptr, *xl = nullptr, *xm = nullptr, *aty = nullptr, *x0 = nullptr, *x0l = nullptr, *xbest = nullptr;
+  double *y = nullptr, *yl = nullptr, *ym = nullptr, *gx = nullptr, *gxl = nullptr, *y0 = nullptr, *y0l = nullptr,
+         *ybest = nullptr;
+  double *tn[6] = {}, *tm[6] = {};
+  double *xds_ = nullptr, *yds_ = nullptr;  // iterates at the start of an outer iteration (omega update)
+  double *part_x = nullptr, *part_y = nullptr, *part_r = nullptr, *red_out = nullptr;
+  PdhgState* st_dev = nullptr;
+  PdhgState* host_state_ = nullptr;
+  double* host_red_ = nullptr;
+  ConeTable XI{}, YI{}, CON{}, SLK{};
+  int grid_reflect_ = 1, grid_vec_n_ = 1, grid_vec_m_ = 1;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  int attempts_per_graph_ = 32;
+  double ginf_ = 0.0, hNrm1 = 0, hNrmInf = 0, cNrm1 = 0, cNrmInf = 0;
+  // algorithm state (host mirror of Solution / PDHGCLPInfo)
+  PdhgState S{};
+  Converge ci[2];
+  Infea ii[2];
+  int exit_code_ = PDCS_EXIT_CONTINUE;
+  int returned_seq_ = 0;
+  double pobj_ = 1e30, dobj_ = 1e30;
+  double max_kkt_ = 1e30, min_kkt_ = 1e30;
+  double pres_best_ = 1e30, dres_best_ = 1e30;
+  double ndg_[2] = {1e30, 1e30}, ndg_thr_ = 0, ndg_r_ = 1e30, kkt_err_[2] = {1e30, 1e30}, kkt_thr_ = 0;
+  bool dgap_flag_ = true;
+  double bs_t0_ = 1.0;
+  int64_t restart_used_ = 0, check_count_ = 0;
+  double t_start_ = 0;
+  int64_t kernels_ = 0, graphs_ = 0;
+
+  // ---- setup ----
+  int validate();
+  void setup();
+  void build_bins(const HostCsr& H, const int32_t* d_rp, const int32_t* d_ci, const double* d_v, CsrDev& D);
+  void build_tables(const std::vector<int64_t>& soc_x, const std::vector<int64_t>& rsoc_x,
+                    const std::vector<int64_t>& socG, const std::vector<int64_t>& rsocG);
+  void size_table(ConeTable& T);
+  void capture_graph();
+  // ---- device helpers ----
+  void spmv(const CsrDev& M, const double* xin, double* yout) {
+    spmv_binned_kernel<1><<<M.cta0[kBins], kThreads, 0, s_>>>(M, xin, nullptr, yout, nullptr, nullptr);
+    kernels_++;
+  }
+  void axpby(double* out, double a, const double* u, double b, const double* v, int64_t len) {
+    axpby_kernel<<<grid_for(len), kThreads, 0, s_>>>(out, a, u, b, v, len);
+    kernels_++;
+  }
+  void copy(double* dst, const double* src, int64_t len) {
+    PDCS_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * len, cudaMemcpyDeviceToDevice, s_));
+  }
+  int grid_for(int64_t len) const { return (int)std::max<int64_t>(1, std::min<int64_t>((len + kThreads - 1) / kThreads, 148 * 8)); }
+  template <class Op>
+  void update_project(const Op& op, const ConeTable& T, double* partials) {
+    update_project_kernel<Op><<<T.ctaA + T.ctaB + T.ctaC, kThreads, 0, s_>>>(op, T, partials, nullptr);
+    kernels_++;
+  }
+  // reduce partials of the last kernel to host values
+  void finalize(const double* partials, int nblocks, int nacc, uint32_t maxmask, double* out_host) {
+    finalize_partials_kernel2<<<nacc, kThreads, 0, s_>>>(partials, nblocks, nacc, maxmask, red_out);
+    kernels_++;
+    PDCS_CUDA(cudaMemcpyAsync(host_red_, red_out, sizeof(double) * nacc, cudaMemcpyDeviceToHost, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    for (int k = 0; k < nacc; ++k) out_host[k] = host_red_[k];
+  }
+  void dots(DotSpec spec, double* out_host) {
+    int g = grid_for(spec.len);
+    for (int k = spec.count; k < 4; ++k) {
+      spec.a[k] = spec.a[0];
+      spec.b[k] = nullptr;
+      spec.sa[k] = nullptr;
+      spec.kind[k] = DK_DOT;
+    }
+    dots_kernel<<<g, kThreads, 0, s_>>>(spec, part_r);
+    kernels_++;
+    uint32_t mask = 0;
+    for (int k = 0; k < 4; ++k)
+      if (spec.kind[k] == DK_MAXABS) mask |= 1u << k;
+    double tmp[4];
+    finalize(part_r, g, 4, mask, tmp);
+    for (int k = 0; k < spec.count; ++k) out_host[k] = tmp[k];
+  }
+  double nrm2(const double* a, int64_t len) {
+    DotSpec d{};
+    d.a[0] = a;
+    d.kind[0] = DK_DOT;
+    d.count = 1;
+    d.len = len;
+    double v;
+    dots(d, &v);
+    return std::sqrt(v);
+  }
+  void push_state() {
+    // synchronous w.r.t. the pinned staging buffer, which the next push reuses
+    *host_state_ = S;
+    PDCS_CUDA(cudaMemcpyAsync(st_dev, host_state_, sizeof(PdhgState), cudaMemcpyHostToDevice, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+  }
+  void pull_state() {
+    PDCS_CUDA(cudaMemcpyAsync(host_state_, st_dev, sizeof(PdhgState), cudaMemcpyDeviceToHost, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    S = *host_state_;
+  }
+  // ---- algorithm ----
+  double decay(double mk) const { return std::min(0.9 + 0.1 * std::log10(mk * 1e5), 1.0); }
+  void converge_info(const double* xs, const double* ys, Converge& C, double* gxs, double* atys);
+  void exit_check();
+  void check_termination();
+  double mnorm(const double* dx, const double* dy, double ta, double si);
+  double binary_search(double r, const double* px, const double* py, double ta, double si);
+  double kkt_error(const Converge& C) const {
+    return std::sqrt(S.omega * S.omega * C.l2_abs_p * C.l2_abs_p + C.l2_abs_d * C.l2_abs_d / (S.omega * S.omega) +
+                     C.abs_gap * C.abs_gap);
+  }
+  void restart_threshold(bool dgap);
+  bool restart_check(bool dgap);
+  double init_omega() {
+    double hn = nrm2(h_s, m_), cn = nrm2(c_s, n_);
+    return (hn > 1e-10 && cn > 1e-10) ? cn / hn : 1.0;
+  }
+  void run_until_halt();
+  void main_loop();
+  void log_progress();
+};
+
+// ---------------------------------------------------------------------------
+int Solver::validate() {
+  if (P.n < 0 || P.m < 0 || P.nb < 0 || P.nb > P.n || P.nnz < 0) return PDCS_ERR_INVALID;
+  if ((P.m > 0 && (!P.G_rowptr || !P.h)) || (P.n > 0 && !P.c) || (P.nnz > 0 && (!P.G_colind || !P.G_val)))
+    return PDCS_ERR_INVALID;
+  if (P.nb > 0 && (!P.bl || !P.bu)) return PDCS_ERR_INVALID;
+  if (P.nnz > INT32_MAX || P.n > INT32_MAX || P.m > INT32_MAX) return PDCS_ERR_INVALID;
+  int64_t msum = P.mGzero + P.mGnonnegative + 3 * (P.expG + P.dual_expG);
+  for (int64_t i = 0; i < P.n_socG; ++i) msum += P.socG[i];
+  for (int64_t i = 0; i < P.n_rsocG; ++i) msum += P.rsocG[i];
+  if (msum != P.m) return PDCS_ERR_M_MISMATCH;
+  for (int64_t i = 0; i < P.n_socG; ++i) if (P.socG[i] < 2) return PDCS_ERR_SOC_DIM;
+  for (int64_t i = 0; i < P.n_soc_x; ++i) if (P.soc_x[i] < 2) return PDCS_ERR_SOC_DIM;
+  for (int64_t i = 0; i < P.n_rsocG; ++i) if (P.rsocG[i] < 3) return PDCS_ERR_RSOC_DIM;
+  for (int64_t i = 0; i < P.n_rsoc_x; ++i) if (P.rsoc_x[i] < 3) return PDCS_ERR_RSOC_DIM;
+  int64_t nsum = P.nb + 3 * (P.exp_x + P.dual_exp_x);
+  for (int64_t i = 0; i < P.n_soc_x; ++i) nsum += P.soc_x[i];
+  for (int64_t i = 0; i < P.n_rsoc_x; ++i) nsum += P.rsoc_x[i];
+  if (nsum > P.n) return PDCS_ERR_N_MISMATCH;
+  if (O.use_preconditioner == 0 || O.use_adaptive_restart == 0 || O.use_adaptive_step_size_weight == 0 ||
+      O.use_aggressive == 0 || O.use_accelerated != 0 || O.precision != 0)
+    return PDCS_ERR_UNSUPPORTED;  // only the reference GPU module's live main loop (rpdhg_alg_gpu_gen.jl:1886-1927)
+  return PDCS_OK;
+}
+
+void Solver::build_bins(const HostCsr& H, const int32_t* d_rp, const int32_t* d_ci, const double* d_v, CsrDev& D) {
+  D.m = H.m;
+  D.n = H.n;
+  D.nnz = H.rp[H.m];
+  D.rp = d_rp;
+  D.ci = d_ci;
+  D.v = d_v;
+  std::vector<std::vector<int32_t>> bins(kBins);
+  for (int64_t i = 0; i < H.m; ++i) {
+    int64_t L = H.rp[i + 1] - H.rp[i];
+    int b;
+    if (L > 1024) b = kBins - 1;
+    else {
+      int g = 1;
+      b = 0;
+      while (g < 32 && (int64_t)g * 4 < L) {
+        g *= 2;
+        b++;
+      }
+    }
+    bins[b].push_back((int32_t)i);
+  }
+  std::vector<int32_t> perm;
+  perm.reserve(H.m);
+  int64_t off = 0;
+  int32_t cta = 0;
+  for (int b = 0; b < kBins; ++b) {
+    D.bin_off[b] = off;
+    D.cta0[b] = cta;
+    int64_t R = (int64_t)bins[b].size();
+    off += R;
+    perm.insert(perm.end(), bins[b].begin(), bins[b].end());
+    if (R == 0) continue;
+    if (b < kBins - 1) {
+      int64_t rows_per_cta = kThreads >> b;
+      cta += (int32_t)std::min<int64_t>((R + rows_per_cta - 1) / rows_per_cta, 148 * 16);
+    } else {
+      cta += (int32_t)std::min<int64_t>(R, 148 * 8);
+    }
+  }
+  D.bin_off[kBins] = off;
+  D.cta0[kBins] = std::max(cta, 1);
+  int32_t* d_perm = A.alloc<int32_t>(perm.size());
+  if (!perm.empty())
+    PDCS_CUDA(cudaMemcpyAsync(d_perm, perm.data(), perm.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s_));
+  D.perm = d_perm;
+}
+
+void Solver::size_table(ConeTable& T) {
+  T.elem_total = 0;
+  for (int s = 0; s < T.nseg; ++s) T.elem_total += T.seg_len[s];
+  auto cap = [](int64_t v) { return (int32_t)std::min<int64_t>(v, 148 * 8); };
+  T.ctaA = T.elem_total > 0 ? cap((T.elem_total + kThreads - 1) / kThreads) : 0;
+  T.ctaB = T.nwc > 0 ? cap((T.nwc + kWarps - 1) / kWarps) : 0;
+  int64_t ne = T.exp_count + T.dexp_count;
+  T.ctaC = ne > 0 ? cap((ne + kThreads - 1) / kThreads) : 0;
+  if (T.ctaA + T.ctaB + T.ctaC == 0) T.ctaA = 1;  // at least one CTA writes the partials
+}
+
+void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<int64_t>& rsoc_x,
+                          const std::vector<int64_t>& socG, const std::vector<int64_t>& rsocG) {
+  // warp-cone lists (shared by the iteration and KKT tables of each vector)
+  auto upload_wc = [&](const std::vector<int64_t>& soc, const std::vector<int64_t>& rsoc, int64_t start0,
+                       int64_t*& d_start, int32_t*& d_len, int8_t*& d_kind) {
+    std::vector<int64_t> stv;
+    std::vector<int32_t> lv;
+    std::vector<int8_t> kv;
+    int64_t s = start0;
+    for (int64_t d : soc) { stv.push_back(s); lv.push_back((int32_t)d); kv.push_back(PK_SOC); s += d; }
+    for (int64_t d : rsoc) { stv.push_back(s); lv.push_back((int32_t)d); kv.push_back(PK_RSOC); s += d; }
+    d_start = A.alloc<int64_t>(stv.size());
+    d_len = A.alloc<int32_t>(lv.size());
+    d_kind = A.alloc<int8_t>(kv.size());
+    if (!stv.empty()) {
+      PDCS_CUDA(cudaMemcpyAsync(d_start, stv.data(), stv.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s_));
+      PDCS_CUDA(cudaMemcpyAsync(d_len, lv.data(), lv.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s_));
+      PDCS_CUDA(cudaMemcpyAsync(d_kind, kv.data(), kv.size() * sizeof(int8_t), cudaMemcpyHostToDevice, s_));
+      PDCS_CUDA(cudaStreamSynchronize(s_));
+    }
+    return s;
+  };
+  int64_t *xs = nullptr, *ys = nullptr;
+  int32_t *xlen = nullptr, *ylen = nullptr;
+  int8_t *xk = nullptr, *yk = nullptr;
+  int64_t xe = upload_wc(soc_x, rsoc_x, nb_, xs, xlen, xk);
+  int64_t ye = upload_wc(socG, rsocG, P.mGzero + P.mGnonnegative, ys, ylen, yk);
+  ConeTable base_x{};
+  base_x.len = n_;
+  base_x.nwc = (int64_t)(soc_x.size() + rsoc_x.size());
+  base_x.wc_start = xs;
+  base_x.wc_len = xlen;
+  base_x.wc_kind = xk;
+  base_x.exp_base = xe;
+  base_x.exp_count = P.exp_x;
+  base_x.dexp_base = xe + 3 * P.exp_x;
+  base_x.dexp_count = P.dual_exp_x;
+  if (nb_ > 0) {
+    base_x.nseg = 1;
+    base_x.seg_start[0] = 0;
+    base_x.seg_len[0] = nb_;
+    base_x.seg_kind[0] = PK_BOX;
+  }
+  XI = base_x;
+  XI.lo = bl_s;
+  XI.hi = bu_s;
+  XI.exp_kind = PK_EXP;    // code 27
+  XI.dexp_kind = PK_DEXP;  // code 29
+  XI.S = Dr;
+  SLK = base_x;
+  SLK.lo = lam_l;
+  SLK.hi = lam_u;
+  SLK.exp_kind = PK_DEXP;  // code 28
+  SLK.dexp_kind = PK_EXP;  // code 26
+  SLK.S = nullptr;
+  ConeTable base_y{};
+  base_y.len = m_;
+  base_y.nwc = (int64_t)(socG.size() + rsocG.size());
+  base_y.wc_start = ys;
+  base_y.wc_len = ylen;
+  base_y.wc_kind = yk;
+  base_y.exp_base = ye;
+  base_y.exp_count = P.expG;
+  base_y.dexp_base = ye + 3 * P.expG;
+  base_y.dexp_count = P.dual_expG;
+  int ns = 0;
+  if (P.mGzero > 0) {
+    base_y.seg_start[ns] = 0;
+    base_y.seg_len[ns] = P.mGzero;
+    ns++;
+  }
+  if (P.mGnonnegative > 0) {
+    base_y.seg_start[ns] = P.mGzero;
+    base_y.seg_len[ns] = P.mGnonnegative;
+    base_y.seg_kind[ns] = PK_NONNEG;
+    ns++;
+  }
+  base_y.nseg = ns;
+  YI = base_y;
+  CON = base_y;
+  if (P.mGzero > 0) {
+    YI.seg_kind[0] = PK_FREE;   // code 1
+    CON.seg_kind[0] = PK_ZERO;  // code 2
+  }
+  YI.exp_kind = PK_DEXP;   // code 12: y in Dl o K_exp^*
+  YI.dexp_kind = PK_EXP;   // code 15
+  YI.S = Dl;
+  CON.exp_kind = PK_EXP;   // code 13
+  CON.dexp_kind = PK_DEXP; // code 16
+  CON.S = nullptr;
+  size_table(XI);
+  size_table(SLK);
+  size_table(YI);
+  size_table(CON);
+}
+
+void Solver::setup() {
+  n_ = P.n;
+  m_ = P.m;
+  nb_ = P.nb;
+  nnz_ = P.nnz;
+  if (O.stream) {
+    s_ = static_cast<cudaStream_t>(O.stream);
+  } else {
+    PDCS_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    own_stream_ = true;
+  }
+  PDCS_CUDA(cudaMallocHost(&host_state_, sizeof(PdhgState)));
+  PDCS_CUDA(cudaMallocHost(&host_red_, 16 * sizeof(double)));
+  // ---- host copies of the problem ----
+  HostCsr H;
+  H.m = m_;
+  H.n = n_;
+  H.rp.resize(m_ + 1);
+  H.ci.resize(nnz_);
+  H.v.resize(nnz_);
+  std::vector<double> c(n_), h(m_), bl(nb_), bu(nb_);
+  auto get = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return;
+    if (P.on_device) PDCS_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+    else std::memcpy(dst, src, bytes);
+  };
+  get(H.rp.data(), P.G_rowptr, sizeof(int32_t) * (m_ + 1));
+  get(H.ci.data(), P.G_colind, sizeof(int32_t) * nnz_);
+  get(H.v.data(), P.G_val, sizeof(double) * nnz_);
+  get(c.data(), P.c, sizeof(double) * n_);
+  get(h.data(), P.h, sizeof(double) * m_);
+  get(bl.data(), P.bl, sizeof(double) * nb_);
+  get(bu.data(), P.bu, sizeof(double) * nb_);
+  if (H.rp[0] != 0 || H.rp[m_] != nnz_) throw std::invalid_argument("rowptr");
+  for (int64_t j = 0; j < nb_; ++j)
+    if (!(bl[j] <= bu[j])) throw std::domain_error("bounds");
+  for (int64_t k = 0; k < nnz_; ++k)
+    if (H.ci[k] < 0 || H.ci[k] >= n_) throw std::invalid_argument("colind");
+  // raw norms (cal_constant, def_struct.jl:968-976)
+  for (double v : h) { hNrm1 += std::fabs(v); hNrmInf = std::max(hNrmInf, std::fabs(v)); }
+  for (double v : c) { cNrm1 += std::fabs(v); cNrmInf = std::max(cNrmInf, std::fabs(v)); }
+  std::vector<double> c_raw_h = c, h_raw_h = h, bl_fin_h(nb_), bu_fin_h(nb_), lam_l_h(nb_), lam_u_h(nb_);
+  const double inf = INFINITY;
+  for (int64_t j = 0; j < nb_; ++j) {
+    bl_fin_h[j] = std::isinf(bl[j]) ? 0.0 : bl[j];
+    bu_fin_h[j] = std::isinf(bu[j]) ? 0.0 : bu[j];
+    lam_l_h[j] = (bu[j] == inf) ? 0.0 : -inf;  // gen_lambd, def_rpdhg_gen.jl:5-17
+    lam_u_h[j] = (bl[j] == -inf) ? 0.0 : inf;
+  }
+  // ---- Ruiz (10) + Pock-Chambolle (alpha = 1) equilibration (preprocess.jl:347-591) ----
+  std::vector<double> Drh(n_, 1.0), Dlh(m_, 1.0);
+  auto scale_data = [&](const std::vector<double>& var, const std::vector<double>& con) {
+    for (int64_t j = 0; j < n_; ++j) { c[j] /= var[j]; Drh[j] *= var[j]; }
+    for (int64_t j = 0; j < nb_; ++j) { bl[j] *= var[j]; bu[j] *= var[j]; }
+    for (int64_t i = 0; i < m_; ++i) {
+      h[i] /= con[i];
+      Dlh[i] *= con[i];
+      for (int32_t k = H.rp[i]; k < H.rp[i + 1]; ++k) H.v[k] /= (con[i] * var[H.ci[k]]);
+    }
+  };
+  int method = O.rescaling_method;
+  if (method == 1 || method == 3) {
+    for (int it = 0; it < 10; ++it) {
+      std::vector<double> var(n_, 0.0), con(m_, 0.0);
+      for (int64_t i = 0; i < m_; ++i)
+        for (int32_t k = H.rp[i]; k < H.rp[i + 1]; ++k) {
+          double a = std::fabs(H.v[k]);
+          con[i] = std::max(con[i], a);
+          var[H.ci[k]] = std::max(var[H.ci[k]], a);
+        }
+      for (auto& v : var) v = (v == 0.0) ? 1.0 : std::sqrt(v);
+      for (auto& v : con) v = (v == 0.0) ? 1.0 : std::sqrt(v);
+      scale_data(var, con);
+    }
+  }
+  if (method == 2 || method == 3) {
+    std::vector<double> var(n_, 0.0), con(m_, 0.0);
+    for (int64_t i = 0; i < m_; ++i)
+      for (int32_t k = H.rp[i]; k < H.rp[i + 1]; ++k) {
+        double a = std::fabs(H.v[k]);
+        con[i] += a;
+        var[H.ci[k]] += a;
+      }
+    for (auto& v : var) v = (v == 0.0) ? 1.0 : std::sqrt(v);
+    for (auto& v : con) v = (v == 0.0) ? 1.0 : std::sqrt(v);
+    scale_data(var, con);
+  }
+  ginf_ = 0.0;
+  for (double v : H.v) ginf_ = std::max(ginf_, std::fabs(v));
+  HostCsr Ht = transpose(H);
+  // ---- upload ----
+  auto up = [&](auto* dst, const auto& vec) {
+    if (!vec.empty())
+      PDCS_CUDA(cudaMemcpyAsync(dst, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice, s_));
+  };
+  int32_t* g_rp = A.alloc<int32_t>(m_ + 1);
+  int32_t* g_ci = A.alloc<int32_t>(nnz_);
+  double* g_v = A.alloc<double>(nnz_);
+  int32_t* t_rp = A.alloc<int32_t>(n_ + 1);
+  int32_t* t_ci = A.alloc<int32_t>(nnz_);
+  double* t_v = A.alloc<double>(nnz_);
+  up(g_rp, H.rp);
+  up(g_ci, H.ci);
+  up(g_v, H.v);
+  up(t_rp, Ht.rp);
+  up(t_ci, Ht.ci);
+  up(t_v, Ht.v);
+  build_bins(H, g_rp, g_ci, g_v, G_);
+  build_bins(Ht, t_rp, t_ci, t_v, Gt_);
+  auto vecn = [&]() { return A.alloc<double>(n_); };
+  auto vecm = [&]() { return A.alloc<double>(m_); };
+  c_s = vecn(); c_raw = vecn(); Dr = vecn();
+  h_s = vecm(); h_raw = vecm(); Dl = vecm();
+  bl_s = A.alloc<double>(nb_); bu_s = A.alloc<double>(nb_);
+  lam_l = A.alloc<double>(nb_); lam_u = A.alloc<double>(nb_);
+  bl_fin = A.alloc<double>(nb_); bu_fin = A.alloc<double>(nb_);
+  up(c_s, c); up(c_raw, c_raw_h); up(Dr, Drh);
+  up(h_s, h); up(h_raw, h_raw_h); up(Dl, Dlh);
+  up(bl_s, bl); up(bu_s, bu); up(lam_l, lam_l_h); up(lam_u, lam_u_h); up(bl_fin, bl_fin_h); up(bu_fin, bu_fin_h);
+  x = vecn(); xl = vecn(); xm = vecn(); aty = vecn(); x0 = vecn(); x0l = vecn(); xbest = vecn();
+  y = vecm(); yl = vecm(); ym = vecm(); gx = vecm(); gxl = vecm(); y0 = vecm(); y0l = vecm(); ybest = vecm();
+  for (int k = 0; k < 6; ++k) { tn[k] = vecn(); tm[k] = vecm(); }
+  xds_ = vecn();
+  yds_ = vecm();
+  // initial point (zeros, or the scaled warm start)
+  std::vector<double> x_init(n_, 0.0), y_init(m_, 0.0);
+  if (O.warm_start && O.primal_sol && O.dual_sol) {
+    for (int64_t j = 0; j < n_; ++j) x_init[j] = O.primal_sol[j] * Drh[j];
+    for (int64_t i = 0; i < m_; ++i) y_init[i] = O.dual_sol[i] * Dlh[i];
+  }
+  up(x, x_init); up(y, y_init);
+  copy(xl, x, n_); copy(xm, x, n_); copy(xbest, x, n_);
+  copy(yl, y, m_); copy(ym, y, m_); copy(ybest, y, m_);
+  // cone tables
+  std::vector<int64_t> soc_x(P.soc_x, P.soc_x + P.n_soc_x), rsoc_x(P.rsoc_x, P.rsoc_x + P.n_rsoc_x);
+  std::vector<int64_t> socG(P.socG, P.socG + P.n_socG), rsocG(P.rsocG, P.rsocG + P.n_rsocG);
+  build_tables(soc_x, rsoc_x, socG, rsocG);
+  int maxgrid = std::max({XI.ctaA + XI.ctaB + XI.ctaC, YI.ctaA + YI.ctaB + YI.ctaC, SLK.ctaA + SLK.ctaB + SLK.ctaC,
+                          CON.ctaA + CON.ctaB + CON.ctaC, 148 * 8});
+  part_x = A.alloc<double>((size_t)maxgrid * 8);
+  part_y = A.alloc<double>((size_t)maxgrid * 8);
+  part_r = A.alloc<double>((size_t)maxgrid * 8);
+  red_out = A.alloc<double>(16);
+  st_dev = A.alloc<PdhgState>(1);
+  grid_reflect_ = grid_for(std::max(n_, m_));
+  attempts_per_graph_ = O.attempts_per_graph > 0 ? O.attempts_per_graph : 32;
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+}
+
+void Solver::capture_graph() {
+  PDCS_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+  const int32_t* act = &st_dev->active;
+  for (int a = 0; a < attempts_per_graph_; ++a) {
+    spmv_binned_kernel<1><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, yl, nullptr, aty, nullptr, act);
+    OpPrimalStep op1{xl, aty, c_s, x, st_dev, 0.0};
+    update_project_kernel<OpPrimalStep><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, act);
+    spmv_binned_kernel<2><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, x, xl, gx, gxl, act);
+    OpDualStep op2{yl, gx, gxl, h_s, y, st_dev, 0.0};
+    update_project_kernel<OpDualStep><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, act);
+    control_kernel<<<1, kThreads, 0, s_>>>(st_dev, part_x, XI.ctaA + XI.ctaB + XI.ctaC, part_y,
+                                           YI.ctaA + YI.ctaB + YI.ctaC);
+    reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, x, xl, xm, n_, y, yl, ym, m_);
+  }
+  PDCS_CUDA(cudaStreamEndCapture(s_, &graph_));
+  PDCS_CUDA(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+}
+
+// converge_info_calculation_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:126-183), on
+// the scaled iterates: G_raw x_raw = Dl o (G~ x~),  G_raw' y_raw = Dr o (G~' y~).
+void Solver::converge_info(const double* xs, const double* ys, Converge& C, double* gxs, double* atys) {
+  spmv(G_, xs, gxs);
+  spmv(Gt_, ys, atys);
+  double rp[7], rd[7];
+  OpResidual opp{gxs, Dl, 1.0, nullptr, 0.0, h_raw, tm[5], bl_fin, bu_fin, 0};
+  update_project(opp, CON, part_r);
+  finalize(part_r, CON.ctaA + CON.ctaB + CON.ctaC, 7, 0b0010110u, rp);
+  OpResidual opd{atys, Dr, -1.0, c_raw, 1.0, nullptr, tn[5], bl_fin, bu_fin, nb_};
+  update_project(opd, SLK, part_r);
+  finalize(part_r, SLK.ctaA + SLK.ctaB + SLK.ctaC, 7, 0b0010110u, rd);
+  DotSpec d1{};
+  d1.a[0] = c_raw; d1.b[0] = xs; d1.sa[0] = Dr; d1.kind[0] = DK_DOT;  // c'(x~/Dr), divisor applies to a
+  d1.count = 1;
+  d1.len = n_;
+  double pobj;
+  dots(d1, &pobj);
+  // c_raw_j * x_j / Dr_j : the divisor is on a, a = c_raw, so (c_raw/Dr)*x~ -- same value
+  DotSpec d2{};
+  d2.a[0] = h_raw; d2.b[0] = ys; d2.sa[0] = Dl; d2.kind[0] = DK_DOT;
+  d2.count = 1;
+  d2.len = m_;
+  double hy;
+  dots(d2, &hy);
+  double dobj = hy + rd[6];
+  C.pobj = pobj;
+  C.dobj = dobj;
+  C.abs_gap = std::fabs(pobj - dobj);
+  C.rel_gap = C.abs_gap / (1.0 + std::max(std::fabs(pobj), std::fabs(dobj)));
+  double l2p = std::sqrt(rp[0]), linfp = rp[1], axinf = rp[4], axnrm1 = rp[5];
+  double l2d = std::sqrt(rd[0]), linfd = rd[1], sinf = rd[2], snrm1 = rd[3], atyinf = rd[4], atynrm1 = rd[5];
+  C.l2_abs_p = l2p;
+  C.linf_abs_p = linfp;
+  C.l2_abs_d = l2d;
+  C.linf_abs_d = linfd;
+  C.l2_rel_p = l2p / (1.0 + std::max(snrm1, std::max(hNrm1, axnrm1)));
+  C.linf_rel_p = linfp / (1.0 + std::max(sinf, std::max(hNrmInf, axinf)));
+  C.l2_rel_d = l2d / (1.0 + std::max(cNrm1, atynrm1));
+  C.linf_rel_d = linfd / (1.0 + std::max(cNrmInf, atyinf));
+}
+
+// exit_condition_check_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:309-352)
+void Solver::exit_check() {
+  double *gxc = tm[0], *gxm = tm[1], *atc = tn[0], *atm = tn[1];
+  converge_info(x, y, ci[0], gxc, atc);
+  converge_info(xm, ym, ci[1], gxm, atm);
+  check_count_++;
+  // infeasibility information (rpdhg_alg_gpu_gen_scaling.jl:185-248).  For the
+  // current iterate the rays are the iterates themselves, so the ray
+  // infeasibilities equal the residuals just computed.
+  auto ray_norms = [&](const double* xr, const double* yr, Infea& I) {
+    DotSpec a{};
+    a.a[0] = xr; a.sa[0] = Dr; a.kind[0] = DK_MAXABS;
+    a.count = 1; a.len = n_;
+    dots(a, &I.primal_ray_norm);
+    DotSpec b{};
+    b.a[0] = yr; b.sa[0] = Dl; b.kind[0] = DK_MAXABS;
+    b.count = 1; b.len = m_;
+    dots(b, &I.dual_ray_norm);
+  };
+  auto push_trend = [&](Infea& I) {
+    if (check_count_ % 4 == 1) {  // the reference pushes with probability 1/4
+      I.ptrend.push_back(ci[0].pobj);
+      I.dtrend.push_back(ci[0].dobj);
+      if (I.ptrend.size() > 20) I.ptrend.erase(I.ptrend.begin());
+      if (I.dtrend.size() > 20) I.dtrend.erase(I.dtrend.begin());
+    }
+  };
+  {
+    Infea& I = ii[0];
+    I.primal_ray_obj = ci[0].pobj;
+    I.dual_ray_obj = ci[0].dobj;
+    I.max_primal_ray_inf = (ci[0].pobj < 0.0) ? ci[0].linf_abs_p : 1e10;
+    I.max_dual_ray_inf = (ci[0].dobj > 0.0) ? ci[0].linf_abs_d : 1e10;
+    ray_norms(x, y, I);
+    push_trend(I);
+  }
+  {
+    // ray = current - average
+    Infea& I = ii[1];
+    double* dxs = tn[2];
+    double* dys = tm[2];
+    axpby(dxs, 1.0, x, -1.0, xm, n_);
+    axpby(dys, 1.0, y, -1.0, ym, m_);
+    double* gd = tm[3];
+    double* ad = tn[3];
+    axpby(gd, 1.0, gxc, -1.0, gxm, m_);
+    axpby(ad, 1.0, atc, -1.0, atm, n_);
+    DotSpec d1{};
+    d1.a[0] = c_raw; d1.b[0] = dxs; d1.sa[0] = Dr; d1.kind[0] = DK_DOT;
+    d1.count = 1; d1.len = n_;
+    double pobj;
+    dots(d1, &pobj);
+    double rp[7], rd[7];
+    I.max_primal_ray_inf = 1e10;
+    if (pobj < 0.0) {
+      OpResidual opp{gd, Dl, 1.0, nullptr, 0.0, h_raw, tm[5], bl_fin, bu_fin, 0};
+      update_project(opp, CON, part_r);
+      finalize(part_r, CON.ctaA + CON.ctaB + CON.ctaC, 7, 0b0010110u, rp);
+      I.max_primal_ray_inf = rp[1];
+    }
+    DotSpec d2{};
+    d2.a[0] = h_raw; d2.b[0] = dys; d2.sa[0] = Dl; d2.kind[0] = DK_DOT;
+    d2.count = 1; d2.len = m_;
+    double hy;
+    dots(d2, &hy);
+    OpResidual opd{ad, Dr, -1.0, c_raw, 1.0, nullptr, tn[5], bl_fin, bu_fin, nb_};
+    update_project(opd, SLK, part_r);
+    finalize(part_r, SLK.ctaA + SLK.ctaB + SLK.ctaC, 7, 0b0010110u, rd);
+    double dobj = hy + rd[6];
+    I.max_dual_ray_inf = (dobj > 0.0) ? rd[1] : 1e10;
+    I.primal_ray_obj = pobj;
+    I.dual_ray_obj = dobj;
+    ray_norms(dxs, dys, I);
+    push_trend(I);
+  }
+  check_termination();
+}
+
+// check_termination_criteria (src/pdcs_gpu/termination.jl:74-260)
+void Solver::check_termination() {
+  auto mono = [](const std::vector<double>& b, bool inc) {
+    if (b.size() < 20) return false;
+    for (size_t i = 1; i < 20; ++i)
+      if (inc ? (b[i] < b[i - 1]) : (b[i] > b[i - 1])) return false;
+    return true;
+  };
+  for (int k = 0; k < 2; ++k) {
+    Converge& C = ci[k];
+    if (std::max(C.linf_rel_p, std::max(C.linf_rel_d, C.rel_gap)) < O.rel_tol) C.status = PDCS_EXIT_OPTIMAL;
+    if (std::max(C.linf_abs_p, std::max(C.linf_abs_d, C.abs_gap)) < O.abs_tol) C.status = PDCS_EXIT_OPTIMAL;
+    if (std::isnan(C.rel_gap)) C.status = PDCS_EXIT_NUMERICAL_NAN;
+    if (std::isinf(C.rel_gap)) C.status = PDCS_EXIT_NUMERICAL_INF;
+    if (C.status == PDCS_EXIT_OPTIMAL) {
+      exit_code_ = PDCS_EXIT_OPTIMAL;
+      pobj_ = C.pobj;
+      dobj_ = C.dobj;
+      returned_seq_ = k;
+      return;
+    }
+    if (C.status == PDCS_EXIT_NUMERICAL_NAN || C.status == PDCS_EXIT_NUMERICAL_INF) {
+      exit_code_ = C.status;
+      return;
+    }
+  }
+  for (int k = 0; k < 2; ++k) {
+    Infea& I = ii[k];
+    if (I.dual_ray_obj > 0.0) {
+      if ((I.dual_ray_obj - I.primal_ray_obj) / (1 + std::fabs(I.dual_ray_obj) + std::fabs(I.primal_ray_obj)) > 0.99999 &&
+          I.max_primal_ray_inf > 1e3 && mono(I.dtrend, true) && I.max_dual_ray_inf > 1e4 && I.dual_ray_obj > 1e14 &&
+          I.dual_ray_norm > 1e8)
+        I.status = PDCS_EXIT_PRIMAL_INFEASIBLE_LOW_ACC;
+      double res = std::max(I.max_dual_ray_inf, 1.0) / I.dual_ray_obj;
+      if (res <= O.eps_primal_infeasible_low_acc) {
+        if (res <= O.eps_primal_infeasible_high_acc) I.status = PDCS_EXIT_PRIMAL_INFEASIBLE_HIGH_ACC;
+        if (I.max_dual_ray_inf > 1e8) I.status = PDCS_EXIT_PRIMAL_INFEASIBLE_LOW_ACC;
+        if (mono(I.dtrend, true)) I.status = PDCS_EXIT_PRIMAL_INFEASIBLE_LOW_ACC;
+      }
+    }
+    if ((I.status == 2 && S.iter > 2000) || (I.status == 3 && S.iter > 500)) {
+      exit_code_ = I.status;
+      pobj_ = I.primal_ray_obj;
+      dobj_ = I.dual_ray_obj;
+      return;
+    }
+    if (I.primal_ray_obj < 0.0) {
+      if ((I.primal_ray_obj - I.dual_ray_obj) / (1 + std::fabs(I.primal_ray_obj) + std::fabs(I.dual_ray_obj)) > 0.99999 &&
+          I.max_dual_ray_inf > 1e3 && mono(I.ptrend, false) && I.max_primal_ray_inf > 1e4 &&
+          -I.primal_ray_obj > 1e14 && I.primal_ray_norm > 1e8)
+        I.status = PDCS_EXIT_DUAL_INFEASIBLE_LOW_ACC;
+      double res = std::max(I.max_primal_ray_inf, 1.0) / (-I.primal_ray_obj);
+      if (res <= O.eps_dual_infeasible_low_acc) {
+        if (res <= O.eps_dual_infeasible_high_acc) I.status = PDCS_EXIT_DUAL_INFEASIBLE_HIGH_ACC;
+        if (I.max_primal_ray_inf > 1e8) I.status = PDCS_EXIT_DUAL_INFEASIBLE_LOW_ACC;
+        if (mono(I.ptrend, false)) I.status = PDCS_EXIT_DUAL_INFEASIBLE_LOW_ACC;
+      }
+    }
+    if ((I.status == 4 && S.iter > 2000) || (I.status == 5 && S.iter > 500)) {
+      exit_code_ = I.status;
+      pobj_ = I.primal_ray_obj;
+      dobj_ = I.dual_ray_obj;
+      return;
+    }
+  }
+  if ((double)S.iter >= (double)O.max_outer_iter * (double)O.max_inner_iter) {
+    exit_code_ = PDCS_EXIT_MAX_ITER;
+    pobj_ = ci[0].pobj;
+    dobj_ = ci[0].dobj;
+    return;
+  }
+  if (O.time_limit > 0 && now_s() - t_start_ > O.time_limit) {
+    exit_code_ = PDCS_EXIT_TIME_LIMIT;
+    return;
+  }
+  exit_code_ = PDCS_EXIT_CONTINUE;
+}
+
+// Mnorm (rpdhg_alg_gpu_gen.jl:133-138)
+double Solver::mnorm(const double* dx, const double* dy, double ta, double si) {
+  double* gdx = tm[4];
+  spmv(G_, dx, gdx);
+  DotSpec d{};
+  d.a[0] = dy; d.b[0] = gdx; d.kind[0] = DK_DOT;
+  d.count = 1; d.len = m_;
+  double ygx;
+  dots(d, &ygx);
+  DotSpec e{};
+  e.a[0] = dx; e.kind[0] = DK_DOT;
+  e.count = 1; e.len = n_;
+  double xx;
+  dots(e, &xx);
+  DotSpec f{};
+  f.a[0] = dy; f.kind[0] = DK_DOT;
+  f.count = 1; f.len = m_;
+  double yy;
+  dots(f, &yy);
+  return xx / ta - 2.0 * ygx + yy / si;
+}
+
+// binary_search_duality_gap_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:20-117);
+// the doubling loop's `tRight = t, tLeft = t / 2, break` parses as
+// `tRight = ((t, tLeft) = (t / 2, break))`, i.e. a plain break.
+double Solver::binary_search(double r, const double* px, const double* py, double ta, double si) {
+  double* h1 = tn[2];
+  double* h2 = tm[2];
+  double* xs = tn[3];
+  double* ys = tm[3];
+  double* gpx = tm[1];
+  double* gxs = tm[4];
+  spmv(Gt_, py, h1);
+  axpby(h1, 1.0, h1, -1.0, c_s, n_);
+  spmv(G_, px, gpx);
+  axpby(h2, -1.0, gpx, 1.0, h_s, m_);
+  double last_h1dx = 0.0, last_h2dy = 0.0;
+  auto approx = [&](double t) {
+    OpAxpyProj ox{px, h1, t * ta / 2, xs, nullptr, nullptr};
+    update_project(ox, XI, part_r);
+    double rx[3];
+    finalize(part_r, XI.ctaA + XI.ctaB + XI.ctaC, 3, 0u, rx);
+    spmv(G_, xs, gxs);
+    OpAxpyProj oy{py, h2, t * si / 2, ys, gxs, gpx};
+    update_project(oy, YI, part_r);
+    double ry[3];
+    finalize(part_r, YI.ctaA + YI.ctaB + YI.ctaC, 3, 0u, ry);
+    last_h1dx = rx[1];
+    last_h2dy = ry[1];
+    return rx[0] / ta - 2.0 * ry[2] + ry[0] / si;
+  };
+  double t = bs_t0_, tR = t, tL = 0.0;
+  for (int k = 1; k <= 1000; ++k) {
+    double val = approx(t);
+    if (val > r && val < r + 1e-6) {
+      tR = t;
+      tL = std::max(t - 0.01, 0.0);
+      val = approx(tL);
+      if (val < r) break;
+    }
+    if (val < r && val > r - 1e-6) {
+      tL = t;
+      tR = t + 0.01;
+      val = approx(tR);
+      if (val > r) break;
+    }
+    if (val > r) break;
+    t *= 2;
+  }
+  double tM = 0.5 * (tR + tL);
+  int64_t count = 0;
+  while (tR - tL > 1e-6) {
+    tM = 0.5 * (tR + tL);
+    if (approx(tM) < r) tL = tM; else tR = tM;
+    if (++count > 1000000) break;
+  }
+  bs_t0_ = tM;
+  return (last_h1dx + last_h2dy) / r;
+}
+
+// restart_threshold_calculation_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:354-393)
+void Solver::restart_threshold(bool dgap) {
+  if (dgap) {
+    double* dx = tn[4];
+    double* dy = tm[5];
+    axpby(dx, 1.0, x0, -1.0, x0l, n_);
+    axpby(dy, 1.0, y0, -1.0, y0l, m_);
+    double r = mnorm(dx, dy, S.tau, S.sigma);
+    ndg_r_ = r;
+    ndg_thr_ = binary_search(r, x0, y0, S.tau, S.sigma);
+    if (ndg_thr_ < 0) dgap_flag_ = false;
+  } else {
+    converge_info(x, y, ci[0], tm[0], tn[0]);
+    kkt_thr_ = kkt_error(ci[0]);
+  }
+}
+
+// restart_condition_check_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:395-506)
+bool Solver::restart_check(bool dgap) {
+  auto to_current = [&]() {
+    copy(xm, x, n_);
+    copy(ym, y, m_);
+  };
+  if (dgap) {
+    double* dx = tn[4];
+    double* dy = tm[5];
+    axpby(dx, 1.0, x, -1.0, x0, n_);
+    axpby(dy, 1.0, y, -1.0, y0, m_);
+    double rl = mnorm(dx, dy, S.tau, S.sigma);
+    double rho = binary_search(rl, x, y, S.tau, S.sigma);
+    double rho_m = binary_search(rl, xm, ym, S.tau, S.sigma);
+    ndg_[0] = rho;
+    ndg_[1] = rho_m;
+    for (double beta : {0.4, 0.8}) {
+      if (rho < beta * ndg_thr_ || rho_m < beta * ndg_thr_) {
+        restart_used_++;
+        if (ndg_[0] < ndg_[1] && dgap_flag_) to_current();
+        return true;
+      }
+    }
+  } else {
+    converge_info(x, y, ci[0], tm[0], tn[0]);
+    converge_info(xm, ym, ci[1], tm[1], tn[1]);
+    double lag0 = kkt_err_[0], lag1 = kkt_err_[1];
+    double e0 = kkt_error(ci[0]), e1 = kkt_error(ci[1]);
+    kkt_err_[0] = e0;
+    kkt_err_[1] = e1;
+    bool c1 = e0 < 0.4 * kkt_thr_ || e1 < 0.4 * kkt_thr_;
+    bool c2 = (e0 < 0.8 * kkt_thr_ && e0 > lag0) || (e1 < 0.8 * kkt_thr_ && e1 > lag1);
+    if (c1 || c2) {
+      restart_used_++;
+      if (kkt_err_[0] < kkt_err_[1]) to_current();
+      return true;
+    }
+  }
+  if ((double)S.inner >= (double)S.iter * 0.223 && S.iter > 100000) {
+    restart_used_++;
+    return true;
+  }
+  return false;
+}
+
+void Solver::run_until_halt() {
+  push_state();
+  if (!graph_exec_) capture_graph();
+  while (true) {
+    int64_t to_check = S.check_freq > 0 ? S.check_freq - (S.iter % S.check_freq) : 1 << 20;
+    int64_t graphs = (to_check + attempts_per_graph_ - 1) / attempts_per_graph_;
+    graphs = std::max<int64_t>(1, std::min<int64_t>(graphs, 4));
+    for (int64_t g = 0; g < graphs; ++g) {
+      PDCS_CUDA(cudaGraphLaunch(graph_exec_, s_));
+      graphs_++;
+      kernels_ += 6LL * attempts_per_graph_;
+    }
+    pull_state();
+    if (!S.active) return;
+    if (O.time_limit > 0 && now_s() - t_start_ > O.time_limit) return;
+  }
+}
+
+void Solver::log_progress() {
+  if (!O.verbose) return;
+  std::printf("[pdcs_b200] iter %lld rel_p %.3e rel_d %.3e gap %.3e pobj %.8e dobj %.8e restarts %lld time %.3f\n",
+              (long long)S.iter, ci[0].linf_rel_p, ci[0].linf_rel_d, ci[0].rel_gap, ci[0].pobj, ci[0].dobj,
+              (long long)restart_used_, now_s() - t_start_);
+}
+
+// pdhg_main_iter_average_diagonal_rescaling_restarts_adaptive_weight_resolving_aggressive!
+// (rpdhg_alg_gpu_gen_scaling.jl:770-895)
+void Solver::main_loop() {
+  copy(x0, x, n_);
+  copy(y0, y, m_);
+  copy(x0l, x, n_);
+  copy(y0l, y, m_);
+  S = PdhgState{};
+  S.omega = init_omega();
+  S.eta_p = 1.0 / ginf_;
+  S.tau = 0.9;
+  S.sigma = 0.9;
+  S.check_freq = O.check_terminate_freq;
+  S.attempt_limit = O.attempt_limit;
+  // one restart frequency drives the device halt; both restart tests run on the host
+  int64_t rf = 0;
+  if (O.use_duality_gap_restart) rf = O.duality_gap_restart_freq;
+  if (O.use_kkt_restart) rf = rf ? std::min(rf, O.kkt_restart_freq) : O.kkt_restart_freq;
+  S.restart_freq = rf;
+  S.restart_enabled = rf > 0;
+  for (int64_t outer = 1; outer <= O.max_outer_iter; ++outer) {
+    // update_best_sol! (:640-649)
+    if (ci[0].l2_rel_p < pres_best_) { pres_best_ = ci[0].l2_rel_p; copy(xbest, x, n_); }
+    if (ci[0].l2_rel_d < dres_best_) { dres_best_ = ci[0].l2_rel_d; copy(ybest, y, m_); }
+    max_kkt_ = std::max(std::max(ci[0].l2_rel_p, ci[0].l2_rel_d), ci[0].rel_gap);
+    min_kkt_ = std::min(std::min(std::min(ci[0].l2_rel_p, ci[0].l2_rel_d), ci[0].rel_gap), min_kkt_);
+    double extra = -0.1 * std::log10(max_kkt_) + 0.2;
+    copy(x0l, x0, n_);
+    copy(y0l, y0, m_);
+    copy(x0, xm, n_);
+    copy(y0, ym, m_);
+    copy(x, xm, n_);
+    copy(y, ym, m_);
+    if (O.use_kkt_restart) restart_threshold(false);
+    else restart_threshold(dgap_flag_);
+    // resolving triggers (:810-838) are evaluated; the pessimistic resolving
+    // loop itself is not part of this build (reported via verbose output)
+    if (O.verbose) {
+      double pd = ci[0].l2_rel_p / ci[0].l2_rel_d;
+      bool f1 = outer > 10 && max_kkt_ > 1e5, f2 = outer > 80 && (pd > 1e10 || pd < 1e-10),
+           f3 = outer > 10 && S.tau < 1e-6 && S.sigma < 1e-6;
+      if (f1 || f2 || f3) std::printf("[pdcs_b200] resolving trigger at outer %lld\n", (long long)outer);
+    }
+    double* xds = xds_;
+    double* yds = yds_;
+    copy(xl, x, n_);
+    copy(yl, y, m_);
+    copy(xds, x, n_);
+    copy(yds, y, m_);
+    // start of the inner loop (:839-842) and of the first step call (:667, :676)
+    S.inner = 0;
+    S.eta_cum = 0.0;
+    S.extra = extra;
+    S.dec = decay(max_kkt_);
+    S.dec_next = S.dec;
+    S.eta = std::max(S.eta_p, 1e-6);
+    S.reject_count = 0;
+    S.ps = (S.eta / S.omega) * S.dec;
+    S.ds = (S.eta * S.omega) * S.dec;
+    S.active = 1;
+    S.halt_reason = HALT_NONE;
+    S.do_reflect = 0;
+    bool restart = false;
+    while (!restart) {
+      run_until_halt();
+      if (O.time_limit > 0 && now_s() - t_start_ > O.time_limit && S.active) {
+        exit_code_ = PDCS_EXIT_TIME_LIMIT;
+        return;
+      }
+      int reason = S.halt_reason;
+      S.halt_reason = HALT_NONE;
+      if (reason == HALT_LIMIT) {
+        exit_code_ = PDCS_EXIT_ATTEMPT_LIMIT;
+        return;
+      }
+      if (reason == HALT_CHECK) {
+        exit_check();
+        max_kkt_ = std::max(std::max(ci[0].l2_rel_p, ci[0].l2_rel_d), ci[0].rel_gap);
+        S.dec_next = decay(max_kkt_);
+        log_progress();
+        if (exit_code_ != PDCS_EXIT_CONTINUE) return;
+        if (S.attempt_limit > 0 && S.iter >= S.attempt_limit) {
+          exit_code_ = PDCS_EXIT_ATTEMPT_LIMIT;
+          return;
+        }
+        if (S.accepted) {
+          post_accept(S, false);
+        } else {
+          after_reject(S);
+          if (S.reject_count > 1000000) {
+            S.eta = S.eta_p;
+            post_accept(S, true);
+          }
+        }
+        if (S.do_reflect) {
+          push_state();
+          reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, x, xl, xm, n_, y, yl, ym, m_);
+          kernels_++;
+          S.do_reflect = 0;
+        }
+        reason = S.halt_reason;
+        S.halt_reason = HALT_NONE;
+        if (reason == HALT_NONE) {
+          S.active = 1;
+          continue;
+        }
+      }
+      if (reason == HALT_ARTIFICIAL) {
+        restart_used_++;
+        restart = true;
+        break;
+      }
+      if (reason == HALT_RESTART_CHECK) {
+        bool brk = false;
+        if (O.use_kkt_restart && O.kkt_restart_freq > 0 && S.iter % O.kkt_restart_freq == 0) {
+          if (restart_check(false) || outer == 1) brk = true;
+        }
+        if (!brk && O.use_duality_gap_restart && O.duality_gap_restart_freq > 0 &&
+            S.iter % O.duality_gap_restart_freq == 0) {
+          if (restart_check(dgap_flag_) || outer == 1) brk = true;
+        }
+        if (brk) {
+          restart = true;
+          break;
+        }
+        S.active = 1;
+        continue;
+      }
+    }
+    // dynamic_primal_weight_update (:284-307)
+    DotSpec d{};
+    d.a[0] = xds; d.b[0] = x; d.kind[0] = DK_DIFF2;
+    d.count = 1; d.len = n_;
+    double xn2;
+    dots(d, &xn2);
+    DotSpec e{};
+    e.a[0] = yds; e.b[0] = y; e.kind[0] = DK_DIFF2;
+    e.count = 1; e.len = m_;
+    double yn2;
+    dots(e, &yn2);
+    double xn = std::sqrt(xn2), yn = std::sqrt(yn2), om = S.omega;
+    if ((om > 1e4 || om < 1e-4) && restart_used_ % 20 == 0 && restart_used_ != 0) S.omega = init_omega();
+    else if ((om > 3e4 || om < 1.0 / 3e4) && restart_used_ % 10 == 0 && restart_used_ != 0) S.omega = init_omega();
+    else if (xn > 1e-10 && yn > 1e-10) S.omega = std::exp(0.5 * std::log(yn / xn) + 0.5 * std::log(om));
+  }
+  exit_code_ = PDCS_EXIT_MAX_ITER;
+}
+
+int Solver::run(pdcs_result* res) {
+  int rc = validate();
+  if (rc != PDCS_OK) return rc;
+  double t0 = now_s();
+  setup();
+  converge_info(x, y, ci[0], tm[0], tn[0]);  // rpdhg_alg_gpu_gen.jl:1865-1881
+  t_start_ = now_s();
+  res->setup_time = t_start_ - t0;
+  main_loop();
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  res->time = now_s() - t_start_;
+  const bool mean = (exit_code_ == PDCS_EXIT_OPTIMAL && returned_seq_ == 1);
+  double* xo = tn[0];
+  double* yo = tm[0];
+  div_kernel<<<grid_for(n_), kThreads, 0, s_>>>(xo, mean ? xm : x, Dr, n_);
+  div_kernel<<<grid_for(m_), kThreads, 0, s_>>>(yo, mean ? ym : y, Dl, m_);
+  if (res->x) PDCS_CUDA(cudaMemcpyAsync(res->x, xo, sizeof(double) * n_, cudaMemcpyDeviceToHost, s_));
+  if (res->y) PDCS_CUDA(cudaMemcpyAsync(res->y, yo, sizeof(double) * m_, cudaMemcpyDeviceToHost, s_));
+  if (res->x_device) PDCS_CUDA(cudaMemcpyAsync(res->x_device, xo, sizeof(double) * n_, cudaMemcpyDeviceToDevice, s_));
+  if (res->y_device) PDCS_CUDA(cudaMemcpyAsync(res->y_device, yo, sizeof(double) * m_, cudaMemcpyDeviceToDevice, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  const Converge& C = ci[mean ? 1 : 0];
+  res->exit_code = exit_code_;
+  res->returned_sequence = mean ? 1 : 0;
+  res->pObj = (exit_code_ == PDCS_EXIT_OPTIMAL || exit_code_ == PDCS_EXIT_MAX_ITER) ? C.pobj : pobj_;
+  res->dObj = (exit_code_ == PDCS_EXIT_OPTIMAL || exit_code_ == PDCS_EXIT_MAX_ITER) ? C.dobj : dobj_;
+  res->iter = S.iter;
+  res->restart_used = restart_used_;
+  res->l_inf_rel_primal_res = C.linf_rel_p;
+  res->l_inf_rel_dual_res = C.linf_rel_d;
+  res->rel_gap = C.rel_gap;
+  res->l_2_rel_primal_res = C.l2_rel_p;
+  res->l_2_rel_dual_res = C.l2_rel_d;
+  res->l_inf_abs_primal_res = C.linf_abs_p;
+  res->l_inf_abs_dual_res = C.linf_abs_d;
+  res->abs_gap = C.abs_gap;
+  res->kernel_launches = kernels_;
+  res->graph_launches = graphs_;
+  return PDCS_OK;
+}
+
+}  // namespace pdcs
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int pdcs_default_options(pdcs_options* o) {
+  if (!o) return PDCS_ERR_INVALID;
+  std::memset(o, 0, sizeof(*o));
+  o->rescaling_method = 3;
+  o->use_preconditioner = 1;
+  o->use_adaptive_restart = 1;
+  o->use_adaptive_step_size_weight = 1;
+  o->use_aggressive = 1;
+  o->use_accelerated = 0;
+  o->use_resolving = 1;
+  o->warm_start = 0;
+  o->max_outer_iter = 10000;
+  o->max_inner_iter = 500000;
+  o->abs_tol = 1e-6;
+  o->rel_tol = 1e-6;
+  o->eps_primal_infeasible_low_acc = 1e-12;
+  o->eps_dual_infeasible_low_acc = 1e-12;
+  o->eps_primal_infeasible_high_acc = 1e-16;
+  o->eps_dual_infeasible_high_acc = 1e-16;
+  o->print_freq = 2000;
+  o->check_terminate_freq = 2000;
+  o->verbose = 0;
+  o->use_kkt_restart = 0;
+  o->time_limit = 0.0;
+  o->kkt_restart_freq = 2000;
+  o->use_duality_gap_restart = 1;
+  o->precision = 0;
+  o->duality_gap_restart_freq = 2000;
+  o->attempt_limit = 0;
+  o->stream = nullptr;
+  o->attempts_per_graph = 32;
+  return PDCS_OK;
+}
+
+int pdcs_solve(const pdcs_problem* prob, const pdcs_options* opts, pdcs_result* res) {
+  if (!prob || !res) return PDCS_ERR_INVALID;
+  pdcs_options o;
+  if (opts) o = *opts;
+  else pdcs_default_options(&o);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PDCS_ERR_NO_DEVICE;
+  try {
+    pdcs::Solver s(prob, &o);
+    return s.run(res);
+  } catch (const pdcs::CudaError& e) {
+    std::fprintf(stderr, "pdcs_solve: %s\n", e.what());
+    return PDCS_ERR_CUDA;
+  } catch (const std::domain_error&) {
+    return PDCS_ERR_BOUNDS;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "pdcs_solve: %s\n", e.what());
+    return PDCS_ERR_INVALID;
+  }
+}
+
+int pdcs_block_proj(double* arr, const double* bl, const double* bu, const double* S, const int64_t* head_start,
+                    const int64_t* ns, int64_t blkNum, const int64_t* proj_type, void* stream) {
+  if (blkNum < 0) return PDCS_ERR_INVALID;
+  if (blkNum == 0) return PDCS_OK;
+  if (!arr || !head_start || !ns || !proj_type) return PDCS_ERR_INVALID;
+  int64_t grid = std::min<int64_t>((blkNum + pdcs::kWarps - 1) / pdcs::kWarps, 148 * 16);
+  pdcs::block_proj_kernel<<<(int)grid, pdcs::kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      arr, bl, bu, S, head_start, ns, blkNum, proj_type);
+  return cudaGetLastError() == cudaSuccess ? PDCS_OK : PDCS_ERR_CUDA;
+}
+
+int pdcs_spmv_csr(int64_t m, int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* colind, const double* val,
+                  const double* x, double* y, void* stream) {
+  if (m < 0 || n < 0 || nnz < 0) return PDCS_ERR_INVALID;
+  if (m == 0) return PDCS_OK;
+  if (!rowptr || !y || (nnz > 0 && (!colind || !val || !x))) return PDCS_ERR_INVALID;
+  if (m > INT32_MAX || nnz > INT32_MAX) return PDCS_ERR_INVALID;
+  // rows in natural order, one lane group per row sized from the average row length
+  pdcs::CsrDev D{};
+  D.m = m;
+  D.n = n;
+  D.nnz = nnz;
+  D.rp = rowptr;
+  D.ci = colind;
+  D.v = val;
+  int64_t avg = (nnz + m - 1) / m;
+  int b = 0, g = 1;
+  while (g < 32 && (int64_t)g * 4 < avg) { g *= 2; b++; }
+  for (int k = 0; k <= pdcs::kBins; ++k) {
+    D.bin_off[k] = (k <= b) ? 0 : m;
+  }
+  int64_t rows_per_cta = pdcs::kThreads / g;
+  int32_t ctas = (int32_t)std::max<int64_t>(1, std::min<int64_t>((m + rows_per_cta - 1) / rows_per_cta, 148 * 16));
+  for (int k = 0; k <= pdcs::kBins; ++k) D.cta0[k] = (k <= b) ? 0 : ctas;
+  D.perm = nullptr;
+  pdcs::spmv_identity_kernel<<<ctas, pdcs::kThreads, 0, static_cast<cudaStream_t>(stream)>>>(D, b, x, y);
+  return cudaGetLastError() == cudaSuccess ? PDCS_OK : PDCS_ERR_CUDA;
+}
+
+const char* pdcs_version(void) { return "pdcs_b200 0.1.0 (sm_100a, FP64)"; }
+
+}  // extern "C"

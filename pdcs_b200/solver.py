@@ -1,0 +1,250 @@
+"""Python front-end mirroring PDCS's solver entry point.
+
+``rpdhg_gpu_solve`` takes the keyword arguments of the reference's
+``rpdhg_gpu_solve`` (src/pdcs_gpu/rpdhg_alg_gpu_gen.jl:1219-1268) and returns a
+``Solution`` whose fields follow the ones the reference's wrappers read
+(``x.recovered_primal.primal_sol.x``, ``y.recovered_dual.dual_sol.y``,
+``info.exit_status`` / ``exit_code`` / ``pObj`` / ``dObj`` / ``iter`` / ``time``,
+src/pdcs_gpu/MOI_wrapper/MOI_wrapper.jl:648-658).  Validation errors raise
+like the reference (rpdhg_alg_gpu_gen.jl:1331-1375, :84, :94).
+
+Inputs may be numpy / scipy (copied to the device by the library) or CUDA
+torch tensors (used in place, zero copy).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import math
+from types import SimpleNamespace
+from typing import Optional, Sequence
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import capi
+
+_RESCALING = {"none": 0, "ruiz": 1, "pock_chambolle": 2, "ruiz_pock_chambolle": 3}
+
+
+@dataclasses.dataclass
+class Info:
+    exit_status: str
+    exit_code: int
+    pObj: float
+    dObj: float
+    iter: int
+    time: float
+    setup_time: float
+    restart_used: int
+    l_inf_rel_primal_res: float
+    l_inf_rel_dual_res: float
+    rel_gap: float
+    l_2_rel_primal_res: float
+    l_2_rel_dual_res: float
+    l_inf_abs_primal_res: float
+    l_inf_abs_dual_res: float
+    abs_gap: float
+    returned_sequence: int
+    kernel_launches: int
+    graph_launches: int
+
+
+class Solution:
+    """Result of a solve; ``x`` / ``y`` are the recovered (original-scale) vectors."""
+
+    def __init__(self, x, y, info: Info):
+        self.x = SimpleNamespace(recovered_primal=SimpleNamespace(primal_sol=SimpleNamespace(x=x)))
+        self.y = SimpleNamespace(recovered_dual=SimpleNamespace(dual_sol=SimpleNamespace(y=y)))
+        self.info = info
+        self.primal = x
+        self.dual = y
+
+    def __repr__(self):
+        i = self.info
+        return (f"Solution(exit_status={i.exit_status}, iter={i.iter}, pObj={i.pObj:.10g}, "
+                f"dObj={i.dObj:.10g}, time={i.time:.4f}s)")
+
+
+def _is_torch_cuda(a):
+    return type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False)
+
+
+class _Holder:
+    """Keeps host buffers alive and returns raw pointers for the C struct."""
+
+    def __init__(self):
+        self.keep = []
+
+    def f64(self, a):
+        if a is None:
+            return None
+        if _is_torch_cuda(a):
+            import torch
+            a = a.to(torch.float64).contiguous()
+            self.keep.append(a)
+            return a.data_ptr()
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        self.keep.append(a)
+        return a.ctypes.data if a.size else None
+
+    def i32(self, a):
+        if _is_torch_cuda(a):
+            import torch
+            a = a.to(torch.int32).contiguous()
+            self.keep.append(a)
+            return a.data_ptr()
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+        self.keep.append(a)
+        return a.ctypes.data if a.size else None
+
+    def i64(self, a):
+        a = np.ascontiguousarray(np.asarray(list(a), dtype=np.int64))
+        self.keep.append(a)
+        return a.ctypes.data if a.size else None
+
+
+def rpdhg_gpu_solve(*, n: int, m: int, nb: int, c, G, h, mGzero: int, mGnonnegative: int,
+                    socG: Sequence[int], rsocG: Sequence[int], expG: int, dual_expG: int,
+                    bl, bu, soc_x: Sequence[int], rsoc_x: Sequence[int], exp_x: int = 0,
+                    dual_exp_x: int = 0, Dl=None, Dr=None,
+                    rescaling_method: str = "ruiz_pock_chambolle", use_preconditioner: bool = True,
+                    use_adaptive_restart: bool = True, use_adaptive_step_size_weight: bool = True,
+                    use_aggressive: bool = True, use_accelerated: bool = False,
+                    use_resolving: bool = True, primal_sol=None, dual_sol=None,
+                    warm_start: bool = False, max_outer_iter: int = 10000,
+                    max_inner_iter: int = 500000, abs_tol: float = 1e-6, rel_tol: float = 1e-6,
+                    eps_primal_infeasible_low_acc: float = 1e-12,
+                    eps_dual_infeasible_low_acc: float = 1e-12,
+                    eps_primal_infeasible_high_acc: float = 1e-16,
+                    eps_dual_infeasible_high_acc: float = 1e-16, print_freq: int = 2000,
+                    check_terminate_freq: int = 2000, verbose: int = 0,
+                    time_limit: float = math.inf, method: str = "average",
+                    logfile_name: Optional[str] = None, use_kkt_restart: bool = False,
+                    kkt_restart_freq: int = 2000, use_duality_gap_restart: bool = True,
+                    duality_gap_restart_freq: int = 2000, attempt_limit: int = 0,
+                    attempts_per_graph: int = 32, stream=None, device_output: bool = False) -> Solution:
+    """Solve min c'x s.t. Gx - h in K_d, bl <= x[:nb] <= bu, x[nb:] in K_p on the GPU."""
+    if method not in ("average", "halpern"):
+        raise ValueError("method only available for :average and :halpern")
+    if method == "halpern":
+        raise NotImplementedError("method=:halpern is not wired into the reference GPU module either")
+    on_device = _is_torch_cuda(c)
+    if not on_device:
+        G = sp.csr_matrix(G)
+        G.sort_indices()
+        if G.shape[0] != m:
+            raise ValueError("m does not match the size of G")
+        if G.shape[1] != n:
+            raise ValueError("n does not match the size of G")
+        rowptr, colind, val = G.indptr, G.indices, G.data
+        nnz = G.nnz
+        bl = np.asarray(bl, dtype=np.float64)
+        bu = np.asarray(bu, dtype=np.float64)
+        if bl.shape != (nb,) or bu.shape != (nb,):
+            raise ValueError("bl and bu must have length nb")
+        if not np.all(bl <= bu):
+            raise ValueError("Not all elements of bl are less than or equal to the corresponding elements in bu")
+    else:
+        rowptr, colind, val = G  # (crow_indices, col_indices, values) tensors on the device
+        nnz = int(val.numel())
+    if m != mGzero + mGnonnegative + sum(socG) + sum(rsocG) + (expG + dual_expG) * 3:
+        raise ValueError("m does not match the sum of mGzero, mGnonnegative, socG, rsocG, "
+                         "and (expG + dual_expG) * 3")
+    for q in list(socG) + list(soc_x):
+        if q < 2:
+            raise ValueError("The size of the SOC must be greater than 1")
+    for q in list(rsocG) + list(rsoc_x):
+        if q < 3:
+            raise ValueError("The size of the rotated SOC must be greater than 2")
+    if warm_start and (primal_sol is None or dual_sol is None or len(primal_sol) != n or len(dual_sol) != m):
+        raise ValueError("Warmstart doesn't match the problem size")
+
+    L = capi.load()
+    hold = _Holder()
+    P = capi.PdcsProblem()
+    P.n, P.m, P.nb, P.nnz = n, m, nb, nnz
+    P.G_rowptr, P.G_colind, P.G_val = hold.i32(rowptr), hold.i32(colind), hold.f64(val)
+    P.c, P.h, P.bl, P.bu = hold.f64(c), hold.f64(h), hold.f64(bl), hold.f64(bu)
+    P.mGzero, P.mGnonnegative = mGzero, mGnonnegative
+    P.socG, P.n_socG = hold.i64(socG), len(socG)
+    P.rsocG, P.n_rsocG = hold.i64(rsocG), len(rsocG)
+    P.expG, P.dual_expG = expG, dual_expG
+    P.soc_x, P.n_soc_x = hold.i64(soc_x), len(soc_x)
+    P.rsoc_x, P.n_rsoc_x = hold.i64(rsoc_x), len(rsoc_x)
+    P.exp_x, P.dual_exp_x = exp_x, dual_exp_x
+    P.on_device = 1 if on_device else 0
+
+    O = capi.PdcsOptions()
+    L.pdcs_default_options(C.byref(O))
+    O.rescaling_method = _RESCALING[rescaling_method.lstrip(":")]
+    O.use_preconditioner = int(use_preconditioner)
+    O.use_adaptive_restart = int(use_adaptive_restart)
+    O.use_adaptive_step_size_weight = int(use_adaptive_step_size_weight)
+    O.use_aggressive = int(use_aggressive)
+    O.use_accelerated = int(use_accelerated)
+    O.use_resolving = int(use_resolving)
+    O.warm_start = int(warm_start)
+    if warm_start:
+        O.primal_sol = hold.f64(np.asarray(primal_sol, dtype=np.float64))
+        O.dual_sol = hold.f64(np.asarray(dual_sol, dtype=np.float64))
+    O.max_outer_iter, O.max_inner_iter = max_outer_iter, max_inner_iter
+    O.abs_tol, O.rel_tol = abs_tol, rel_tol
+    O.eps_primal_infeasible_low_acc = eps_primal_infeasible_low_acc
+    O.eps_dual_infeasible_low_acc = eps_dual_infeasible_low_acc
+    O.eps_primal_infeasible_high_acc = eps_primal_infeasible_high_acc
+    O.eps_dual_infeasible_high_acc = eps_dual_infeasible_high_acc
+    O.print_freq, O.check_terminate_freq = print_freq, check_terminate_freq
+    O.verbose = int(verbose)
+    O.use_kkt_restart = int(use_kkt_restart)
+    O.time_limit = 0.0 if not math.isfinite(time_limit) else float(time_limit)
+    O.kkt_restart_freq = kkt_restart_freq
+    O.use_duality_gap_restart = int(use_duality_gap_restart)
+    O.duality_gap_restart_freq = duality_gap_restart_freq
+    O.attempt_limit = attempt_limit
+    O.attempts_per_graph = attempts_per_graph
+    O.stream = stream
+
+    R = capi.PdcsResult()
+    if device_output:
+        import torch
+        xo = torch.empty(n, dtype=torch.float64, device="cuda")
+        yo = torch.empty(m, dtype=torch.float64, device="cuda")
+        R.x_device, R.y_device = xo.data_ptr(), yo.data_ptr()
+    else:
+        xo = np.zeros(n)
+        yo = np.zeros(m)
+        R.x, R.y = (xo.ctypes.data if n else None), (yo.ctypes.data if m else None)
+    rc = L.pdcs_solve(C.byref(P), C.byref(O), C.byref(R))
+    capi.check(rc, "pdcs_solve")
+    info = Info(exit_status=capi.EXIT_STATUS.get(R.exit_code, str(R.exit_code)),
+                exit_code=R.exit_code, pObj=R.pObj, dObj=R.dObj, iter=R.iter, time=R.time,
+                setup_time=R.setup_time, restart_used=R.restart_used,
+                l_inf_rel_primal_res=R.l_inf_rel_primal_res,
+                l_inf_rel_dual_res=R.l_inf_rel_dual_res, rel_gap=R.rel_gap,
+                l_2_rel_primal_res=R.l_2_rel_primal_res, l_2_rel_dual_res=R.l_2_rel_dual_res,
+                l_inf_abs_primal_res=R.l_inf_abs_primal_res,
+                l_inf_abs_dual_res=R.l_inf_abs_dual_res, abs_gap=R.abs_gap,
+                returned_sequence=R.returned_sequence, kernel_launches=R.kernel_launches,
+                graph_launches=R.graph_launches)
+    return Solution(xo, yo, info)
+
+
+def solve_problem(prob, **kw) -> Solution:
+    """Convenience: solve a pdcs_b200.problems.ConicProblem."""
+    return rpdhg_gpu_solve(**prob.kwargs(), **kw)
+
+
+def block_proj(arr, codes, head_start, ns, S=None, bl=None, bu=None, stream=None):
+    """Project blocks of a CUDA float64 tensor in place (pdcs_block_proj)."""
+    import torch
+    dev = arr.device
+    assert arr.is_cuda and arr.dtype == torch.float64 and arr.is_contiguous()
+    hs = torch.as_tensor(np.asarray(head_start, dtype=np.int64), device=dev)
+    nn = torch.as_tensor(np.asarray(ns, dtype=np.int64), device=dev)
+    cc = torch.as_tensor(np.asarray(codes, dtype=np.int64), device=dev)
+    ptr = lambda t: None if t is None else t.data_ptr()
+    rc = capi.load().pdcs_block_proj(arr.data_ptr(), ptr(bl), ptr(bu), ptr(S), hs.data_ptr(),
+                                     nn.data_ptr(), len(codes), cc.data_ptr(), stream)
+    capi.check(rc, "pdcs_block_proj")
+    return arr

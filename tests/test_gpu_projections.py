@@ -1,0 +1,73 @@
+"""CUDA block projections (pdcs_block_proj) vs the oracle's golden outputs."""
+import numpy as np
+import pytest
+
+from oracle import binding as B
+
+GOLDEN = "tests/golden/projections.npz"
+pytestmark = pytest.mark.gpu
+
+
+def _run(cuda, v, S, heads, lens, codes, bl=None, bu=None):
+    import torch
+    from pdcs_b200 import solver
+    arr = torch.tensor(v, dtype=torch.float64, device=cuda)
+    St = None if S is None else torch.tensor(S, dtype=torch.float64, device=cuda)
+    blt = None if bl is None else torch.tensor(bl, dtype=torch.float64, device=cuda)
+    but = None if bu is None else torch.tensor(bu, dtype=torch.float64, device=cuda)
+    solver.block_proj(arr, codes, heads, lens, S=St, bl=blt, bu=but)
+    torch.cuda.synchronize()
+    return arr.cpu().numpy()
+
+
+def _blocks_from_lengths(lens):
+    heads = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.int64)
+    return heads, np.asarray(lens, dtype=np.int64)
+
+
+@pytest.mark.parametrize("kind,code", [("soc", 22), ("rsoc", 25)])
+def test_scaled_soc_rsoc_match_golden(cuda, kind, code):
+    g = np.load(GOLDEN)
+    v, S, P, lens = g[kind + "_v"], g[kind + "_S"], g[kind + "_p"], g[kind + "_len"]
+    heads, ns = _blocks_from_lengths(lens)
+    out = _run(cuda, v, S, heads, ns, [code] * len(lens))
+    for h, d in zip(heads, ns):
+        sl = slice(h, h + d)
+        scale = max(1.0, np.abs(v[sl]).max())
+        assert np.abs(out[sl] - P[sl]).max() <= 1e-12 * scale, (kind, d, out[sl], P[sl])
+
+
+@pytest.mark.parametrize("kind,code", [("exp", 27), ("dexp", 29)])
+def test_scaled_exp_match_golden(cuda, kind, code):
+    g = np.load(GOLDEN)
+    v, S, P = g[kind + "_v"], g[kind + "_S"], g[kind + "_p"]
+    nblk = len(v) // 3
+    heads = np.arange(nblk, dtype=np.int64) * 3
+    out = _run(cuda, v, S, heads, np.full(nblk, 3, np.int64), [code] * nblk)
+    for i in range(nblk):
+        sl = slice(3 * i, 3 * i + 3)
+        scale = max(1.0, np.abs(v[sl]).max())
+        assert np.abs(out[sl] - P[sl]).max() <= 1e-12 * scale, (kind, v[sl], S[sl], out[sl], P[sl])
+
+
+def test_unscaled_codes_match_oracle(cuda):
+    rng = np.random.default_rng(42)
+    blocks, kinds, codes = [], [], []
+    for _ in range(200):
+        c = rng.choice([2, 3, 5, 8, 13, 11, 17, 26, 28, 20, 23])
+        d = {2: rng.integers(1, 9), 3: rng.integers(1, 9), 5: rng.integers(2, 40), 20: rng.integers(2, 40),
+             8: rng.integers(3, 40), 23: rng.integers(3, 40), 17: rng.integers(1, 9)}.get(c, 3)
+        blocks.append(rng.standard_normal(int(d)) * rng.choice([0.1, 1, 10]))
+        codes.append(int(c))
+    lens = [len(b) for b in blocks]
+    heads, ns = _blocks_from_lengths(lens)
+    v = np.concatenate(blocks)
+    bl = np.full(len(v), -0.5)
+    bu = np.full(len(v), 0.7)
+    out = _run(cuda, v, None, heads, ns, codes, bl=bl, bu=bu)
+    kmap = {2: "zero", 3: "nonneg", 5: "soc", 20: "soc", 8: "rsoc", 23: "rsoc", 13: "exp", 26: "exp",
+            11: "dexp", 28: "dexp", 17: "box"}
+    for h, d, c in zip(heads, ns, codes):
+        sl = slice(h, h + d)
+        ref = B.project_block(kmap[c], v[sl], None, bl[sl], bu[sl])
+        assert np.abs(out[sl] - ref).max() <= 1e-12 * max(1.0, np.abs(v[sl]).max()), (c, v[sl], out[sl], ref)

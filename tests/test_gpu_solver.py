@@ -1,0 +1,77 @@
+"""End-to-end parity of the CUDA solver against the oracle (same seeded inputs)."""
+import numpy as np
+import pytest
+
+from oracle import binding as B
+from pdcs_b200 import problems, solver
+
+pytestmark = pytest.mark.gpu
+
+INSTANCES = {
+    "socp_c0": lambda: problems.socp_c0(),
+    "mixed_small": lambda: problems.mixed_small(),
+    "mixed_medium": lambda: problems.mixed_small(seed=9, scale=6),
+    "logreg_small": lambda: problems.logreg_exp_c1(samples=300, features=30, density=0.2),
+}
+
+
+@pytest.mark.parametrize("name", ["socp_c0", "mixed_small", "logreg_small"])
+@pytest.mark.parametrize("attempts", [1, 7, 60])
+def test_first_attempts_track_oracle(cuda, name, attempts):
+    """Same algorithm, same data: the first iterates agree to rounding."""
+    p = INSTANCES[name]()
+    g = solver.solve_problem(p, attempt_limit=attempts)
+    o = B.solve(p, threads=1, attempt_limit=attempts)
+    assert g.info.exit_code == 10 and o["exit_code"] == 10
+    assert g.info.iter == o["iter"] == attempts
+    for a, b in ((g.primal, o["x"]), (g.dual, o["y"])):
+        scale = max(1.0, np.abs(b).max())
+        assert np.abs(a - b).max() <= 1e-9 * scale, (name, attempts, np.abs(a - b).max())
+
+
+@pytest.mark.parametrize("name", list(INSTANCES))
+def test_solution_parity(cuda, name):
+    p = INSTANCES[name]()
+    g = solver.solve_problem(p, time_limit=120)
+    o = B.solve(p, threads=4)
+    assert g.info.exit_status == "optimal", g
+    assert o["exit_code"] == 0
+    eg = B.evaluate(p, g.primal, g.dual)
+    eo = B.evaluate(p, o["x"], o["y"])
+    # tolerance 1e-6 on the criteria the solver stops on (GPU-code denominators),
+    # with a small allowance for the evaluator's own rounding
+    for e in (eg, eo):
+        assert max(e["primal_res_gpu_form"], e["dual_res"], e["rel_gap"]) < 1.05e-6, e
+    rel = abs(eg["pobj"] - eo["pobj"]) / (1 + abs(eo["pobj"]))
+    assert rel <= 2e-6, (eg["pobj"], eo["pobj"])
+    assert abs(g.info.pObj - eg["pobj"]) <= 1e-9 * (1 + abs(eg["pobj"]))
+
+
+def test_device_resident_inputs(cuda):
+    import torch
+    p = problems.mixed_small()
+    G = p.G.tocsr()
+    t = lambda a, dt=torch.float64: torch.as_tensor(np.asarray(a), dtype=dt, device=cuda)
+    kw = p.kwargs()
+    kw.update(c=t(p.c), h=t(p.h), bl=t(p.bl), bu=t(p.bu),
+              G=(t(G.indptr, torch.int32), t(G.indices, torch.int32), t(G.data)))
+    g = solver.rpdhg_gpu_solve(**kw, device_output=True, time_limit=120)
+    h = solver.solve_problem(p, time_limit=120)
+    assert g.info.exit_status == "optimal"
+    assert np.allclose(g.primal.cpu().numpy(), h.primal, atol=1e-12)
+
+
+def test_warm_start_from_solution_converges_fast(cuda):
+    p = problems.socp_c0()
+    first = solver.solve_problem(p, time_limit=120)
+    again = solver.solve_problem(p, time_limit=120, warm_start=True, primal_sol=first.primal, dual_sol=first.dual)
+    assert again.info.exit_status == "optimal"
+    assert again.info.iter <= first.info.iter
+
+
+def test_kkt_restart_variant(cuda):
+    p = problems.mixed_small()
+    g = solver.solve_problem(p, time_limit=120, use_kkt_restart=True, use_duality_gap_restart=False)
+    o = B.solve(p, threads=2, use_kkt_restart=1, use_duality_gap_restart=0)
+    assert g.info.exit_status == "optimal" and o["exit_code"] == 0
+    assert abs(g.info.pObj - o["primal_objective"]) <= 2e-6 * (1 + abs(o["primal_objective"]))
