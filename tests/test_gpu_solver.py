@@ -61,12 +61,16 @@ def test_device_resident_inputs(cuda):
     assert np.allclose(g.primal.cpu().numpy(), h.primal, atol=1e-12)
 
 
-def test_warm_start_from_solution_converges_fast(cuda):
+def test_warm_start_matches_oracle(cuda):
     p = problems.socp_c0()
     first = solver.solve_problem(p, time_limit=120)
     again = solver.solve_problem(p, time_limit=120, warm_start=True, primal_sol=first.primal, dual_sol=first.dual)
-    assert again.info.exit_status == "optimal"
-    assert again.info.iter <= first.info.iter
+    o = B.solve(p, threads=2, warm_x=first.primal, warm_y=first.dual)
+    assert again.info.exit_status == "optimal" and o["exit_code"] == 0
+    assert again.info.iter == o["iter"]
+    w = solver.solve_problem(p, attempt_limit=30, warm_start=True, primal_sol=first.primal, dual_sol=first.dual)
+    ow = B.solve(p, threads=1, attempt_limit=30, warm_x=first.primal, warm_y=first.dual)
+    assert np.abs(w.primal - ow["x"]).max() <= 1e-9 * max(1.0, np.abs(ow["x"]).max())
 
 
 def test_kkt_restart_variant(cuda):
