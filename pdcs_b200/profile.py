@@ -1,0 +1,43 @@
+"""Bounded solve runner for profiling:  python -m pdcs_b200.profile --workload logreg --attempts 64
+
+Builds a seeded workload, uploads it to the GPU and runs the solver for a fixed
+number of PDHG attempts (or to convergence with --attempts 0), printing the
+result.  Used for the ncu launch lists and captures under profiles/.
+"""
+import argparse
+import sys
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="logreg", choices=["logreg", "logreg_small", "socp", "mixed"])
+    ap.add_argument("--attempts", type=int, default=64)
+    ap.add_argument("--samples", type=int, default=20000)
+    ap.add_argument("--features", type=int, default=500)
+    ap.add_argument("--repeat", type=int, default=1)
+    a = ap.parse_args(argv)
+    import numpy as np
+    import torch
+    from . import problems, solver
+    if a.workload == "logreg":
+        p = problems.logreg_exp_c1(samples=a.samples, features=a.features)
+    elif a.workload == "logreg_small":
+        p = problems.logreg_exp_c1(samples=2000, features=100)
+    elif a.workload == "socp":
+        p = problems.socp_c0()
+    else:
+        p = problems.mixed_small(scale=20)
+    dev = torch.device("cuda", 0)
+    G = p.G.tocsr()
+    t = lambda x, dt=torch.float64: torch.as_tensor(np.asarray(x), dtype=dt, device=dev)
+    kw = p.kwargs()
+    kw.update(c=t(p.c), h=t(p.h), bl=t(p.bl), bu=t(p.bu),
+              G=(t(G.indptr, torch.int32), t(G.indices, torch.int32), t(G.data)))
+    for _ in range(a.repeat):
+        sol = solver.rpdhg_gpu_solve(**kw, attempt_limit=a.attempts)
+    print(sol, "kernels", sol.info.kernel_launches, file=sys.stderr)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
