@@ -170,21 +170,115 @@ __global__ void __launch_bounds__(kThreads) reflect_kernel(PdhgState* st, double
   }
 }
 
-// y = A x with rows in natural order and one lane-group size (pdcs_spmv_csr)
-__global__ void __launch_bounds__(kThreads) spmv_identity_kernel(CsrDev A, int bin, const double* __restrict__ x,
-                                                                 double* __restrict__ y) {
-  const int g = 1 << bin;
-  const int lane_g = threadIdx.x & (g - 1);
-  const int64_t rows_per_cta = kThreads / g;
-  const int64_t warp_first = (int64_t)blockIdx.x * rows_per_cta + (threadIdx.x >> 5) * (32 / g);
-  for (int64_t qb = warp_first; qb < A.m; qb += (int64_t)gridDim.x * rows_per_cta) {
-    const int64_t row = qb + (threadIdx.x & 31) / g;
-    const bool valid = row < A.m;
-    const int32_t kb = valid ? A.rp[row] : 0, ke = valid ? A.rp[row + 1] : 0;
-    double s0 = 0.0;
-    for (int32_t k = kb + lane_g; k < ke; k += g) s0 = fma(A.v[k], x[A.ci[k]], s0);
-    for (int o = g >> 1; o > 0; o >>= 1) s0 += __shfl_down_sync(kFull, s0, o, g);
-    if (valid && lane_g == 0) y[row] = s0;
+// ---------------------------------------------------------------------------
+// Merge-path CSR SpMV (Merrill & Garland, "Merge-based parallel sparse
+// matrix-vector multiplication", SC'16): the m row ends and the nnz nonzeros
+// form m + nnz merge items split evenly over CTAs (kMergeItems per CTA, 8 per
+// thread), so the work per CTA is independent of the row-length distribution.
+// Every row end is consumed by exactly one thread, which writes y[row]; the
+// partial sum of a row that continues past a thread's items is combined
+// inside the CTA, and the partial of a row that continues past the CTA
+// becomes the CTA's carry (carry_row / carry_val, one entry per CTA), added
+// in CTA order by spmv_merge_fixup_kernel.
+// ---------------------------------------------------------------------------
+constexpr int kMergeIPT = 8;
+constexpr int kMergeItems = kThreads * kMergeIPT;
+
+__device__ inline void merge_path_search(int64_t diag, const int32_t* __restrict__ row_end, int64_t nrows,
+                                         int64_t nnz, int64_t* row, int64_t* k) {
+  int64_t lo = diag - nnz > 0 ? diag - nnz : 0;
+  int64_t hi = diag < nrows ? diag : nrows;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if ((int64_t)row_end[mid] <= diag - mid - 1) lo = mid + 1;
+    else hi = mid;
+  }
+  *row = lo;
+  *k = diag - lo;
+}
+
+__global__ void __launch_bounds__(kThreads) spmv_merge_kernel(int64_t m, int64_t nnz, const int32_t* __restrict__ rp,
+                                                              const int32_t* __restrict__ ci,
+                                                              const double* __restrict__ v,
+                                                              const double* __restrict__ x, double* __restrict__ y,
+                                                              int32_t* __restrict__ carry_row,
+                                                              double* __restrict__ carry_val) {
+  const int64_t total = m + nnz;
+  const int64_t d0 = (int64_t)blockIdx.x * kMergeItems;
+  const int64_t d1 = d0 + kMergeItems < total ? d0 + kMergeItems : total;
+  const int32_t* row_end = rp + 1;
+  __shared__ int64_t s_r0, s_r1;
+  __shared__ int64_t s_row[kThreads];
+  __shared__ double s_val[kThreads];
+  if (threadIdx.x == 0) {
+    int64_t kk;
+    merge_path_search(d0, row_end, m, nnz, &s_r0, &kk);
+    merge_path_search(d1, row_end, m, nnz, &s_r1, &kk);
+  }
+  __syncthreads();
+  const int nvalid = (int)((d1 - d0 + kMergeIPT - 1) / kMergeIPT);
+  const int t = threadIdx.x;
+  const int64_t dt = d0 + (int64_t)t * kMergeIPT;
+  int64_t row = -1;
+  double sum = 0.0;
+  if (t < nvalid) {
+    const int64_t dte = dt + kMergeIPT < d1 ? dt + kMergeIPT : d1;
+    // search only inside this CTA's row range [s_r0, s_r1]
+    int64_t lo = dt - nnz > s_r0 ? dt - nnz : s_r0;
+    int64_t hi = dt < s_r1 ? dt : s_r1;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if ((int64_t)row_end[mid] <= dt - mid - 1) lo = mid + 1;
+      else hi = mid;
+    }
+    row = lo;
+    int64_t k = dt - lo;
+    for (int64_t it = dt; it < dte; ++it) {
+      if (row < m && k < (int64_t)row_end[row]) {
+        sum = fma(v[k], x[ci[k]], sum);
+        ++k;
+      } else {
+        y[row] = sum;  // this thread consumed the end of `row`
+        sum = 0.0;
+        ++row;
+      }
+    }
+    if (row >= m) row = -1;  // finished every row: nothing carried
+  }
+  s_row[t] = row;
+  s_val[t] = sum;
+  __syncthreads();
+  // Threads t..u-1 that all stop inside row r form a run.  If thread u < nvalid
+  // exists it started inside row r and moved past it, so it consumed row r's
+  // end and already wrote y[r]; otherwise row r continues into the next CTA.
+  const int64_t r = s_row[t];
+  if (t < nvalid && r >= 0 && (t == 0 || s_row[t - 1] != r)) {
+    double acc = 0.0;
+    int u = t;
+    while (u < nvalid && s_row[u] == r) acc += s_val[u++];
+    if (u < nvalid) {
+      y[r] += acc;
+    } else {
+      carry_row[blockIdx.x] = (int32_t)r;
+      carry_val[blockIdx.x] = acc;
+    }
+  }
+  if (t == 0 && s_row[nvalid - 1] < 0) {  // no row continues past this CTA
+    carry_row[blockIdx.x] = -1;
+    carry_val[blockIdx.x] = 0.0;
+  }
+}
+
+// y[carry_row[c]] += carry_val[c], summing consecutive carries of one row in CTA order
+__global__ void spmv_merge_fixup_kernel(int64_t nctas, const int32_t* __restrict__ carry_row,
+                                        const double* __restrict__ carry_val, double* __restrict__ y) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nctas; c += stride) {
+    const int32_t r = carry_row[c];
+    if (r < 0 || (c > 0 && carry_row[c - 1] == r)) continue;
+    double acc = 0.0;
+    for (int64_t u = c; u < nctas && carry_row[u] == r; ++u) acc += carry_val[u];
+    y[r] += acc;
   }
 }
 
@@ -1469,26 +1563,22 @@ int pdcs_spmv_csr(int64_t m, int64_t n, int64_t nnz, const int32_t* rowptr, cons
   if (m == 0) return PDCS_OK;
   if (!rowptr || !y || (nnz > 0 && (!colind || !val || !x))) return PDCS_ERR_INVALID;
   if (m > INT32_MAX || nnz > INT32_MAX) return PDCS_ERR_INVALID;
-  // rows in natural order, one lane group per row sized from the average row length
-  pdcs::CsrDev D{};
-  D.m = m;
-  D.n = n;
-  D.nnz = nnz;
-  D.rp = rowptr;
-  D.ci = colind;
-  D.v = val;
-  int64_t avg = (nnz + m - 1) / m;
-  int b = 0, g = 1;
-  while (g < 32 && (int64_t)g * 4 < avg) { g *= 2; b++; }
-  for (int k = 0; k <= pdcs::kBins; ++k) {
-    D.bin_off[k] = (k <= b) ? 0 : m;
-  }
-  int64_t rows_per_cta = pdcs::kThreads / g;
-  int32_t ctas = (int32_t)std::max<int64_t>(1, std::min<int64_t>((m + rows_per_cta - 1) / rows_per_cta, 148 * 16));
-  for (int k = 0; k <= pdcs::kBins; ++k) D.cta0[k] = (k <= b) ? 0 : ctas;
-  D.perm = nullptr;
-  pdcs::spmv_identity_kernel<<<ctas, pdcs::kThreads, 0, static_cast<cudaStream_t>(stream)>>>(D, b, x, y);
-  return cudaGetLastError() == cudaSuccess ? PDCS_OK : PDCS_ERR_CUDA;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int64_t nctas = (m + nnz + pdcs::kMergeItems - 1) / pdcs::kMergeItems;
+  if (nctas > INT32_MAX) return PDCS_ERR_INVALID;
+  // workspace for the per-CTA row carries (stream-ordered, like cuSPARSE's SpMV buffer)
+  void* ws = nullptr;
+  const size_t carry_bytes = ((size_t)nctas * sizeof(double) + 255) & ~(size_t)255;
+  if (cudaMallocAsync(&ws, carry_bytes + (size_t)nctas * sizeof(int32_t), s) != cudaSuccess) return PDCS_ERR_CUDA;
+  double* carry_val = static_cast<double*>(ws);
+  int32_t* carry_row = reinterpret_cast<int32_t*>(static_cast<char*>(ws) + carry_bytes);
+  pdcs::spmv_merge_kernel<<<(unsigned)nctas, pdcs::kThreads, 0, s>>>(m, nnz, rowptr, colind, val, x, y, carry_row,
+                                                                   carry_val);
+  int fg = (int)std::min<int64_t>((nctas + pdcs::kThreads - 1) / pdcs::kThreads, 148 * 8);
+  pdcs::spmv_merge_fixup_kernel<<<fg, pdcs::kThreads, 0, s>>>(nctas, carry_row, carry_val, y);
+  cudaError_t e = cudaGetLastError();
+  if (cudaFreeAsync(ws, s) != cudaSuccess) return PDCS_ERR_CUDA;
+  return e == cudaSuccess ? PDCS_OK : PDCS_ERR_CUDA;
 }
 
 const char* pdcs_version(void) { return "pdcs_b200 0.1.0 (sm_100a, FP64)"; }
