@@ -36,6 +36,7 @@ extern "C" {
 #define PDCS_ERR_N_MISMATCH (-7)     /* cone blocks of x exceed n              */
 #define PDCS_ERR_NO_DEVICE (-8)      /* no CUDA device                         */
 #define PDCS_ERR_UNSUPPORTED (-9)    /* option combination not implemented     */
+#define PDCS_ERR_NOALLOC_LIMIT (-10) /* problem exceeds the fixed scratch of pdcs_spmv_csr_noalloc */
 
 /* ---- solver exit codes (pdcs_result.exit_code), as the reference --------- */
 #define PDCS_EXIT_OPTIMAL 0
@@ -153,6 +154,22 @@ int pdcs_block_proj(double* arr, const double* bl, const double* bu, const doubl
  * Applying it to the CSR of G' replaces union_adjoint! (:864-866). */
 int pdcs_spmv_csr(int64_t m, int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* colind,
                   const double* val, const double* x, double* y, void* stream);
+
+/* Same result as pdcs_spmv_csr, without allocating.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc -- a host
+ * whose device memory is owned by its own pool allocator (Julia's CUDA.jl
+ * pool, PyTorch's caching allocator) and must not be bypassed or fragmented,
+ * or a latency-critical loop where a driver allocation would stall.  The
+ * row-carry scratch is a file-scope device array of 65536 entries, so
+ * m + nnz must not exceed 134,217,728 (PDCS_ERR_NOALLOC_LIMIT otherwise);
+ * every GPU that loads the library keeps those 768 KiB until the process
+ * exits.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, once per device); make that first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (different streams, no ordering) race on it.  Allocates nothing:
+ * no cudaMalloc, cudaFree or allocating library routine. */
+int pdcs_spmv_csr_noalloc(int64_t m, int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* colind,
+                          const double* val, const double* x, double* y, void* stream);
 
 /* Library version string. */
 const char* pdcs_version(void);

@@ -26,6 +26,7 @@ ERRORS = {
     -7: "cone blocks of x exceed n",
     -8: "no CUDA device",
     -9: "The combination of options is not supported.",
+    -10: "m + nnz exceeds the fixed scratch of pdcs_spmv_csr_noalloc (134217728 merge items)",
 }
 EXIT_STATUS = {
     0: "optimal", 1: "max_iter", 2: "primal_infeasible_low_acc", 3: "primal_infeasible_high_acc",
@@ -80,7 +81,8 @@ class PdcsResult(C.Structure):
 
 
 # every symbol declared in include/pdcs.h
-EXPORTS = ["pdcs_default_options", "pdcs_solve", "pdcs_block_proj", "pdcs_spmv_csr", "pdcs_version"]
+EXPORTS = ["pdcs_default_options", "pdcs_solve", "pdcs_block_proj", "pdcs_spmv_csr", "pdcs_spmv_csr_noalloc",
+           "pdcs_version"]
 
 _lib = None
 
@@ -102,6 +104,8 @@ def load():
     L.pdcs_block_proj.restype = C.c_int
     L.pdcs_spmv_csr.argtypes = [C.c_int64, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp]
     L.pdcs_spmv_csr.restype = C.c_int
+    L.pdcs_spmv_csr_noalloc.argtypes = [C.c_int64, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.pdcs_spmv_csr_noalloc.restype = C.c_int
     L.pdcs_version.restype = C.c_char_p
     _lib = L
     return L

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1579,6 +1580,61 @@ int pdcs_spmv_csr(int64_t m, int64_t n, int64_t nnz, const int32_t* rowptr, cons
   cudaError_t e = cudaGetLastError();
   if (cudaFreeAsync(ws, s) != cudaSuccess) return PDCS_ERR_CUDA;
   return e == cudaSuccess ? PDCS_OK : PDCS_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// pdcs_spmv_csr_noalloc: pdcs_spmv_csr for callers that cannot allocate
+// device memory (see include/pdcs.h).  The per-CTA carries live in a
+// file-scope device array, sized for kNoAllocMaxCtas CTAs: 65536 CTAs of
+// 2048 merge items, i.e. m + nnz <= 134,217,728; 768 KiB that every GPU which
+// loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+static constexpr int64_t kNoAllocMaxCtas = 65536;
+static __device__ __align__(256) unsigned char g_spmv_noalloc_scratch[kNoAllocMaxCtas * (sizeof(double) + sizeof(int32_t))];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 128;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array for the current device.  In host code
+// the array's name is only a host-side stand-in; the address must come from
+// cudaGetSymbolAddress with the device current, once per device.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return PDCS_ERR_CUDA;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return PDCS_ERR_INVALID;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_spmv_noalloc_scratch) != cudaSuccess || !p) return PDCS_ERR_CUDA;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return PDCS_OK;
+}
+}  // namespace
+
+int pdcs_spmv_csr_noalloc(int64_t m, int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* colind,
+                          const double* val, const double* x, double* y, void* stream) {
+  if (m < 0 || n < 0 || nnz < 0) return PDCS_ERR_INVALID;
+  if (m == 0) return PDCS_OK;
+  if (!rowptr || !y || (nnz > 0 && (!colind || !val || !x))) return PDCS_ERR_INVALID;
+  if (m > INT32_MAX || nnz > INT32_MAX) return PDCS_ERR_INVALID;
+  const int64_t nctas = (m + nnz + pdcs::kMergeItems - 1) / pdcs::kMergeItems;
+  if (nctas > kNoAllocMaxCtas) return PDCS_ERR_NOALLOC_LIMIT;
+  void* base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc != PDCS_OK) return rc;
+  // every CTA writes its own carry entry, so nothing needs clearing between calls
+  double* carry_val = static_cast<double*>(base);
+  int32_t* carry_row = reinterpret_cast<int32_t*>(static_cast<char*>(base) + kNoAllocMaxCtas * sizeof(double));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  pdcs::spmv_merge_kernel<<<(unsigned)nctas, pdcs::kThreads, 0, s>>>(m, nnz, rowptr, colind, val, x, y, carry_row,
+                                                                   carry_val);
+  int fg = (int)std::min<int64_t>((nctas + pdcs::kThreads - 1) / pdcs::kThreads, 148 * 8);
+  pdcs::spmv_merge_fixup_kernel<<<fg, pdcs::kThreads, 0, s>>>(nctas, carry_row, carry_val, y);
+  return cudaGetLastError() == cudaSuccess ? PDCS_OK : PDCS_ERR_CUDA;
 }
 
 const char* pdcs_version(void) { return "pdcs_b200 0.1.0 (sm_100a, FP64)"; }
