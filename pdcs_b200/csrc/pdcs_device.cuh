@@ -195,19 +195,37 @@ struct ExpCtx {
   __device__ double Q(double x) const { return ds * ds + dr * dr * x * (x - 1.0); }
   __device__ double N1(double x) const { return dr * r * (x - 1.0) + ds * s; }
   __device__ double N2(double x) const { return ds * r - dr * s * x; }
-  __device__ double fs(double x, int zmask) const {  // f(x) e^{-|x|}
-    double ax = fabs(x);
-    double n1 = (zmask & 1) ? 0.0 : N1(x);
-    double n2 = (zmask & 2) ? 0.0 : N2(x);
-    return n1 * dt * exp(x - ax) - dr * ds * n2 * exp(-x - ax) / dt - t * Q(x) * exp(-ax);
+  // f(x) e^{-|x|} (same sign as f, never overflows) and its derivative, from one
+  // exponential: e^{x-|x|} and e^{-x-|x|} are 1 or e^{-2|x|} = (e^{-|x|})^2.
+  // also returns the size of the terms of f, the scale of its rounding noise
+  __device__ void gd(double x, int zmask, double& g, double& dg, double& mag) const;
+  __device__ void gd(double x, int zmask, double& g, double& dg) const {
+    double mag;
+    gd(x, zmask, g, dg, mag);
   }
-  __device__ double dfs(double x) const {
-    double ax = fabs(x), sg = x >= 0.0 ? 1.0 : -1.0;
-    double fp = dt * exp(x - ax) * (dr * r + N1(x)) + (dr * ds / dt) * exp(-x - ax) * (dr * s + N2(x)) -
-                t * dr * dr * (2.0 * x - 1.0) * exp(-ax);
-    return fp - sg * fs(x, 0);
+  __device__ double fs(double x, int zmask) const {
+    double g, dg;
+    gd(x, zmask, g, dg);
+    return g;
   }
 };
+
+// One out-of-line copy: the exponential is the bulk of the code, and the
+// exp-cone kernels are otherwise large enough to stall on instruction fetch.
+__device__ __noinline__ void ExpCtx::gd(double x, int zmask, double& g, double& dg, double& mag) const {
+  const double e3 = exp(-fabs(x));
+  const double e3s = e3 * e3;
+  const double e1 = x >= 0.0 ? 1.0 : e3s;
+  const double e2 = x >= 0.0 ? e3s : 1.0;
+  const double n1 = (zmask & 1) ? 0.0 : N1(x);
+  const double n2 = (zmask & 2) ? 0.0 : N2(x);
+  const double a = n1 * dt * e1, b = dr * ds * n2 * e2 / dt, c = t * Q(x) * e3;
+  const double f = a - b - c;
+  const double fp = dt * e1 * (dr * r + n1) + (dr * ds / dt) * e2 * (dr * s + n2) - t * dr * dr * (2.0 * x - 1.0) * e3;
+  g = f;
+  dg = fp - (x >= 0.0 ? f : -f);
+  mag = fabs(a) + fabs(b) + fabs(c);
+}
 
 __device__ inline bool d_in_kexp(double r, double s, double t) {
   if (s > 0.0) return s * exp(r / s) <= t;
@@ -218,44 +236,10 @@ __device__ inline bool d_in_kexp_dual(double a, double b, double c) {
   return (a == 0.0 && b >= 0.0 && c >= 0.0);
 }
 
-__device__ inline bool exp_root_dev(const ExpCtx& C, double* rho_out) {
-  double bv[4];
-  int bt[4];
-  int nb = 0;
-  auto push = [&](double x, int tg) {
-    if (!isfinite(x)) return;
-    // insertion into the sorted list, merging equal values
-    int k = nb;
-    for (int q = 0; q < nb; ++q)
-      if (bv[q] == x) { bt[q] |= tg; return; }
-    while (k > 0 && bv[k - 1] > x) { bv[k] = bv[k - 1]; bt[k] = bt[k - 1]; --k; }
-    bv[k] = x;
-    bt[k] = tg;
-    ++nb;
-  };
-  if (C.r != 0.0) push(1.0 - C.ds * C.s / (C.dr * C.r), 1);
-  if (C.s != 0.0) push(C.ds * C.r / (C.dr * C.s), 2);
-  double ratio = C.ds / C.dr;
-  double disc = 1.0 - 4.0 * ratio * ratio;
-  if (disc >= 0.0) {
-    double sq = sqrt(disc);
-    push(0.5 * (1.0 - sq), 4);
-    push(0.5 * (1.0 + sq), 4);
-  }
-  const double kInfD = __longlong_as_double(0x7ff0000000000000LL);
-  for (int j = 0; j <= nb; ++j) {
-    double lo = (j == 0) ? -kInfD : bv[j - 1];
-    double hi = (j == nb) ? kInfD : bv[j];
-    int tlo = (j == 0) ? 0 : bt[j - 1];
-    int thi = (j == nb) ? 0 : bt[j];
-    double p;
-    if (isinf(lo) && isinf(hi)) p = 0.0;
-    else if (isinf(lo)) p = hi - fmax(1.0, fabs(hi));
-    else if (isinf(hi)) p = lo + fmax(1.0, fabs(lo));
-    else p = 0.5 * (lo + hi);
-    double Qp = C.Q(p);
-    if (!(C.N1(p) * Qp > 0.0 && C.N2(p) * Qp > 0.0)) continue;
-    double sg = Qp > 0.0 ? 1.0 : -1.0;
+// Bracketed safeguarded Newton on one admissible interval (cold start).
+__device__ __noinline__ bool exp_root_bracketed(const ExpCtx& C, double lo, double hi, int tlo, int thi, double p,
+                                                double sg, double* rho_out) {
+  const double eps = 2.220446049250313e-16;
     double a, ga, b, gb;
     if (isinf(lo)) {
       double step = fmax(1.0, fabs(p));
@@ -284,32 +268,95 @@ __device__ inline bool exp_root_dev(const ExpCtx& C, double* rho_out) {
       b = hi;
       gb = sg * C.fs(b, thi & 3);
     }
-    if (!(isfinite(ga) && isfinite(gb))) continue;
-    if (!((ga <= 0.0 && gb >= 0.0) || (ga >= 0.0 && gb <= 0.0))) continue;
+    if (!(isfinite(ga) && isfinite(gb))) return false;
+    if (!((ga <= 0.0 && gb >= 0.0) || (ga >= 0.0 && gb <= 0.0))) return false;
     if (ga == 0.0) { *rho_out = a; return true; }
     if (gb == 0.0) { *rho_out = b; return true; }
     double L = a, R = b;
     bool inc = ga < 0.0;
     double x = 0.5 * (L + R);
     for (int it = 0; it < 400; ++it) {
-      double gx = sg * C.fs(x, 0);
+      double gx, dgx;
+      C.gd(x, 0, gx, dgx);
+      gx *= sg;
       if (gx == 0.0) break;
       if ((gx < 0.0) == inc) L = x; else R = x;
       double lo2 = fmin(L, R), hi2 = fmax(L, R);
-      if (hi2 - lo2 <= 2.0 * 2.220446049250313e-16 * fmax(1.0, fabs(x))) break;
-      double xn = x - gx / (sg * C.dfs(x));
+      if (hi2 - lo2 <= 2.0 * eps * fmax(1.0, fabs(x))) break;
+      double xn = x - gx / (sg * dgx);
       if (!(xn > lo2 && xn < hi2) || !isfinite(xn)) xn = 0.5 * (lo2 + hi2);
       if (xn == x) break;
       x = xn;
     }
     *rho_out = x;
     return true;
+}
+
+// rho_hint: warm start (the root of the previous projection of this cone, or NaN)
+__device__ inline bool exp_root_dev(const ExpCtx& C, double* rho_out, double rho_hint) {
+  double bv[4];
+  int bt[4];
+  int nb = 0;
+  auto push = [&](double x, int tg) {
+    if (!isfinite(x)) return;
+    for (int q = 0; q < nb; ++q)
+      if (bv[q] == x) { bt[q] |= tg; return; }
+    int k = nb;
+    while (k > 0 && bv[k - 1] > x) { bv[k] = bv[k - 1]; bt[k] = bt[k - 1]; --k; }
+    bv[k] = x;
+    bt[k] = tg;
+    ++nb;
+  };
+  if (C.r != 0.0) push(1.0 - C.ds * C.s / (C.dr * C.r), 1);
+  if (C.s != 0.0) push(C.ds * C.r / (C.dr * C.s), 2);
+  double ratio = C.ds / C.dr;
+  double disc = 1.0 - 4.0 * ratio * ratio;
+  if (disc >= 0.0) {
+    double sq = sqrt(disc);
+    push(0.5 * (1.0 - sq), 4);
+    push(0.5 * (1.0 + sq), 4);
+  }
+  const double kInfD = __longlong_as_double(0x7ff0000000000000LL);
+  const double eps = 2.220446049250313e-16;
+  for (int j = 0; j <= nb; ++j) {
+    double lo = (j == 0) ? -kInfD : bv[j - 1];
+    double hi = (j == nb) ? kInfD : bv[j];
+    int tlo = (j == 0) ? 0 : bt[j - 1];
+    int thi = (j == nb) ? 0 : bt[j];
+    double p;
+    if (isinf(lo) && isinf(hi)) p = 0.0;
+    else if (isinf(lo)) p = hi - fmax(1.0, fabs(hi));
+    else if (isinf(hi)) p = lo + fmax(1.0, fabs(lo));
+    else p = 0.5 * (lo + hi);
+    double Qp = C.Q(p);
+    if (!(C.N1(p) * Qp > 0.0 && C.N2(p) * Qp > 0.0)) continue;
+    const double sg = Qp > 0.0 ? 1.0 : -1.0;
+    // The admissible interval holds exactly one root (the KKT point), so a
+    // Newton sequence that stays inside it converges to the projection.
+    if (isfinite(rho_hint) && rho_hint > lo && rho_hint < hi) {
+      double x = rho_hint;
+      bool ok = false;
+      for (int it = 0; it < 12; ++it) {
+        double g, dg, mag;
+        C.gd(x, 0, g, dg, mag);
+        if (fabs(g) <= 8.0 * eps * mag) { ok = true; break; }  // at the rounding floor of f
+        double xn = x - g / dg;
+        if (!(xn > lo && xn < hi) || !isfinite(xn)) break;
+        if (fabs(xn - x) <= 4.0 * eps * fmax(1.0, fabs(x))) { x = xn; ok = true; break; }
+        x = xn;
+      }
+      if (ok) { *rho_out = x; return true; }
+    }
+    if (exp_root_bracketed(C, lo, hi, tlo, thi, p, sg, rho_out)) return true;
+    continue;
   }
   return false;
 }
 
+
 // Projection of (r, s, t) onto (dr, ds, dt) o K_exp, in place.
-__device__ inline void proj_exp_scaled_dev(double& r, double& s, double& t, double dr, double ds, double dt) {
+__device__ inline void proj_exp_scaled_dev(double& r, double& s, double& t, double dr, double ds, double dt,
+                                           double* rho_ws = nullptr) {
   if (!(isfinite(r) && isfinite(s) && isfinite(t))) return;
   if (d_in_kexp(r / dr, s / ds, t / dt)) return;
   if (d_in_kexp_dual(-dr * r, -ds * s, -dt * t)) {
@@ -324,7 +371,9 @@ __device__ inline void proj_exp_scaled_dev(double& r, double& s, double& t, doub
   double scale = fmax(fabs(r), fmax(fabs(s), fabs(t)));
   ExpCtx C{r / scale, s / scale, t / scale, dr, ds, dt};
   double rho;
-  if (exp_root_dev(C, &rho)) {
+  const double hint = rho_ws ? *rho_ws : __longlong_as_double(0x7ff8000000000000LL);
+  if (exp_root_dev(C, &rho, hint)) {
+    if (rho_ws) *rho_ws = rho;
     double q = C.Q(rho), n1 = C.N1(rho), n2 = C.N2(rho);
     double c1 = fabs(n1) / (fabs(dr * C.r * rho) + fabs(dr * C.r) + fabs(ds * C.s));
     double c2 = fabs(n2) / (fabs(ds * C.r) + fabs(dr * C.s * rho));
@@ -356,9 +405,10 @@ __device__ inline void proj_exp_scaled_dev(double& r, double& s, double& t, doub
 }
 
 // S o K_exp^* via Moreau: P(v) = v + P_{(1/S) o K}(-v).
-__device__ inline void proj_dexp_scaled_dev(double& r, double& s, double& t, double Sr, double Ss, double St) {
+__device__ inline void proj_dexp_scaled_dev(double& r, double& s, double& t, double Sr, double Ss, double St,
+                                            double* rho_ws = nullptr) {
   double a = -r, b = -s, c = -t;
-  proj_exp_scaled_dev(a, b, c, 1.0 / Sr, 1.0 / Ss, 1.0 / St);
+  proj_exp_scaled_dev(a, b, c, 1.0 / Sr, 1.0 / Ss, 1.0 / St, rho_ws);
   r += a;
   s += b;
   t += c;

@@ -40,7 +40,9 @@ struct PdhgState {
   long long iter, iter_stepsize, inner, reject_count;
   long long check_freq, restart_freq, attempt_limit;
   int32_t active, do_reflect, halt_reason, accepted;
-  int32_t force_restart, restart_enabled, pad0, pad1;
+  int32_t force_restart, restart_enabled;
+  uint32_t done_ctas;  // CTAs of the dual step that have finished (last one runs the control step)
+  int32_t pad1;
 };
 
 // Shared by the control kernel and the host (after a checkpoint):
@@ -102,7 +104,11 @@ template <int NV>
 __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const double* __restrict__ x0,
                                                               const double* __restrict__ x1,
                                                               double* __restrict__ y0, double* __restrict__ y1,
-                                                              const int32_t* __restrict__ active) {
+                                                              const int32_t* __restrict__ active,
+                                                              int32_t* __restrict__ clear_flag = nullptr) {
+  // first kernel of a PDHG attempt: the previous attempt's reflection (if any)
+  // has run by now, so its flag is cleared here, before the halt check
+  if (clear_flag && blockIdx.x == 0 && threadIdx.x == 0) *clear_flag = 0;
   if (active && !*active) return;
   const int cta = blockIdx.x;
   int bin = 0;
@@ -123,13 +129,26 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const d
       const bool valid = q < r1;
       const int32_t row = valid ? A.perm[q] : 0;
       const int32_t kb = valid ? A.rp[row] : 0, ke = valid ? A.rp[row + 1] : 0;
-      double s0 = 0.0, s1 = 0.0;
-      for (int32_t k = kb + lane_g; k < ke; k += g) {
-        const double a = A.v[k];
-        const int32_t col = A.ci[k];
-        s0 = fma(a, x0[col], s0);
-        if (NV == 2) s1 = fma(a, x1[col], s1);
+      double s0 = 0.0, s1 = 0.0, t0 = 0.0, t1 = 0.0;
+      int32_t k = kb + lane_g;
+      for (; k + g < ke; k += 2 * g) {  // two independent gathers in flight
+        const double a = A.v[k], b = A.v[k + g];
+        const int32_t ca = A.ci[k], cb = A.ci[k + g];
+        s0 = fma(a, x0[ca], s0);
+        t0 = fma(b, x0[cb], t0);
+        if (NV == 2) {
+          s1 = fma(a, x1[ca], s1);
+          t1 = fma(b, x1[cb], t1);
+        }
       }
+      if (k < ke) {
+        const double a = A.v[k];
+        const int32_t ca = A.ci[k];
+        s0 = fma(a, x0[ca], s0);
+        if (NV == 2) s1 = fma(a, x1[ca], s1);
+      }
+      s0 += t0;
+      s1 += t1;
       for (int o = g >> 1; o > 0; o >>= 1) {
         s0 += __shfl_down_sync(kFull, s0, o, g);
         if (NV == 2) s1 += __shfl_down_sync(kFull, s1, o, g);
@@ -195,6 +214,7 @@ struct ConeTable {
   int64_t dexp_base, dexp_count;
   int32_t dexp_kind;
   const double* S;           // scaling (NULL: unscaled)
+  double* rho_ws;            // per exp/dual-exp cone warm start of the root (NULL: none)
   int64_t elem_total;        // sum of seg_len
   int32_t ctaA, ctaB, ctaC;  // CTAs for elementwise / warp cones / exp cones
 };
@@ -228,6 +248,64 @@ __device__ inline void block_reduce_store(double (&acc)[N], const int32_t* kinds
     for (int w = 1; w < kWarps; ++w) v = (kinds[k] == ACC_MAX) ? fmax(v, sh[k][w]) : v + sh[k][w];
     partials[(int64_t)k * nblocks + blockIdx.x] = v;
   }
+}
+
+// The control step of one PDHG attempt (rpdhg_alg_gpu_gen_scaling.jl:711-765):
+// reduce the step's partial sums (fixed order), form eta_bar and eta', decide
+// accept / retry / halt.  Run by one CTA of kThreads threads.
+__device__ inline void control_block(PdhgState* st, const double* px, int nbx, const double* py, int nby) {
+  __shared__ double sh[3][kThreads];
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int i = threadIdx.x; i < nbx; i += kThreads) a += __ldcg(px + i);
+  for (int i = threadIdx.x; i < nby; i += kThreads) {
+    b += __ldcg(py + i);
+    c += __ldcg(py + nby + i);
+  }
+  sh[0][threadIdx.x] = a;
+  sh[1][threadIdx.x] = b;
+  sh[2][threadIdx.x] = c;
+  __syncthreads();
+  for (int s2 = kThreads / 2; s2 > 0; s2 >>= 1) {
+    if (threadIdx.x < s2) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + s2];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + s2];
+      sh[2][threadIdx.x] += sh[2][threadIdx.x + s2];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  PdhgState s = *st;
+  s.done_ctas = 0;
+  s.sum_dx2 = sh[0][0];
+  s.sum_dy2 = sh[1][0];
+  s.sum_dgdy = sh[2][0];
+  s.do_reflect = 0;
+  double num = s.omega * s.sum_dx2 + s.sum_dy2 / s.omega;
+  double den = 2.0 * fabs(s.sum_dgdy);
+  s.eta_bar = num / (den + 1e-20);
+  s.iter += 1;
+  s.iter_stepsize += 1;
+  double k1 = (double)(s.iter_stepsize + 1);
+  s.eta_p = fmin((1.0 - pow(k1, -0.3)) * s.eta_bar, (1.0 + pow(k1, -0.6)) * s.eta);
+  s.tau = s.eta / s.omega;
+  s.sigma = s.eta * s.omega;
+  s.accepted = (s.eta <= s.eta_bar) ? 1 : 0;
+  if (s.check_freq > 0 && s.iter % s.check_freq == 0) {
+    s.halt_reason = HALT_CHECK;  // the host runs the exit check, then decides
+    s.active = 0;
+  } else if (s.attempt_limit > 0 && s.iter >= s.attempt_limit) {
+    s.halt_reason = HALT_LIMIT;
+    s.active = 0;
+  } else if (s.accepted) {
+    post_accept(s, false);
+  } else {
+    after_reject(s);
+    if (s.reject_count > 1000000) {
+      s.eta = s.eta_p;  // the forced return hands back the last eta (:757-764)
+      post_accept(s, true);
+    }
+  }
+  *st = s;
 }
 
 // Generic update + projection.  Op supplies:
@@ -336,14 +414,25 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
         S1 = T.S[j + 1];
         S2 = T.S[j + 2];
       }
-      if (kind == PK_EXP) proj_exp_scaled_dev(r, s, t, S0, S1, S2);
-      else proj_dexp_scaled_dev(r, s, t, S0, S1, S2);
+      double* ws = T.rho_ws ? T.rho_ws + k : nullptr;
+      if (kind == PK_EXP) proj_exp_scaled_dev(r, s, t, S0, S1, S2, ws);
+      else proj_dexp_scaled_dev(r, s, t, S0, S1, S2, ws);
       op.fin(j, z0, r, acc);
       op.fin(j + 1, z1, s, acc);
       op.fin(j + 2, z2, t, acc);
     }
   }
   block_reduce_store<Op::NACC>(acc, Op::kinds(), partials, nblocks);
+  if constexpr (Op::kFusedControl) {
+    // last CTA to finish runs the attempt's control step (no waiting: the
+    // counter tells each CTA whether it is the last one)
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(&op.st->done_ctas, 1u) == (unsigned)nblocks - 1);
+    __syncthreads();
+    if (last) control_block(op.st, op.ctrl_px, op.ctrl_nbx, partials, nblocks);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -357,6 +446,7 @@ __device__ __constant__ int32_t kResid7[7] = {ACC_SUM, ACC_MAX, ACC_MAX, ACC_SUM
 // x = P(x_lag + ps (aty - c)); acc: sum (x - x_lag)^2
 struct OpPrimalStep {
   static constexpr int NACC = 1;
+  static constexpr bool kFusedControl = false;
   __device__ static const int32_t* kinds() { return kSum1; }
   const double* xl;
   const double* aty;
@@ -376,14 +466,17 @@ struct OpPrimalStep {
 // y = P(y_lag - ds (2 gx - gxl - h)); acc: sum (y - y_lag)^2, sum (y - y_lag)(gx - gxl)
 struct OpDualStep {
   static constexpr int NACC = 2;
+  static constexpr bool kFusedControl = true;
   __device__ static const int32_t* kinds() { return kSum2; }
   const double* yl;
   const double* gx;
   const double* gxl;
   const double* h;
   double* out;
-  const PdhgState* st;
+  PdhgState* st;
   double ds;
+  const double* ctrl_px;  // partials of the primal step (control step input)
+  int ctrl_nbx;
   __device__ void load() { ds = st->ds; }
   __device__ double z(int64_t i) const { return yl[i] - ds * ((2.0 * gx[i] - gxl[i]) - h[i]); }
   __device__ void fin(int64_t i, double, double p, double* acc) const {
@@ -398,6 +491,7 @@ struct OpDualStep {
 // [2] sum (out - base)*(g1 - g0) when g1 != NULL (restart binary search, Mnorm)
 struct OpAxpyProj {
   static constexpr int NACC = 3;
+  static constexpr bool kFusedControl = false;
   __device__ static const int32_t* kinds() { return kSum3; }
   const double* base;
   const double* dir;
@@ -422,6 +516,7 @@ struct OpAxpyProj {
 //      [4] max |a*u*su|, [5] sum |a*u*su|, [6] box dual objective contribution
 struct OpResidual {
   static constexpr int NACC = 7;
+  static constexpr bool kFusedControl = false;
   __device__ static const int32_t* kinds() { return kResid7; }
   const double* u;
   const double* su;

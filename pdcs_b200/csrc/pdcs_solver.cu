@@ -84,71 +84,11 @@ __global__ void __launch_bounds__(kThreads) dots_kernel(DotSpec spec, double* pa
   }
 }
 
-__global__ void control_kernel(PdhgState* st, const double* __restrict__ px, int nbx, const double* __restrict__ py,
-                               int nby) {
-  if (!st->active) {
-    if (threadIdx.x == 0) st->do_reflect = 0;
-    return;
-  }
-  __shared__ double sh[3][kThreads];
-  double a = 0.0, b = 0.0, c = 0.0;
-  for (int i = threadIdx.x; i < nbx; i += kThreads) a += px[i];
-  for (int i = threadIdx.x; i < nby; i += kThreads) {
-    b += py[i];
-    c += py[nby + i];
-  }
-  sh[0][threadIdx.x] = a;
-  sh[1][threadIdx.x] = b;
-  sh[2][threadIdx.x] = c;
-  __syncthreads();
-  for (int s = kThreads / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
-      sh[0][threadIdx.x] += sh[0][threadIdx.x + s];
-      sh[1][threadIdx.x] += sh[1][threadIdx.x + s];
-      sh[2][threadIdx.x] += sh[2][threadIdx.x + s];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x != 0) return;
-  PdhgState s = *st;
-  s.sum_dx2 = sh[0][0];
-  s.sum_dy2 = sh[1][0];
-  s.sum_dgdy = sh[2][0];
-  s.do_reflect = 0;
-  // eta_bar and eta' (rpdhg_alg_gpu_gen_scaling.jl:711-715)
-  double num = s.omega * s.sum_dx2 + s.sum_dy2 / s.omega;
-  double den = 2.0 * fabs(s.sum_dgdy);
-  s.eta_bar = num / (den + 1e-20);
-  s.iter += 1;
-  s.iter_stepsize += 1;
-  double k1 = (double)(s.iter_stepsize + 1);
-  s.eta_p = fmin((1.0 - pow(k1, -0.3)) * s.eta_bar, (1.0 + pow(k1, -0.6)) * s.eta);
-  s.tau = s.eta / s.omega;
-  s.sigma = s.eta * s.omega;
-  s.accepted = (s.eta <= s.eta_bar) ? 1 : 0;
-  if (s.check_freq > 0 && s.iter % s.check_freq == 0) {
-    s.halt_reason = HALT_CHECK;  // the host runs the exit check, then decides
-    s.active = 0;
-  } else if (s.attempt_limit > 0 && s.iter >= s.attempt_limit) {
-    s.halt_reason = HALT_LIMIT;
-    s.active = 0;
-  } else if (s.accepted) {
-    post_accept(s, false);
-  } else {
-    after_reject(s);
-    if (s.reject_count > 1000000) {
-      s.eta = s.eta_p;  // the forced return hands back the last eta (:757-764)
-      post_accept(s, true);
-    }
-  }
-  *st = s;
-}
-
 __global__ void __launch_bounds__(kThreads) reflect_kernel(PdhgState* st, double* __restrict__ x,
                                                            double* __restrict__ xl, double* __restrict__ xm,
                                                            int64_t n, double* __restrict__ y, double* __restrict__ yl,
                                                            double* __restrict__ ym, int64_t m) {
-  if (!st->do_reflect) return;
+  if (!st->do_reflect) return;  // set by this attempt's control step, cleared by the next attempt's first kernel
   const double tmp = st->refl_tmp, inv = st->refl_inv, e = st->refl_extra, eta = st->refl_eta, cum = st->refl_cum;
   const double wsum = cum + eta;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -620,7 +560,7 @@ void Solver::build_bins(const HostCsr& H, const int32_t* d_rp, const int32_t* d_
   for (int64_t i = 0; i < H.m; ++i) {
     int64_t L = H.rp[i + 1] - H.rp[i];
     int b;
-    if (L > 1024) b = kBins - 1;
+    if (L > 128) b = kBins - 1;  // CTA per row
     else {
       int g = 1;
       b = 0;
@@ -758,6 +698,12 @@ void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<i
   CON.exp_kind = PK_EXP;   // code 13
   CON.dexp_kind = PK_DEXP; // code 16
   CON.S = nullptr;
+  // per-cone warm starts of the exponential-cone root (NaN = none yet)
+  int64_t nxe = P.exp_x + P.dual_exp_x, nye = P.expG + P.dual_expG;
+  XI.rho_ws = A.alloc<double>(nxe);
+  YI.rho_ws = A.alloc<double>(nye);
+  PDCS_CUDA(cudaMemsetAsync(XI.rho_ws, 0xff, sizeof(double) * std::max<int64_t>(nxe, 1), s_));
+  PDCS_CUDA(cudaMemsetAsync(YI.rho_ws, 0xff, sizeof(double) * std::max<int64_t>(nye, 1), s_));
   size_table(XI);
   size_table(SLK);
   size_table(YI);
@@ -917,14 +863,14 @@ void Solver::capture_graph() {
   PDCS_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
   const int32_t* act = &st_dev->active;
   for (int a = 0; a < attempts_per_graph_; ++a) {
-    spmv_binned_kernel<1><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, yl, nullptr, aty, nullptr, act);
+    spmv_binned_kernel<1><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, yl, nullptr, aty, nullptr, act,
+                                                                &st_dev->do_reflect);
     OpPrimalStep op1{xl, aty, c_s, x, st_dev, 0.0};
     update_project_kernel<OpPrimalStep><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, act);
     spmv_binned_kernel<2><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, x, xl, gx, gxl, act);
-    OpDualStep op2{yl, gx, gxl, h_s, y, st_dev, 0.0};
+    // the dual step's last CTA runs the attempt's control step
+    OpDualStep op2{yl, gx, gxl, h_s, y, st_dev, 0.0, part_x, XI.ctaA + XI.ctaB + XI.ctaC};
     update_project_kernel<OpDualStep><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, act);
-    control_kernel<<<1, kThreads, 0, s_>>>(st_dev, part_x, XI.ctaA + XI.ctaB + XI.ctaC, part_y,
-                                           YI.ctaA + YI.ctaB + YI.ctaC);
     reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, x, xl, xm, n_, y, yl, ym, m_);
   }
   PDCS_CUDA(cudaStreamEndCapture(s_, &graph_));
@@ -1281,7 +1227,7 @@ void Solver::run_until_halt() {
     for (int64_t g = 0; g < graphs; ++g) {
       PDCS_CUDA(cudaGraphLaunch(graph_exec_, s_));
       graphs_++;
-      kernels_ += 6LL * attempts_per_graph_;
+      kernels_ += 5LL * attempts_per_graph_;
     }
     pull_state();
     if (!S.active) return;

@@ -243,3 +243,19 @@ def batch_socp_c3(count=4096, seed=20261206, nmin=50, nmax=5000, density=0.02):
                                    socG=socG, density=density, seed=seed + 1000 + k,
                                    name=f"batch_socp_{k}"))
     return out
+
+
+def primal_infeasible_lp():
+    """x1 + x2 >= 1 and -x1 - x2 >= 0 with x free: no feasible point."""
+    G = sp.csr_matrix(np.array([[1.0, 1.0], [-1.0, -1.0], [1.0, 0.0]]))
+    return ConicProblem(n=2, m=3, nb=2, c=np.array([1.0, 1.0]), G=G, h=np.array([1.0, 0.0, -5.0]),
+                        mGzero=0, mGnonnegative=3, bl=np.full(2, -np.inf), bu=np.full(2, np.inf),
+                        name="primal_infeasible_lp")
+
+
+def dual_infeasible_lp():
+    """min -x1 s.t. x1 - x2 >= 0, x2 >= 0, x free: unbounded below."""
+    G = sp.csr_matrix(np.array([[1.0, -1.0], [0.0, 1.0]]))
+    return ConicProblem(n=2, m=2, nb=2, c=np.array([-1.0, 0.0]), G=G, h=np.zeros(2),
+                        mGzero=0, mGnonnegative=2, bl=np.full(2, -np.inf), bu=np.full(2, np.inf),
+                        name="dual_infeasible_lp")

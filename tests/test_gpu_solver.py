@@ -79,3 +79,14 @@ def test_kkt_restart_variant(cuda):
     o = B.solve(p, threads=2, use_kkt_restart=1, use_duality_gap_restart=0)
     assert g.info.exit_status == "optimal" and o["exit_code"] == 0
     assert abs(g.info.pObj - o["primal_objective"]) <= 2e-6 * (1 + abs(o["primal_objective"]))
+
+
+@pytest.mark.parametrize("name", ["primal_infeasible_lp", "dual_infeasible_lp"])
+def test_infeasibility_status_matches_oracle(cuda, name):
+    p = getattr(problems, name)()
+    g = solver.solve_problem(p, time_limit=60)
+    o = B.solve(p, threads=1, time_limit=60)
+    # same certificate class (primal: 2/3, dual: 4/5); the low/high accuracy
+    # label depends on objective trends that differ with rounding
+    cls = {2: "primal", 3: "primal", 4: "dual", 5: "dual"}
+    assert cls.get(g.info.exit_code) == cls.get(o["exit_code"]) is not None, (g.info.exit_code, o["exit_code"])

@@ -57,3 +57,10 @@ def test_preconditioner_equilibrates():
     assert np.all(np.isfinite(Dr)) and np.all(Dr > 0) and np.all(Dl > 0)
     nz = rowmax > 0
     assert np.median(rowmax[nz]) < 2.0
+
+
+@pytest.mark.parametrize("name,code", [("primal_infeasible_lp", 2), ("dual_infeasible_lp", 5)])
+def test_oracle_infeasibility_certificates(name, code):
+    p = getattr(problems, name)()
+    r = B.solve(p, threads=1, time_limit=60)
+    assert r["exit_code"] == code
