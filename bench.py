@@ -279,7 +279,7 @@ def run_ours(args):
             dist.all_reduce(ii, op=dist.ReduceOp.SUM)
             eit = int(ii[0])
         e2e = {"value": eit / et, "unit": "iter/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "ms_per_step": 1e3 * et / args.steps}
+               "ms_per_step": 1e3 * et / args.steps, "iterations_per_solve": sol_h.info.iter}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -295,6 +295,8 @@ def run_ours(args):
                 "kkt": {"l_inf_rel_primal_res": last.l_inf_rel_primal_res,
                         "l_inf_rel_dual_res": last.l_inf_rel_dual_res, "rel_gap": last.rel_gap},
                 "setup_ms": last.setup_time * 1e3,
+                "breakdown_ms": {"iterations": last.time_iterations * 1e3, "exit_checks": last.time_exit_checks * 1e3,
+                                 "restarts": last.time_restarts * 1e3, "restart_probes": last.restart_probes},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
                 "roofline": roofline, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)

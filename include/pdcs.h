@@ -125,6 +125,10 @@ typedef struct {
   double l_inf_abs_primal_res, l_inf_abs_dual_res, abs_gap;
   int64_t kernel_launches;   /* kernels launched by the library in the main loop */
   int64_t graph_launches;
+  double time_iterations;    /* seconds in PDHG attempts (CUDA graphs)            */
+  double time_exit_checks;   /* seconds in termination checks (every check_terminate_freq) */
+  double time_restarts;      /* seconds in restart thresholds / restart checks    */
+  int64_t restart_probes;    /* projections probes of the restart binary searches */
 } pdcs_result;
 
 /* Fills *opts with the reference's defaults. */

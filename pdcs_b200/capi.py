@@ -77,7 +77,9 @@ class PdcsResult(C.Structure):
                 ("rel_gap", C.c_double), ("l_2_rel_primal_res", C.c_double),
                 ("l_2_rel_dual_res", C.c_double), ("l_inf_abs_primal_res", C.c_double),
                 ("l_inf_abs_dual_res", C.c_double), ("abs_gap", C.c_double),
-                ("kernel_launches", C.c_int64), ("graph_launches", C.c_int64)]
+                ("kernel_launches", C.c_int64), ("graph_launches", C.c_int64),
+                ("time_iterations", C.c_double), ("time_exit_checks", C.c_double),
+                ("time_restarts", C.c_double), ("restart_probes", C.c_int64)]
 
 
 # every symbol declared in include/pdcs.h

@@ -19,6 +19,7 @@
 
 #include "../../include/pdcs.h"
 #include "pdcs_kernels.cuh"
+#include "pdcs_preprocess.cuh"
 
 namespace pdcs {
 
@@ -336,32 +337,6 @@ struct Arena {
   }
 };
 
-struct HostCsr {
-  int64_t m = 0, n = 0;
-  std::vector<int32_t> rp, ci;
-  std::vector<double> v;
-};
-
-static HostCsr transpose(const HostCsr& A) {
-  HostCsr T;
-  T.m = A.n;
-  T.n = A.m;
-  T.rp.assign(A.n + 1, 0);
-  const int64_t nnz = A.rp[A.m];
-  T.ci.resize(nnz);
-  T.v.resize(nnz);
-  for (int64_t k = 0; k < nnz; ++k) T.rp[A.ci[k] + 1]++;
-  for (int64_t j = 0; j < A.n; ++j) T.rp[j + 1] += T.rp[j];
-  std::vector<int32_t> pos(T.rp.begin(), T.rp.end() - 1);
-  for (int64_t i = 0; i < A.m; ++i)
-    for (int32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-      int32_t q = pos[A.ci[k]]++;
-      T.ci[q] = (int32_t)i;
-      T.v[q] = A.v[k];
-    }
-  return T;
-}
-
 struct Converge {
   double pobj = 1e30, dobj = 1e30, abs_gap = 1e30, rel_gap = 1e30;
   double linf_rel_p = 1e30, linf_rel_d = 1e30, l2_rel_p = 1e30, l2_rel_d = 1e30;
@@ -405,6 +380,7 @@ class Solver {
   double *tn[6] = {}, *tm[6] = {};
   double *xds_ = nullptr, *yds_ = nullptr;  // iterates at the start of an outer iteration (omega update)
   double *part_x = nullptr, *part_y = nullptr, *part_r = nullptr, *red_out = nullptr;
+  double *part_a = nullptr, *part_b = nullptr;  // partials of host-driven (non-graph) reductions
   PdhgState* st_dev = nullptr;
   PdhgState* host_state_ = nullptr;
   double* host_red_ = nullptr;
@@ -428,12 +404,23 @@ class Solver {
   double bs_t0_ = 1.0;
   int64_t restart_used_ = 0, check_count_ = 0;
   double t_start_ = 0;
-  int64_t kernels_ = 0, graphs_ = 0;
+  int64_t kernels_ = 0, graphs_ = 0, probes_ = 0;
+  double t_iter_ = 0, t_exit_ = 0, t_restart_ = 0;
+  struct Timer {
+    double& acc;
+    double t0;
+    explicit Timer(double& a) : acc(a), t0(now_s()) {}
+    ~Timer() { acc += now_s() - t0; }
+  };
 
   // ---- setup ----
   int validate();
   void setup();
-  void build_bins(const HostCsr& H, const int32_t* d_rp, const int32_t* d_ci, const double* d_v, CsrDev& D);
+  void build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
+                  const int32_t* d_ci, const double* d_v, CsrDev& D);
+  int warp_grid(int64_t rows) const {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((rows * 32 + kThreads - 1) / kThreads, 148 * 16));
+  }
   void build_tables(const std::vector<int64_t>& soc_x, const std::vector<int64_t>& rsoc_x,
                     const std::vector<int64_t>& socG, const std::vector<int64_t>& rsocG);
   void size_table(ConeTable& T);
@@ -491,6 +478,37 @@ class Solver {
     dots(d, &v);
     return std::sqrt(v);
   }
+  // ---- asynchronous reductions: results land in slots of red_out, fetched together ----
+  void finalize_async(const double* partials, int nblocks, int nacc, uint32_t maxmask, int slot) {
+    finalize_partials_kernel2<<<nacc, kThreads, 0, s_>>>(partials, nblocks, nacc, maxmask, red_out + slot);
+    kernels_++;
+  }
+  void dots_async(DotSpec spec, double* partials, int slot) {
+    int g = grid_for(spec.len);
+    uint32_t mask = 0;
+    for (int k = spec.count; k < 4; ++k) {
+      spec.a[k] = spec.a[0];
+      spec.b[k] = nullptr;
+      spec.sa[k] = nullptr;
+      spec.kind[k] = DK_DOT;
+    }
+    for (int k = 0; k < 4; ++k)
+      if (spec.kind[k] == DK_MAXABS) mask |= 1u << k;
+    dots_kernel<<<g, kThreads, 0, s_>>>(spec, partials);
+    kernels_++;
+    finalize_async(partials, g, spec.count, mask, slot);
+  }
+  const double* fetch(int count) {
+    PDCS_CUDA(cudaMemcpyAsync(host_red_, red_out, sizeof(double) * count, cudaMemcpyDeviceToHost, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    return host_red_;
+  }
+  template <class Op>
+  int launch_project(const Op& op, const ConeTable& T, double* partials) {
+    update_project(op, T, partials);
+    return T.ctaA + T.ctaB + T.ctaC;
+  }
+
   void push_state() {
     // synchronous w.r.t. the pinned staging buffer, which the next push reuses
     *host_state_ = S;
@@ -549,16 +567,17 @@ int Solver::validate() {
   return PDCS_OK;
 }
 
-void Solver::build_bins(const HostCsr& H, const int32_t* d_rp, const int32_t* d_ci, const double* d_v, CsrDev& D) {
-  D.m = H.m;
-  D.n = H.n;
-  D.nnz = H.rp[H.m];
+void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
+                        const int32_t* d_ci, const double* d_v, CsrDev& D) {
+  D.m = rows;
+  D.n = cols;
+  D.nnz = rp[rows];
   D.rp = d_rp;
   D.ci = d_ci;
   D.v = d_v;
   std::vector<std::vector<int32_t>> bins(kBins);
-  for (int64_t i = 0; i < H.m; ++i) {
-    int64_t L = H.rp[i + 1] - H.rp[i];
+  for (int64_t i = 0; i < rows; ++i) {
+    int64_t L = rp[i + 1] - rp[i];
     int b;
     if (L > 128) b = kBins - 1;  // CTA per row
     else {
@@ -572,7 +591,7 @@ void Solver::build_bins(const HostCsr& H, const int32_t* d_rp, const int32_t* d_
     bins[b].push_back((int32_t)i);
   }
   std::vector<int32_t> perm;
-  perm.reserve(H.m);
+  perm.reserve(rows);
   int64_t off = 0;
   int32_t cta = 0;
   for (int b = 0; b < kBins; ++b) {
@@ -722,125 +741,149 @@ void Solver::setup() {
     own_stream_ = true;
   }
   PDCS_CUDA(cudaMallocHost(&host_state_, sizeof(PdhgState)));
-  PDCS_CUDA(cudaMallocHost(&host_red_, 16 * sizeof(double)));
-  // ---- host copies of the problem ----
-  HostCsr H;
-  H.m = m_;
-  H.n = n_;
-  H.rp.resize(m_ + 1);
-  H.ci.resize(nnz_);
-  H.v.resize(nnz_);
-  std::vector<double> c(n_), h(m_), bl(nb_), bu(nb_);
-  auto get = [&](void* dst, const void* src, size_t bytes) {
-    if (bytes == 0) return;
-    if (P.on_device) PDCS_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
-    else std::memcpy(dst, src, bytes);
-  };
-  get(H.rp.data(), P.G_rowptr, sizeof(int32_t) * (m_ + 1));
-  get(H.ci.data(), P.G_colind, sizeof(int32_t) * nnz_);
-  get(H.v.data(), P.G_val, sizeof(double) * nnz_);
-  get(c.data(), P.c, sizeof(double) * n_);
-  get(h.data(), P.h, sizeof(double) * m_);
-  get(bl.data(), P.bl, sizeof(double) * nb_);
-  get(bu.data(), P.bu, sizeof(double) * nb_);
-  if (H.rp[0] != 0 || H.rp[m_] != nnz_) throw std::invalid_argument("rowptr");
-  for (int64_t j = 0; j < nb_; ++j)
-    if (!(bl[j] <= bu[j])) throw std::domain_error("bounds");
-  for (int64_t k = 0; k < nnz_; ++k)
-    if (H.ci[k] < 0 || H.ci[k] >= n_) throw std::invalid_argument("colind");
-  // raw norms (cal_constant, def_struct.jl:968-976)
-  for (double v : h) { hNrm1 += std::fabs(v); hNrmInf = std::max(hNrmInf, std::fabs(v)); }
-  for (double v : c) { cNrm1 += std::fabs(v); cNrmInf = std::max(cNrmInf, std::fabs(v)); }
-  std::vector<double> c_raw_h = c, h_raw_h = h, bl_fin_h(nb_), bu_fin_h(nb_), lam_l_h(nb_), lam_u_h(nb_);
-  const double inf = INFINITY;
-  for (int64_t j = 0; j < nb_; ++j) {
-    bl_fin_h[j] = std::isinf(bl[j]) ? 0.0 : bl[j];
-    bu_fin_h[j] = std::isinf(bu[j]) ? 0.0 : bu[j];
-    lam_l_h[j] = (bu[j] == inf) ? 0.0 : -inf;  // gen_lambd, def_rpdhg_gen.jl:5-17
-    lam_u_h[j] = (bl[j] == -inf) ? 0.0 : inf;
-  }
-  // ---- Ruiz (10) + Pock-Chambolle (alpha = 1) equilibration (preprocess.jl:347-591) ----
-  std::vector<double> Drh(n_, 1.0), Dlh(m_, 1.0);
-  auto scale_data = [&](const std::vector<double>& var, const std::vector<double>& con) {
-    for (int64_t j = 0; j < n_; ++j) { c[j] /= var[j]; Drh[j] *= var[j]; }
-    for (int64_t j = 0; j < nb_; ++j) { bl[j] *= var[j]; bu[j] *= var[j]; }
-    for (int64_t i = 0; i < m_; ++i) {
-      h[i] /= con[i];
-      Dlh[i] *= con[i];
-      for (int32_t k = H.rp[i]; k < H.rp[i + 1]; ++k) H.v[k] /= (con[i] * var[H.ci[k]]);
-    }
-  };
-  int method = O.rescaling_method;
-  if (method == 1 || method == 3) {
-    for (int it = 0; it < 10; ++it) {
-      std::vector<double> var(n_, 0.0), con(m_, 0.0);
-      for (int64_t i = 0; i < m_; ++i)
-        for (int32_t k = H.rp[i]; k < H.rp[i + 1]; ++k) {
-          double a = std::fabs(H.v[k]);
-          con[i] = std::max(con[i], a);
-          var[H.ci[k]] = std::max(var[H.ci[k]], a);
-        }
-      for (auto& v : var) v = (v == 0.0) ? 1.0 : std::sqrt(v);
-      for (auto& v : con) v = (v == 0.0) ? 1.0 : std::sqrt(v);
-      scale_data(var, con);
-    }
-  }
-  if (method == 2 || method == 3) {
-    std::vector<double> var(n_, 0.0), con(m_, 0.0);
-    for (int64_t i = 0; i < m_; ++i)
-      for (int32_t k = H.rp[i]; k < H.rp[i + 1]; ++k) {
-        double a = std::fabs(H.v[k]);
-        con[i] += a;
-        var[H.ci[k]] += a;
-      }
-    for (auto& v : var) v = (v == 0.0) ? 1.0 : std::sqrt(v);
-    for (auto& v : con) v = (v == 0.0) ? 1.0 : std::sqrt(v);
-    scale_data(var, con);
-  }
-  ginf_ = 0.0;
-  for (double v : H.v) ginf_ = std::max(ginf_, std::fabs(v));
-  HostCsr Ht = transpose(H);
-  // ---- upload ----
-  auto up = [&](auto* dst, const auto& vec) {
-    if (!vec.empty())
-      PDCS_CUDA(cudaMemcpyAsync(dst, vec.data(), vec.size() * sizeof(vec[0]), cudaMemcpyHostToDevice, s_));
-  };
+  PDCS_CUDA(cudaMallocHost(&host_red_, 64 * sizeof(double)));
+  part_r = A.alloc<double>((size_t)148 * 8 * 8);
+  red_out = A.alloc<double>(64);
+  // ---- raw problem data on the device (copied: the caller's buffers are never modified) ----
   int32_t* g_rp = A.alloc<int32_t>(m_ + 1);
   int32_t* g_ci = A.alloc<int32_t>(nnz_);
   double* g_v = A.alloc<double>(nnz_);
+  c_raw = A.alloc<double>(n_);
+  h_raw = A.alloc<double>(m_);
+  double* bl_raw = A.alloc<double>(nb_);
+  double* bu_raw = A.alloc<double>(nb_);
+  const cudaMemcpyKind kind = P.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  auto put = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes) PDCS_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, s_));
+  };
+  put(g_rp, P.G_rowptr, sizeof(int32_t) * (m_ + 1));
+  put(g_ci, P.G_colind, sizeof(int32_t) * nnz_);
+  put(g_v, P.G_val, sizeof(double) * nnz_);
+  put(c_raw, P.c, sizeof(double) * n_);
+  put(h_raw, P.h, sizeof(double) * m_);
+  put(bl_raw, P.bl, sizeof(double) * nb_);
+  put(bu_raw, P.bu, sizeof(double) * nb_);
+  // ---- input checks ----
+  int32_t* d_err = A.alloc<int32_t>(1);
+  PDCS_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int32_t), s_));
+  check_inputs_kernel<<<grid_for(std::max(std::max(m_, nnz_), nb_)), kThreads, 0, s_>>>(m_, n_, nnz_, nb_, g_rp, g_ci,
+                                                                                        bl_raw, bu_raw, d_err);
+  int32_t* h_err = reinterpret_cast<int32_t*>(host_red_);
+  PDCS_CUDA(cudaMemcpyAsync(h_err, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  if (*h_err & IE_BOUNDS) throw std::domain_error("bounds");
+  if (*h_err) throw std::invalid_argument("csr");
+  // raw norms (cal_constant, def_struct.jl:968-976)
+  {
+    DotSpec d{};
+    d.a[0] = h_raw; d.kind[0] = DK_SUMABS;
+    d.a[1] = h_raw; d.kind[1] = DK_MAXABS;
+    d.count = 2; d.len = m_;
+    double r[2];
+    dots(d, r);
+    hNrm1 = r[0];
+    hNrmInf = r[1];
+    DotSpec e{};
+    e.a[0] = c_raw; e.kind[0] = DK_SUMABS;
+    e.a[1] = c_raw; e.kind[1] = DK_MAXABS;
+    e.count = 2; e.len = n_;
+    dots(e, r);
+    cNrm1 = r[0];
+    cNrmInf = r[1];
+  }
+  // ---- G' structure: stable radix sort of the column keys keeps G's row order ----
+  int32_t* row_of = A.alloc<int32_t>(nnz_);
   int32_t* t_rp = A.alloc<int32_t>(n_ + 1);
+  int32_t* col_cnt = A.alloc<int32_t>(n_ + 1);
+  int32_t* keys_sorted = A.alloc<int32_t>(nnz_);
+  int32_t* perm_in = A.alloc<int32_t>(nnz_);
+  int32_t* perm_t = A.alloc<int32_t>(nnz_);
+  PDCS_CUDA(cudaMemsetAsync(col_cnt, 0, sizeof(int32_t) * (n_ + 1), s_));
+  expand_rows_kernel<<<warp_grid(m_), kThreads, 0, s_>>>(m_, g_rp, g_ci, row_of, col_cnt);
+  iota_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(perm_in, nnz_);
+  {
+    size_t b1 = 0, b2 = 0;
+    int bits = 1;
+    while ((int64_t(1) << bits) <= n_) ++bits;
+    PDCS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b1, col_cnt, t_rp, (int)(n_ + 1), s_));
+    PDCS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b2, g_ci, keys_sorted, perm_in, perm_t, (int)nnz_, 0, bits,
+                                              s_));
+    void* tmp = A.alloc<char>(std::max(b1, b2));
+    PDCS_CUDA(cub::DeviceScan::ExclusiveSum(tmp, b1, col_cnt, t_rp, (int)(n_ + 1), s_));
+    if (nnz_ > 0)
+      PDCS_CUDA(cub::DeviceRadixSort::SortPairs(tmp, b2, g_ci, keys_sorted, perm_in, perm_t, (int)nnz_, 0, bits, s_));
+  }
+  // ---- Ruiz (10) + Pock-Chambolle (alpha = 1) equilibration on the device ----
+  c_s = A.alloc<double>(n_);
+  Dr = A.alloc<double>(n_);
+  h_s = A.alloc<double>(m_);
+  Dl = A.alloc<double>(m_);
+  bl_s = A.alloc<double>(nb_);
+  bu_s = A.alloc<double>(nb_);
+  copy(c_s, c_raw, n_);
+  copy(h_s, h_raw, m_);
+  copy(bl_s, bl_raw, nb_);
+  copy(bu_s, bu_raw, nb_);
+  fill_kernel<<<grid_for(n_), kThreads, 0, s_>>>(Dr, 1.0, n_);
+  fill_kernel<<<grid_for(m_), kThreads, 0, s_>>>(Dl, 1.0, m_);
+  double* var = A.alloc<double>(n_);
+  double* con = A.alloc<double>(m_);
+  auto pass = [&](bool sum) {
+    if (sum) {
+      row_absstat_kernel<true><<<warp_grid(m_), kThreads, 0, s_>>>(m_, g_rp, g_v, nullptr, con);
+      row_absstat_kernel<true><<<warp_grid(n_), kThreads, 0, s_>>>(n_, t_rp, g_v, perm_t, var);
+    } else {
+      row_absstat_kernel<false><<<warp_grid(m_), kThreads, 0, s_>>>(m_, g_rp, g_v, nullptr, con);
+      row_absstat_kernel<false><<<warp_grid(n_), kThreads, 0, s_>>>(n_, t_rp, g_v, perm_t, var);
+    }
+    sqrt_or_one_kernel<<<grid_for(m_), kThreads, 0, s_>>>(con, m_);
+    sqrt_or_one_kernel<<<grid_for(n_), kThreads, 0, s_>>>(var, n_);
+    scale_matrix_kernel<<<warp_grid(m_), kThreads, 0, s_>>>(m_, g_rp, g_ci, g_v, con, var);
+    scale_vectors_kernel<<<grid_for(std::max(n_, m_)), kThreads, 0, s_>>>(n_, nb_, m_, var, con, c_s, Dr, bl_s, bu_s,
+                                                                        h_s, Dl);
+  };
+  int method = O.rescaling_method;
+  if (method == 1 || method == 3)
+    for (int it = 0; it < 10; ++it) pass(false);
+  if (method == 2 || method == 3) pass(true);
   int32_t* t_ci = A.alloc<int32_t>(nnz_);
   double* t_v = A.alloc<double>(nnz_);
-  up(g_rp, H.rp);
-  up(g_ci, H.ci);
-  up(g_v, H.v);
-  up(t_rp, Ht.rp);
-  up(t_ci, Ht.ci);
-  up(t_v, Ht.v);
-  build_bins(H, g_rp, g_ci, g_v, G_);
-  build_bins(Ht, t_rp, t_ci, t_v, Gt_);
-  auto vecn = [&]() { return A.alloc<double>(n_); };
-  auto vecm = [&]() { return A.alloc<double>(m_); };
-  c_s = vecn(); c_raw = vecn(); Dr = vecn();
-  h_s = vecm(); h_raw = vecm(); Dl = vecm();
-  bl_s = A.alloc<double>(nb_); bu_s = A.alloc<double>(nb_);
+  gather_transpose_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(nnz_, perm_t, row_of, g_v, t_ci, t_v);
+  {
+    DotSpec d{};
+    d.a[0] = g_v; d.kind[0] = DK_MAXABS;
+    d.count = 1; d.len = nnz_;
+    dots(d, &ginf_);
+  }
   lam_l = A.alloc<double>(nb_); lam_u = A.alloc<double>(nb_);
   bl_fin = A.alloc<double>(nb_); bu_fin = A.alloc<double>(nb_);
-  up(c_s, c); up(c_raw, c_raw_h); up(Dr, Drh);
-  up(h_s, h); up(h_raw, h_raw_h); up(Dl, Dlh);
-  up(bl_s, bl); up(bu_s, bu); up(lam_l, lam_l_h); up(lam_u, lam_u_h); up(bl_fin, bl_fin_h); up(bu_fin, bu_fin_h);
+  if (nb_ > 0)
+    box_aux_kernel<<<grid_for(nb_), kThreads, 0, s_>>>(nb_, bl_raw, bu_raw, bl_fin, bu_fin, lam_l, lam_u);
+  // ---- SpMV row bins (host sees only the two row-pointer arrays) ----
+  std::vector<int32_t> rp_h(m_ + 1), trp_h(n_ + 1);
+  PDCS_CUDA(cudaMemcpyAsync(rp_h.data(), g_rp, sizeof(int32_t) * (m_ + 1), cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaMemcpyAsync(trp_h.data(), t_rp, sizeof(int32_t) * (n_ + 1), cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  build_bins(rp_h, m_, n_, g_rp, g_ci, g_v, G_);
+  build_bins(trp_h, n_, m_, t_rp, t_ci, t_v, Gt_);
+  // ---- iterates and work vectors ----
+  auto vecn = [&]() { return A.alloc<double>(n_); };
+  auto vecm = [&]() { return A.alloc<double>(m_); };
   x = vecn(); xl = vecn(); xm = vecn(); aty = vecn(); x0 = vecn(); x0l = vecn(); xbest = vecn();
   y = vecm(); yl = vecm(); ym = vecm(); gx = vecm(); gxl = vecm(); y0 = vecm(); y0l = vecm(); ybest = vecm();
   for (int k = 0; k < 6; ++k) { tn[k] = vecn(); tm[k] = vecm(); }
   xds_ = vecn();
   yds_ = vecm();
-  // initial point (zeros, or the scaled warm start)
-  std::vector<double> x_init(n_, 0.0), y_init(m_, 0.0);
+  // initial point: zeros, or the warm start scaled into the preconditioned space
   if (O.warm_start && O.primal_sol && O.dual_sol) {
-    for (int64_t j = 0; j < n_; ++j) x_init[j] = O.primal_sol[j] * Drh[j];
-    for (int64_t i = 0; i < m_; ++i) y_init[i] = O.dual_sol[i] * Dlh[i];
+    PDCS_CUDA(cudaMemcpyAsync(x, O.primal_sol, sizeof(double) * n_, cudaMemcpyHostToDevice, s_));
+    PDCS_CUDA(cudaMemcpyAsync(y, O.dual_sol, sizeof(double) * m_, cudaMemcpyHostToDevice, s_));
+    mul_kernel<<<grid_for(n_), kThreads, 0, s_>>>(x, Dr, n_);
+    mul_kernel<<<grid_for(m_), kThreads, 0, s_>>>(y, Dl, m_);
+  } else {
+    if (n_) PDCS_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n_, s_));
+    if (m_) PDCS_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * m_, s_));
   }
-  up(x, x_init); up(y, y_init);
   copy(xl, x, n_); copy(xm, x, n_); copy(xbest, x, n_);
   copy(yl, y, m_); copy(ym, y, m_); copy(ybest, y, m_);
   // cone tables
@@ -852,8 +895,10 @@ void Solver::setup() {
   part_x = A.alloc<double>((size_t)maxgrid * 8);
   part_y = A.alloc<double>((size_t)maxgrid * 8);
   part_r = A.alloc<double>((size_t)maxgrid * 8);
-  red_out = A.alloc<double>(16);
+  part_a = A.alloc<double>((size_t)maxgrid * 8);
+  part_b = A.alloc<double>((size_t)maxgrid * 8);
   st_dev = A.alloc<PdhgState>(1);
+  PDCS_CUDA(cudaMemsetAsync(st_dev, 0, sizeof(PdhgState), s_));
   grid_reflect_ = grid_for(std::max(n_, m_));
   attempts_per_graph_ = O.attempts_per_graph > 0 ? O.attempts_per_graph : 32;
   PDCS_CUDA(cudaStreamSynchronize(s_));
@@ -882,26 +927,21 @@ void Solver::capture_graph() {
 void Solver::converge_info(const double* xs, const double* ys, Converge& C, double* gxs, double* atys) {
   spmv(G_, xs, gxs);
   spmv(Gt_, ys, atys);
-  double rp[7], rd[7];
   OpResidual opp{gxs, Dl, 1.0, nullptr, 0.0, h_raw, tm[5], bl_fin, bu_fin, 0};
-  update_project(opp, CON, part_r);
-  finalize(part_r, CON.ctaA + CON.ctaB + CON.ctaC, 7, 0b0010110u, rp);
+  finalize_async(part_a, launch_project(opp, CON, part_a), 7, 0b0010110u, 0);
   OpResidual opd{atys, Dr, -1.0, c_raw, 1.0, nullptr, tn[5], bl_fin, bu_fin, nb_};
-  update_project(opd, SLK, part_r);
-  finalize(part_r, SLK.ctaA + SLK.ctaB + SLK.ctaC, 7, 0b0010110u, rd);
+  finalize_async(part_b, launch_project(opd, SLK, part_b), 7, 0b0010110u, 7);
   DotSpec d1{};
-  d1.a[0] = c_raw; d1.b[0] = xs; d1.sa[0] = Dr; d1.kind[0] = DK_DOT;  // c'(x~/Dr), divisor applies to a
-  d1.count = 1;
-  d1.len = n_;
-  double pobj;
-  dots(d1, &pobj);
-  // c_raw_j * x_j / Dr_j : the divisor is on a, a = c_raw, so (c_raw/Dr)*x~ -- same value
+  d1.a[0] = c_raw; d1.b[0] = xs; d1.sa[0] = Dr; d1.kind[0] = DK_DOT;  // c_raw' (x~ / Dr)
+  d1.count = 1; d1.len = n_;
+  dots_async(d1, part_r, 14);
   DotSpec d2{};
-  d2.a[0] = h_raw; d2.b[0] = ys; d2.sa[0] = Dl; d2.kind[0] = DK_DOT;
-  d2.count = 1;
-  d2.len = m_;
-  double hy;
-  dots(d2, &hy);
+  d2.a[0] = h_raw; d2.b[0] = ys; d2.sa[0] = Dl; d2.kind[0] = DK_DOT;  // h_raw' (y~ / Dl)
+  d2.count = 1; d2.len = m_;
+  dots_async(d2, part_x, 15);
+  const double* r = fetch(16);
+  const double *rp = r, *rd = r + 7;
+  double pobj = r[14], hy = r[15];
   double dobj = hy + rd[6];
   C.pobj = pobj;
   C.dobj = dobj;
@@ -921,6 +961,7 @@ void Solver::converge_info(const double* xs, const double* ys, Converge& C, doub
 
 // exit_condition_check_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:309-352)
 void Solver::exit_check() {
+  Timer tm_(t_exit_);
   double *gxc = tm[0], *gxm = tm[1], *atc = tn[0], *atm = tn[1];
   converge_info(x, y, ci[0], gxc, atc);
   converge_info(xm, ym, ci[1], gxm, atm);
@@ -928,16 +969,6 @@ void Solver::exit_check() {
   // infeasibility information (rpdhg_alg_gpu_gen_scaling.jl:185-248).  For the
   // current iterate the rays are the iterates themselves, so the ray
   // infeasibilities equal the residuals just computed.
-  auto ray_norms = [&](const double* xr, const double* yr, Infea& I) {
-    DotSpec a{};
-    a.a[0] = xr; a.sa[0] = Dr; a.kind[0] = DK_MAXABS;
-    a.count = 1; a.len = n_;
-    dots(a, &I.primal_ray_norm);
-    DotSpec b{};
-    b.a[0] = yr; b.sa[0] = Dl; b.kind[0] = DK_MAXABS;
-    b.count = 1; b.len = m_;
-    dots(b, &I.dual_ray_norm);
-  };
   auto push_trend = [&](Infea& I) {
     if (check_count_ % 4 == 1) {  // the reference pushes with probability 1/4
       I.ptrend.push_back(ci[0].pobj);
@@ -946,52 +977,52 @@ void Solver::exit_check() {
       if (I.dtrend.size() > 20) I.dtrend.erase(I.dtrend.begin());
     }
   };
+  // ray = current - average; G and G' of the difference by linearity
+  double* dxs = tn[2];
+  double* dys = tm[2];
+  double* gd = tm[3];
+  double* ad = tn[3];
+  axpby(dxs, 1.0, x, -1.0, xm, n_);
+  axpby(dys, 1.0, y, -1.0, ym, m_);
+  axpby(gd, 1.0, gxc, -1.0, gxm, m_);
+  axpby(ad, 1.0, atc, -1.0, atm, n_);
+  DotSpec a{};  // n-length: |x/Dr|_inf, |dx/Dr|_inf, c'(dx/Dr)
+  a.a[0] = x; a.sa[0] = Dr; a.kind[0] = DK_MAXABS;
+  a.a[1] = dxs; a.sa[1] = Dr; a.kind[1] = DK_MAXABS;
+  a.a[2] = c_raw; a.b[2] = dxs; a.sa[2] = Dr; a.kind[2] = DK_DOT;
+  a.count = 3; a.len = n_;
+  dots_async(a, part_r, 0);
+  DotSpec b{};  // m-length: |y/Dl|_inf, |dy/Dl|_inf, h'(dy/Dl)
+  b.a[0] = y; b.sa[0] = Dl; b.kind[0] = DK_MAXABS;
+  b.a[1] = dys; b.sa[1] = Dl; b.kind[1] = DK_MAXABS;
+  b.a[2] = h_raw; b.b[2] = dys; b.sa[2] = Dl; b.kind[2] = DK_DOT;
+  b.count = 3; b.len = m_;
+  dots_async(b, part_x, 3);
+  OpResidual opp{gd, Dl, 1.0, nullptr, 0.0, h_raw, tm[5], bl_fin, bu_fin, 0};
+  finalize_async(part_a, launch_project(opp, CON, part_a), 7, 0b0010110u, 6);
+  OpResidual opd{ad, Dr, -1.0, c_raw, 1.0, nullptr, tn[5], bl_fin, bu_fin, nb_};
+  finalize_async(part_b, launch_project(opd, SLK, part_b), 7, 0b0010110u, 13);
+  const double* r = fetch(20);
   {
     Infea& I = ii[0];
     I.primal_ray_obj = ci[0].pobj;
     I.dual_ray_obj = ci[0].dobj;
     I.max_primal_ray_inf = (ci[0].pobj < 0.0) ? ci[0].linf_abs_p : 1e10;
     I.max_dual_ray_inf = (ci[0].dobj > 0.0) ? ci[0].linf_abs_d : 1e10;
-    ray_norms(x, y, I);
+    I.primal_ray_norm = r[0];
+    I.dual_ray_norm = r[3];
     push_trend(I);
   }
   {
-    // ray = current - average
     Infea& I = ii[1];
-    double* dxs = tn[2];
-    double* dys = tm[2];
-    axpby(dxs, 1.0, x, -1.0, xm, n_);
-    axpby(dys, 1.0, y, -1.0, ym, m_);
-    double* gd = tm[3];
-    double* ad = tn[3];
-    axpby(gd, 1.0, gxc, -1.0, gxm, m_);
-    axpby(ad, 1.0, atc, -1.0, atm, n_);
-    DotSpec d1{};
-    d1.a[0] = c_raw; d1.b[0] = dxs; d1.sa[0] = Dr; d1.kind[0] = DK_DOT;
-    d1.count = 1; d1.len = n_;
-    double pobj;
-    dots(d1, &pobj);
-    double rp[7], rd[7];
-    I.max_primal_ray_inf = 1e10;
-    if (pobj < 0.0) {
-      OpResidual opp{gd, Dl, 1.0, nullptr, 0.0, h_raw, tm[5], bl_fin, bu_fin, 0};
-      update_project(opp, CON, part_r);
-      finalize(part_r, CON.ctaA + CON.ctaB + CON.ctaC, 7, 0b0010110u, rp);
-      I.max_primal_ray_inf = rp[1];
-    }
-    DotSpec d2{};
-    d2.a[0] = h_raw; d2.b[0] = dys; d2.sa[0] = Dl; d2.kind[0] = DK_DOT;
-    d2.count = 1; d2.len = m_;
-    double hy;
-    dots(d2, &hy);
-    OpResidual opd{ad, Dr, -1.0, c_raw, 1.0, nullptr, tn[5], bl_fin, bu_fin, nb_};
-    update_project(opd, SLK, part_r);
-    finalize(part_r, SLK.ctaA + SLK.ctaB + SLK.ctaC, 7, 0b0010110u, rd);
-    double dobj = hy + rd[6];
-    I.max_dual_ray_inf = (dobj > 0.0) ? rd[1] : 1e10;
+    double pobj = r[2];
+    double dobj = r[5] + r[13 + 6];
     I.primal_ray_obj = pobj;
     I.dual_ray_obj = dobj;
-    ray_norms(dxs, dys, I);
+    I.max_primal_ray_inf = (pobj < 0.0) ? r[6 + 1] : 1e10;
+    I.max_dual_ray_inf = (dobj > 0.0) ? r[13 + 1] : 1e10;
+    I.primal_ray_norm = r[1];
+    I.dual_ray_norm = r[4];
     push_trend(I);
   }
   check_termination();
@@ -1079,22 +1110,17 @@ void Solver::check_termination() {
 double Solver::mnorm(const double* dx, const double* dy, double ta, double si) {
   double* gdx = tm[4];
   spmv(G_, dx, gdx);
-  DotSpec d{};
+  DotSpec d{};  // m-length: y'Gx, y'y
   d.a[0] = dy; d.b[0] = gdx; d.kind[0] = DK_DOT;
-  d.count = 1; d.len = m_;
-  double ygx;
-  dots(d, &ygx);
+  d.a[1] = dy; d.kind[1] = DK_DOT;
+  d.count = 2; d.len = m_;
+  dots_async(d, part_r, 0);
   DotSpec e{};
   e.a[0] = dx; e.kind[0] = DK_DOT;
   e.count = 1; e.len = n_;
-  double xx;
-  dots(e, &xx);
-  DotSpec f{};
-  f.a[0] = dy; f.kind[0] = DK_DOT;
-  f.count = 1; f.len = m_;
-  double yy;
-  dots(f, &yy);
-  return xx / ta - 2.0 * ygx + yy / si;
+  dots_async(e, part_x, 2);
+  const double* r = fetch(3);
+  return r[2] / ta - 2.0 * r[0] + r[1] / si;
 }
 
 // binary_search_duality_gap_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:20-117);
@@ -1113,18 +1139,16 @@ double Solver::binary_search(double r, const double* px, const double* py, doubl
   axpby(h2, -1.0, gpx, 1.0, h_s, m_);
   double last_h1dx = 0.0, last_h2dy = 0.0;
   auto approx = [&](double t) {
+    probes_++;
     OpAxpyProj ox{px, h1, t * ta / 2, xs, nullptr, nullptr};
-    update_project(ox, XI, part_r);
-    double rx[3];
-    finalize(part_r, XI.ctaA + XI.ctaB + XI.ctaC, 3, 0u, rx);
+    finalize_async(part_a, launch_project(ox, XI, part_a), 3, 0u, 0);
     spmv(G_, xs, gxs);
     OpAxpyProj oy{py, h2, t * si / 2, ys, gxs, gpx};
-    update_project(oy, YI, part_r);
-    double ry[3];
-    finalize(part_r, YI.ctaA + YI.ctaB + YI.ctaC, 3, 0u, ry);
-    last_h1dx = rx[1];
-    last_h2dy = ry[1];
-    return rx[0] / ta - 2.0 * ry[2] + ry[0] / si;
+    finalize_async(part_b, launch_project(oy, YI, part_b), 3, 0u, 3);
+    const double* r = fetch(6);
+    last_h1dx = r[1];
+    last_h2dy = r[4];
+    return r[0] / ta - 2.0 * r[5] + r[3] / si;
   };
   double t = bs_t0_, tR = t, tL = 0.0;
   for (int k = 1; k <= 1000; ++k) {
@@ -1157,6 +1181,7 @@ double Solver::binary_search(double r, const double* px, const double* py, doubl
 
 // restart_threshold_calculation_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:354-393)
 void Solver::restart_threshold(bool dgap) {
+  Timer tm_(t_restart_);
   if (dgap) {
     double* dx = tn[4];
     double* dy = tm[5];
@@ -1174,6 +1199,7 @@ void Solver::restart_threshold(bool dgap) {
 
 // restart_condition_check_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:395-506)
 bool Solver::restart_check(bool dgap) {
+  Timer tm_(t_restart_);
   auto to_current = [&]() {
     copy(xm, x, n_);
     copy(ym, y, m_);
@@ -1218,6 +1244,7 @@ bool Solver::restart_check(bool dgap) {
 }
 
 void Solver::run_until_halt() {
+  Timer tm_(t_iter_);
   push_state();
   if (!graph_exec_) capture_graph();
   while (true) {
@@ -1428,6 +1455,10 @@ int Solver::run(pdcs_result* res) {
   res->abs_gap = C.abs_gap;
   res->kernel_launches = kernels_;
   res->graph_launches = graphs_;
+  res->time_iterations = t_iter_;
+  res->time_exit_checks = t_exit_;
+  res->time_restarts = t_restart_;
+  res->restart_probes = probes_;
   return PDCS_OK;
 }
 

@@ -48,6 +48,10 @@ class Info:
     returned_sequence: int
     kernel_launches: int
     graph_launches: int
+    time_iterations: float = 0.0
+    time_exit_checks: float = 0.0
+    time_restarts: float = 0.0
+    restart_probes: int = 0
 
 
 class Solution:
@@ -226,7 +230,9 @@ def rpdhg_gpu_solve(*, n: int, m: int, nb: int, c, G, h, mGzero: int, mGnonnegat
                 l_inf_abs_primal_res=R.l_inf_abs_primal_res,
                 l_inf_abs_dual_res=R.l_inf_abs_dual_res, abs_gap=R.abs_gap,
                 returned_sequence=R.returned_sequence, kernel_launches=R.kernel_launches,
-                graph_launches=R.graph_launches)
+                graph_launches=R.graph_launches, time_iterations=R.time_iterations,
+                time_exit_checks=R.time_exit_checks, time_restarts=R.time_restarts,
+                restart_probes=R.restart_probes)
     return Solution(xo, yo, info)
 
 
