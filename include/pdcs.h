@@ -105,7 +105,7 @@ typedef struct {
   int64_t attempt_limit;         /* > 0: stop after this many PDHG attempts (sampling) */
   void* stream;                  /* cudaStream_t to run on; NULL = an internal stream */
   int32_t attempts_per_graph;    /* PDHG attempts captured per CUDA graph (default 32) */
-  int32_t reserved;
+  int32_t force_resolving;       /* test hook: enter the resolving fallback at the first outer iteration */
 } pdcs_options;
 
 typedef struct {

@@ -47,7 +47,8 @@ class OracleOptions(C.Structure):
                 ("rescaling", C.c_int32), ("cpu_semantics", C.c_int32),
                 ("threads", C.c_int32), ("verbose", C.c_int32),
                 ("time_limit", C.c_double), ("attempt_limit", C.c_int64),
-                ("warm_x", _f64p), ("warm_y", _f64p)]
+                ("warm_x", _f64p), ("warm_y", _f64p),
+                ("force_resolving", C.c_int32), ("pad", C.c_int32)]
 
 
 class OracleResult(C.Structure):

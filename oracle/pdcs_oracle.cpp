@@ -1222,19 +1222,18 @@ struct Solver {
         double di = (double)inner;
         for (int64_t j = 0; j < n; ++j) xm[j] = (xm[j] * di + x[j]) / (di + 1.0);
         for (int64_t i = 0; i < m; ++i) ym[i] = (ym[i] * di + y[i]) / (di + 1.0);
-        bool brk = false;
+        // :570-596: the restart tests come first and break before the exit check
         if (iter % o.kkt_restart_freq == 0 && o.use_kkt_restart) {
-          if (restart_check(inner, false) || outer == 1) brk = true;
+          if (restart_check(inner, false) || outer == 1) break;
         }
-        if (!brk && iter % o.duality_gap_restart_freq == 0 && o.use_duality_gap_restart) {
-          if (restart_check(inner, dgap_flag) || outer == 1) brk = true;
+        if (iter % o.duality_gap_restart_freq == 0 && o.use_duality_gap_restart) {
+          if (restart_check(inner, dgap_flag) || outer == 1) break;
         }
         if (iter % o.check_terminate_freq == 0) {
           exit_check();
           if (exit_code != 7) return;
         }
         if (out_of_attempts()) return;
-        if (brk) break;
       }
       for (int64_t j = 0; j < n; ++j) xd[j] -= x[j];
       for (int64_t i = 0; i < m; ++i) yd[i] -= y[i];
@@ -1272,7 +1271,7 @@ struct Solver {
       bool f2 = outer > 80 && (pd > 1e10 || pd < 1e-10);
       bool f3 = outer > 10 && tau < 1e-6 && sigma < 1e-6;
       bool f4 = iter > 1000000 && ci[0].rel_gap > 0.98 && ci[0].l2_rel_p > 1.0 && ci[0].l2_rel_d > 1.0;
-      if (f1 || f2 || f3 || f4) {
+      if (f1 || f2 || f3 || f4 || o.force_resolving) {
         resolving();
         return;
       }
@@ -1336,6 +1335,7 @@ void oracle_default_options(oracle_options* o) {
   o->attempt_limit = 0;
   o->warm_x = nullptr;
   o->warm_y = nullptr;
+  o->force_resolving = 0;
 }
 
 int oracle_project_block(int kind, double* v, int64_t len, const double* S, const double* lo,

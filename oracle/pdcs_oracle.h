@@ -76,6 +76,8 @@ typedef struct {
   int64_t attempt_limit; /* >0: stop after this many PDHG attempts (bounded CPU sample) */
   const double* warm_x;  /* optional warm start (original scale) */
   const double* warm_y;
+  int32_t force_resolving; /* test hook: enter the resolving fallback at the first outer iteration */
+  int32_t pad;
 } oracle_options;
 
 typedef struct {

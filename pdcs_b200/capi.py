@@ -64,7 +64,7 @@ class PdcsOptions(C.Structure):
                 ("time_limit", C.c_double), ("kkt_restart_freq", C.c_int64),
                 ("use_duality_gap_restart", C.c_int32), ("precision", C.c_int32),
                 ("duality_gap_restart_freq", C.c_int64), ("attempt_limit", C.c_int64),
-                ("stream", _vp), ("attempts_per_graph", C.c_int32), ("reserved", C.c_int32)]
+                ("stream", _vp), ("attempts_per_graph", C.c_int32), ("force_resolving", C.c_int32)]
 
 
 class PdcsResult(C.Structure):

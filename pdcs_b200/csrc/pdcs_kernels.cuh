@@ -29,6 +29,7 @@ enum HaltReason : int32_t {
   HALT_RESTART_CHECK = 2,  // accepted step with iter % restart_freq == 0
   HALT_ARTIFICIAL = 3,     // inner >= beta_artificial * iter (or forced restart)
   HALT_LIMIT = 4,          // attempt limit reached
+  HALT_RESOLVING_CHECK = 5,  // resolving mode: restart / exit tests due after this step
 };
 
 struct PdhgState {
@@ -42,7 +43,7 @@ struct PdhgState {
   int32_t active, do_reflect, halt_reason, accepted;
   int32_t force_restart, restart_enabled;
   uint32_t done_ctas;  // CTAs of the dual step that have finished (last one runs the control step)
-  int32_t pad1;
+  int32_t resolving;   // fixed-step PDHG with uniform averaging (resolving_pessimistic_step!)
 };
 
 // Shared by the control kernel and the host (after a checkpoint):
@@ -287,6 +288,29 @@ __device__ inline void control_block(PdhgState* st, const double* px, int nbx, c
   s.iter_stepsize += 1;
   double k1 = (double)(s.iter_stepsize + 1);
   s.eta_p = fmin((1.0 - pow(k1, -0.3)) * s.eta_bar, (1.0 + pow(k1, -0.6)) * s.eta);
+  if (s.resolving) {
+    // pdhg_one_iter_diagonal_rescaling! + average_seq (rpdhg_alg_gpu_gen_scaling.jl:250-263,
+    // :561-568): every step is kept; x_lag <- x and the mean is the uniform average
+    s.accepted = 1;
+    s.inner += 1;
+    s.refl_tmp = 1.0;
+    s.refl_inv = 0.0;
+    s.refl_extra = 0.0;
+    s.refl_eta = 1.0;
+    s.refl_cum = (double)s.inner;
+    s.do_reflect = 1;
+    bool due = (s.check_freq > 0 && s.iter % s.check_freq == 0) ||
+               (s.restart_enabled && s.restart_freq > 0 && s.iter % s.restart_freq == 0);
+    if (due) {
+      s.halt_reason = HALT_RESOLVING_CHECK;
+      s.active = 0;
+    } else if (s.attempt_limit > 0 && s.iter >= s.attempt_limit) {
+      s.halt_reason = HALT_LIMIT;
+      s.active = 0;
+    }
+    *st = s;
+    return;
+  }
   s.tau = s.eta / s.omega;
   s.sigma = s.eta * s.omega;
   s.accepted = (s.eta <= s.eta_bar) ? 1 : 0;

@@ -539,6 +539,9 @@ class Solver {
   }
   void run_until_halt();
   void main_loop();
+  double power_method(bool* converged);
+  void resolving();
+  void omega_update(double* xds, double* yds, bool clamp);
   void log_progress();
 };
 
@@ -1304,13 +1307,18 @@ void Solver::main_loop() {
     copy(y, ym, m_);
     if (O.use_kkt_restart) restart_threshold(false);
     else restart_threshold(dgap_flag_);
-    // resolving triggers (:810-838) are evaluated; the pessimistic resolving
-    // loop itself is not part of this build (reported via verbose output)
-    if (O.verbose) {
+    // resolving triggers (:810-838)
+    {
       double pd = ci[0].l2_rel_p / ci[0].l2_rel_d;
-      bool f1 = outer > 10 && max_kkt_ > 1e5, f2 = outer > 80 && (pd > 1e10 || pd < 1e-10),
-           f3 = outer > 10 && S.tau < 1e-6 && S.sigma < 1e-6;
-      if (f1 || f2 || f3) std::printf("[pdcs_b200] resolving trigger at outer %lld\n", (long long)outer);
+      bool f1 = outer > 10 && max_kkt_ > 1e5;
+      bool f2 = outer > 80 && (pd > 1e10 || pd < 1e-10);
+      bool f3 = outer > 10 && S.tau < 1e-6 && S.sigma < 1e-6;
+      bool f4 = S.iter > 1000000 && ci[0].rel_gap > 0.98 && ci[0].l2_rel_p > 1.0 && ci[0].l2_rel_d > 1.0;
+      if (f1 || f2 || f3 || f4 || O.force_resolving) {
+        if (O.verbose) std::printf("[pdcs_b200] resolving fallback at outer %lld\n", (long long)outer);
+        resolving();
+        return;
+      }
     }
     double* xds = xds_;
     double* yds = yds_;
@@ -1398,21 +1406,132 @@ void Solver::main_loop() {
         continue;
       }
     }
-    // dynamic_primal_weight_update (:284-307)
+    omega_update(xds, yds, false);
+  }
+  exit_code_ = PDCS_EXIT_MAX_ITER;
+}
+
+// dynamic_primal_weight_update (rpdhg_alg_gpu_gen_scaling.jl:284-307); the
+// resolving loop clamps the result to [0.8, 1.2] (:632-633)
+void Solver::omega_update(double* xds, double* yds, bool clamp) {
+  DotSpec d{};
+  d.a[0] = xds; d.b[0] = x; d.kind[0] = DK_DIFF2;
+  d.count = 1; d.len = n_;
+  double xn2;
+  dots(d, &xn2);
+  DotSpec e{};
+  e.a[0] = yds; e.b[0] = y; e.kind[0] = DK_DIFF2;
+  e.count = 1; e.len = m_;
+  double yn2;
+  dots(e, &yn2);
+  double xn = std::sqrt(xn2), yn = std::sqrt(yn2), om = S.omega;
+  if ((om > 1e4 || om < 1e-4) && restart_used_ % 20 == 0 && restart_used_ != 0) S.omega = init_omega();
+  else if ((om > 3e4 || om < 1.0 / 3e4) && restart_used_ % 10 == 0 && restart_used_ != 0) S.omega = init_omega();
+  else if (xn > 1e-10 && yn > 1e-10) S.omega = std::exp(0.5 * std::log(yn / xn) + 0.5 * std::log(om));
+  if (clamp) S.omega = std::min(std::max(S.omega, 0.8), 1.2);
+}
+
+// power_method! (def_rpdhg_gen.jl:891-917): sqrt of the largest eigenvalue of
+// G'G (scaled G), tolerance 1e-3, at most 1000 iterations; the start vector
+// is a fixed pseudo-random sequence (the reference draws rand(n)).
+double Solver::power_method(bool* converged) {
+  std::vector<double> b0(n_);
+  uint64_t st = 0x9E3779B97F4A7C15ull;
+  for (int64_t j = 0; j < n_; ++j) {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    b0[j] = (double)(st >> 11) * (1.0 / 9007199254740992.0);
+  }
+  double* b = tn[0];
+  double* ab = tm[0];
+  double* atab = tn[1];
+  PDCS_CUDA(cudaMemcpyAsync(b, b0.data(), sizeof(double) * n_, cudaMemcpyHostToDevice, s_));
+  double nb = nrm2(b, n_);
+  axpby(b, 1.0 / nb, b, 0.0, nullptr, n_);
+  double lam_old = 0.0, lam = 0.0;
+  for (int it = 0; it < 1000; ++it) {
+    spmv(G_, b, ab);
+    spmv(Gt_, ab, atab);
+    nb = nrm2(atab, n_);
+    axpby(b, 1.0 / nb, atab, 0.0, nullptr, n_);
+    spmv(G_, b, ab);
+    spmv(Gt_, ab, atab);
     DotSpec d{};
-    d.a[0] = xds; d.b[0] = x; d.kind[0] = DK_DIFF2;
+    d.a[0] = b; d.b[0] = atab; d.kind[0] = DK_DOT;
     d.count = 1; d.len = n_;
-    double xn2;
-    dots(d, &xn2);
-    DotSpec e{};
-    e.a[0] = yds; e.b[0] = y; e.kind[0] = DK_DIFF2;
-    e.count = 1; e.len = m_;
-    double yn2;
-    dots(e, &yn2);
-    double xn = std::sqrt(xn2), yn = std::sqrt(yn2), om = S.omega;
-    if ((om > 1e4 || om < 1e-4) && restart_used_ % 20 == 0 && restart_used_ != 0) S.omega = init_omega();
-    else if ((om > 3e4 || om < 1.0 / 3e4) && restart_used_ % 10 == 0 && restart_used_ != 0) S.omega = init_omega();
-    else if (xn > 1e-10 && yn > 1e-10) S.omega = std::exp(0.5 * std::log(yn / xn) + 0.5 * std::log(om));
+    dots(d, &lam);
+    if (std::fabs(lam - lam_old) < 1e-3) {
+      *converged = true;
+      return std::sqrt(lam);
+    }
+    lam_old = lam;
+  }
+  *converged = false;
+  return std::sqrt(lam);
+}
+
+// resolving_pessimistic_step! (rpdhg_alg_gpu_gen_scaling.jl:511-638)
+void Solver::resolving() {
+  bool conv = false;
+  double gl = power_method(&conv);
+  double step = (conv ? 0.9 : 0.8) / gl;
+  S.tau = step;
+  S.sigma = step;
+  S.omega = std::min(std::max(init_omega(), 0.8), 1.2);
+  copy(xm, xbest, n_);
+  copy(ym, ybest, m_);
+  for (int64_t outer = 1; outer <= O.max_outer_iter; ++outer) {
+    copy(x0l, x0, n_);
+    copy(y0l, y0, m_);
+    copy(x0, xm, n_);
+    copy(y0, ym, m_);
+    copy(x, xm, n_);
+    copy(y, ym, m_);
+    if (O.use_kkt_restart) restart_threshold(false);
+    else restart_threshold(dgap_flag_);
+    copy(xl, x, n_);
+    copy(yl, y, m_);
+    copy(xds_, x, n_);
+    copy(yds_, y, m_);
+    S.resolving = 1;
+    S.inner = 0;
+    S.ps = S.tau / S.omega;
+    S.ds = S.sigma * S.omega;
+    S.eta = 1.0;  // unused by the fixed-step control
+    S.active = 1;
+    S.halt_reason = HALT_NONE;
+    S.do_reflect = 0;
+    while (true) {
+      run_until_halt();
+      if (O.time_limit > 0 && now_s() - t_start_ > O.time_limit && S.active) {
+        exit_code_ = PDCS_EXIT_TIME_LIMIT;
+        return;
+      }
+      int reason = S.halt_reason;
+      S.halt_reason = HALT_NONE;
+      if (reason == HALT_LIMIT) {
+        exit_code_ = PDCS_EXIT_ATTEMPT_LIMIT;
+        return;
+      }
+      // :570-596: the restart tests come first and break before the exit check
+      bool brk = false;
+      if (O.use_kkt_restart && O.kkt_restart_freq > 0 && S.iter % O.kkt_restart_freq == 0)
+        if (restart_check(false) || outer == 1) brk = true;
+      if (!brk && O.use_duality_gap_restart && O.duality_gap_restart_freq > 0 &&
+          S.iter % O.duality_gap_restart_freq == 0)
+        if (restart_check(dgap_flag_) || outer == 1) brk = true;
+      if (brk) break;
+      if (O.check_terminate_freq > 0 && S.iter % O.check_terminate_freq == 0) {
+        exit_check();
+        log_progress();
+        if (exit_code_ != PDCS_EXIT_CONTINUE) return;
+      }
+      if (S.attempt_limit > 0 && S.iter >= S.attempt_limit) {
+        exit_code_ = PDCS_EXIT_ATTEMPT_LIMIT;
+        return;
+      }
+      S.active = 1;
+    }
+    omega_update(xds_, yds_, true);
   }
   exit_code_ = PDCS_EXIT_MAX_ITER;
 }

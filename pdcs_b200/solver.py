@@ -127,7 +127,8 @@ def rpdhg_gpu_solve(*, n: int, m: int, nb: int, c, G, h, mGzero: int, mGnonnegat
                     logfile_name: Optional[str] = None, use_kkt_restart: bool = False,
                     kkt_restart_freq: int = 2000, use_duality_gap_restart: bool = True,
                     duality_gap_restart_freq: int = 2000, attempt_limit: int = 0,
-                    attempts_per_graph: int = 32, stream=None, device_output: bool = False) -> Solution:
+                    attempts_per_graph: int = 32, stream=None, device_output: bool = False,
+                    force_resolving: bool = False) -> Solution:
     """Solve min c'x s.t. Gx - h in K_d, bl <= x[:nb] <= bu, x[nb:] in K_p on the GPU."""
     if method not in ("average", "halpern"):
         raise ValueError("method only available for :average and :halpern")
@@ -207,6 +208,7 @@ def rpdhg_gpu_solve(*, n: int, m: int, nb: int, c, G, h, mGzero: int, mGnonnegat
     O.duality_gap_restart_freq = duality_gap_restart_freq
     O.attempt_limit = attempt_limit
     O.attempts_per_graph = attempts_per_graph
+    O.force_resolving = int(force_resolving)
     O.stream = stream
 
     R = capi.PdcsResult()

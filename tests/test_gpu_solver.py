@@ -90,3 +90,17 @@ def test_infeasibility_status_matches_oracle(cuda, name):
     # label depends on objective trends that differ with rounding
     cls = {2: "primal", 3: "primal", 4: "dual", 5: "dual"}
     assert cls.get(g.info.exit_code) == cls.get(o["exit_code"]) is not None, (g.info.exit_code, o["exit_code"])
+
+
+@pytest.mark.parametrize("name", ["socp_c0", "mixed_small"])
+def test_resolving_fallback_matches_oracle(cuda, name):
+    """resolving_pessimistic_step!: power-method step, fixed-step PDHG, uniform averaging."""
+    p = INSTANCES[name]()
+    g = solver.solve_problem(p, force_resolving=True, attempt_limit=40)
+    o = B.solve(p, threads=1, force_resolving=1, attempt_limit=40)
+    assert g.info.iter == o["iter"] == 40
+    assert np.abs(g.primal - o["x"]).max() <= 1e-9 * max(1.0, np.abs(o["x"]).max())
+    g = solver.solve_problem(p, force_resolving=True, time_limit=120)
+    o = B.solve(p, threads=2, force_resolving=1, time_limit=120)
+    assert g.info.exit_status == "optimal" and o["exit_code"] == 0
+    assert abs(g.info.pObj - o["primal_objective"]) <= 2e-6 * (1 + abs(o["primal_objective"]))
