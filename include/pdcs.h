@@ -139,6 +139,29 @@ int pdcs_default_options(pdcs_options* opts);
  * (rpdhg_alg_gpu_gen_scaling.jl:770-895). */
 int pdcs_solve(const pdcs_problem* prob, const pdcs_options* opts, pdcs_result* res);
 
+/* Totals of one batched solve. */
+typedef struct {
+  double setup_time;        /* merge + upload + preconditioning seconds */
+  double solve_time;        /* scheduler seconds (all instances, incl. the output gather) */
+  double time_iterations;   /* seconds in shared CUDA graphs of PDHG attempts */
+  int64_t kernel_launches;  /* kernels launched by the batched scheduler */
+  int64_t graph_launches;
+  int64_t service_rounds;   /* batched checkpoint operations (exit checks, restart probes, copies) */
+  int64_t single_fallbacks; /* instances re-solved alone for the resolving fallback */
+} pdcs_batch_info;
+
+/* Solve `count` independent conic programs together.  No counterpart in the
+ * reference, whose rpdhg_gpu_solve takes one program; each instance here
+ * follows that solver's algorithm with its own step sizes, primal weight,
+ * restarts and termination (results[k] as pdcs_solve would fill it; `time` is
+ * the batch's solve time).  Problems must be host data (on_device = 0) whose
+ * variables all lie in the box or a cone block (n = nb + sum(soc_x) +
+ * sum(rsoc_x) + 3 (exp_x + dual_exp_x)); warm starts are not supported.  An
+ * instance that enters the resolving fallback is re-solved alone.  info may
+ * be NULL.  Returns PDCS_OK or the first validation error. */
+int pdcs_solve_batch(int64_t count, const pdcs_problem* problems, const pdcs_options* opts,
+                     pdcs_result* results, pdcs_batch_info* info);
+
 /* Block projections on device memory.  Replaces the projection entry points
  * few_block_proj (cuda/few_block_proj.cu:414-432, bound by gpu_kernel.jl:377-406)
  * and massive/moderate/sufficient_block_proj (cuda/moderate_block_proj.cu:1182,

@@ -6,10 +6,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = [os.path.join(HERE, "csrc", "pdcs_solver.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("pdcs_kernels.cuh", "pdcs_device.cuh")] + [
+DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("pdcs_kernels.cuh", "pdcs_device.cuh", "pdcs_preprocess.cuh",
+                                                     "pdcs_batch.cuh", "pdcs_batch_kernels.cuh")] + [
     os.path.join(ROOT, "include", "pdcs.h")]
 LIB = os.path.join(HERE, "libpdcs_b200.so")
-NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++20",
               "-Xcompiler", "-fPIC", "-shared"]
 
 

@@ -82,9 +82,15 @@ class PdcsResult(C.Structure):
                 ("time_restarts", C.c_double), ("restart_probes", C.c_int64)]
 
 
+class PdcsBatchInfo(C.Structure):
+    _fields_ = [("setup_time", C.c_double), ("solve_time", C.c_double), ("time_iterations", C.c_double),
+                ("kernel_launches", C.c_int64), ("graph_launches", C.c_int64),
+                ("service_rounds", C.c_int64), ("single_fallbacks", C.c_int64)]
+
+
 # every symbol declared in include/pdcs.h
-EXPORTS = ["pdcs_default_options", "pdcs_solve", "pdcs_block_proj", "pdcs_spmv_csr", "pdcs_spmv_csr_noalloc",
-           "pdcs_version"]
+EXPORTS = ["pdcs_default_options", "pdcs_solve", "pdcs_solve_batch", "pdcs_block_proj", "pdcs_spmv_csr",
+           "pdcs_spmv_csr_noalloc", "pdcs_version"]
 
 _lib = None
 
@@ -102,6 +108,8 @@ def load():
     L.pdcs_default_options.restype = C.c_int
     L.pdcs_solve.argtypes = [_P(PdcsProblem), _P(PdcsOptions), _P(PdcsResult)]
     L.pdcs_solve.restype = C.c_int
+    L.pdcs_solve_batch.argtypes = [C.c_int64, _P(PdcsProblem), _P(PdcsOptions), _P(PdcsResult), _P(PdcsBatchInfo)]
+    L.pdcs_solve_batch.restype = C.c_int
     L.pdcs_block_proj.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]
     L.pdcs_block_proj.restype = C.c_int
     L.pdcs_spmv_csr.argtypes = [C.c_int64, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp]

@@ -1,0 +1,1351 @@
+// pdcs_batch.cuh -- batched solver: many independent conic programs in one
+// set of device launches, each with its own step sizes, restarts and
+// termination.  Included by pdcs_solver.cu (it reuses the single-instance
+// solver's setup, tables and helpers).
+//
+// Layout.  The K instances are merged into one block-diagonal program whose
+// x and y are ordered by cone type across instances (x: all box parts, all
+// SOC blocks, RSOC, exp, dual-exp; y: zero, nonneg, SOC, RSOC, exp,
+// dual-exp).  The merged program is a valid single-instance problem, so the
+// device preprocessing (Ruiz + Pock-Chambolle is row/column local, hence per
+// instance), the binned SpMV and the cone tables are the single solver's.
+//
+// Control.  Each instance runs the reference's aggressive main loop
+// (rpdhg_alg_gpu_gen_scaling.jl:770-895) as a C++ coroutine that suspends on
+// every device request.  A scheduler groups the pending requests of all
+// instances by kind and operands and runs each group as ONE masked launch
+// sequence; instances that are iterating share CUDA graphs of PDHG attempts
+// whose control kernel keeps every instance's eta / accept / halt state on
+// the device.  Instances that reach their checkpoints at the same attempt
+// (the common case) are serviced together.
+#pragma once
+#include <array>
+#include <coroutine>
+#include <exception>
+#include <thread>
+#include <type_traits>
+#include <unordered_map>
+#include <utility>
+
+#include "pdcs_batch_kernels.cuh"
+
+namespace pdcs {
+
+// ---------------------------------------------------------------------------
+// Lazily started, awaitable coroutine returning T.
+// ---------------------------------------------------------------------------
+struct CoBase {
+  std::coroutine_handle<> cont;
+  std::exception_ptr ex;
+  std::suspend_always initial_suspend() noexcept { return {}; }
+  struct Final {
+    bool await_ready() noexcept { return false; }
+    template <class P>
+    std::coroutine_handle<> await_suspend(std::coroutine_handle<P> h) noexcept {
+      auto c = h.promise().cont;
+      return c ? c : std::noop_coroutine();
+    }
+    void await_resume() noexcept {}
+  };
+  Final final_suspend() noexcept { return {}; }
+  void unhandled_exception() { ex = std::current_exception(); }
+};
+template <class T>
+struct CoPromise : CoBase {
+  T value{};
+  void return_value(T v) { value = std::move(v); }
+};
+template <>
+struct CoPromise<void> : CoBase {
+  void return_void() {}
+};
+
+template <class T = void>
+class Co {
+ public:
+  struct promise_type : CoPromise<T> {
+    Co get_return_object() { return Co(std::coroutine_handle<promise_type>::from_promise(*this)); }
+  };
+  Co() = default;
+  explicit Co(std::coroutine_handle<promise_type> h) : h_(h) {}
+  Co(Co&& o) noexcept : h_(std::exchange(o.h_, {})) {}
+  Co& operator=(Co&& o) noexcept {
+    if (this != &o) {
+      if (h_) h_.destroy();
+      h_ = std::exchange(o.h_, {});
+    }
+    return *this;
+  }
+  Co(const Co&) = delete;
+  ~Co() {
+    if (h_) h_.destroy();
+  }
+  bool await_ready() const noexcept { return false; }
+  std::coroutine_handle<> await_suspend(std::coroutine_handle<> c) noexcept {
+    h_.promise().cont = c;
+    return h_;
+  }
+  T await_resume() {
+    if (h_.promise().ex) std::rethrow_exception(h_.promise().ex);
+    if constexpr (!std::is_void_v<T>) return std::move(h_.promise().value);
+  }
+  void start() { h_.resume(); }
+  bool done() const { return !h_ || h_.done(); }
+  void rethrow() const {
+    if (h_ && h_.done() && h_.promise().ex) std::rethrow_exception(h_.promise().ex);
+  }
+
+ private:
+  std::coroutine_handle<promise_type> h_;
+};
+
+// ---------------------------------------------------------------------------
+// Device requests.  Requests whose payloads are byte-identical run as one
+// batched operation over the union of the requesting instances.
+// ---------------------------------------------------------------------------
+enum ReqType : int32_t {
+  RQ_NONE = 0,
+  RQ_ITERATE,   // run PDHG attempts until this instance halts
+  RQ_CONVERGE,  // KKT quantities of (p0, p1) -> out[0..15]; G p0 -> p2, G' p1 -> p3
+  RQ_PROBE,     // one binary-search evaluation (restart duality gap)
+  RQ_MNORM,     // G p0 -> p2; out = [p1'(G p0), p1'p1, p0'p0]
+  RQ_SEG,       // per-instance reductions X / Y
+  RQ_LIN,       // dst = a u + b v (up to 6, in order)
+  RQ_SPMV,      // side 0: G p0 -> p1; side 1: G' p0 -> p1
+  RQ_REFLECT,   // reflection + averaging with the instance's current coefficients
+};
+
+struct LinOp {
+  double* dst;
+  const double* u;
+  const double* v;
+  double a, b;
+  int32_t side, pad;
+};
+
+struct ReqPayload {
+  int32_t type, side, count, pad;
+  const double* p[8];
+  LinOp lin[6];
+  SegSide X, Y;
+};
+
+struct Req {
+  ReqPayload key;
+  uint64_t hash = 0;
+  double s0 = 0.0, s1 = 0.0;  // per-instance scalars (probe steps)
+  double out[20] = {};
+};
+
+struct Inst {
+  int64_t k = 0;
+  PdhgState S{};
+  Converge ci[2];
+  Infea ii[2];
+  int exit_code = PDCS_EXIT_CONTINUE;
+  int returned_seq = 0;
+  double pobj = 1e30, dobj = 1e30, max_kkt = 1e30, min_kkt = 1e30, pres_best = 1e30, dres_best = 1e30;
+  double ndg[2] = {1e30, 1e30}, ndg_thr = 0, ndg_r = 1e30, kkt_err[2] = {1e30, 1e30}, kkt_thr = 0;
+  bool dgap_flag = true;
+  double bs_t0 = 1.0;
+  int64_t restart_used = 0, check_count = 0, probes = 0;
+  double hNrm1 = 0, hNrmInf = 0, cNrm1 = 0, cNrmInf = 0, ginf = 1, omega0 = 1;
+  bool needs_single = false;  // resolving fallback: re-solved alone after the batch
+  double t_done = 0;
+  Req req;
+  std::coroutine_handle<> waiting;
+  Co<> task;
+};
+
+struct DevAwait {
+  Inst* I;
+  bool await_ready() const noexcept { return false; }
+  void await_suspend(std::coroutine_handle<> h) noexcept { I->waiting = h; }
+  void await_resume() const noexcept {}
+};
+
+static uint64_t fnv1a(const void* p, size_t n) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  uint64_t h = 1469598103934665603ull;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// masked in-order copies / linear combinations (RQ_LIN)
+struct LinList {
+  LinOp op[6];
+  int32_t count;
+};
+
+__global__ void masked_lin_kernel(LinList L, const int32_t* __restrict__ ix, const int32_t* __restrict__ iy,
+                                  const uint8_t* __restrict__ mask, int64_t n, int64_t m) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int q = 0; q < L.count; ++q) {
+    const LinOp& o = L.op[q];
+    const int64_t len = o.side ? m : n;
+    const int32_t* inst = o.side ? iy : ix;
+    for (int64_t i = t0; i < len; i += stride) {
+      if (!mask[inst[i]]) continue;
+      o.dst[i] = o.a * o.u[i] + (o.v ? o.b * o.v[i] : 0.0);
+    }
+  }
+}
+
+// masked reflection (RQ_REFLECT): the host-side reflection after a checkpoint
+__global__ void masked_reflect_kernel(const PdhgState* __restrict__ sts, const int32_t* __restrict__ ix,
+                                      const int32_t* __restrict__ iy, const uint8_t* __restrict__ mask,
+                                      double* __restrict__ x, double* __restrict__ xl, double* __restrict__ xm,
+                                      int64_t n, double* __restrict__ y, double* __restrict__ yl,
+                                      double* __restrict__ ym, int64_t m) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += stride) {
+    const bool isx = i < n;
+    const int64_t j = isx ? i : i - n;
+    const int32_t k = isx ? ix[j] : iy[j];
+    if (!mask[k]) continue;
+    const PdhgState& s = sts[k];
+    double* v = isx ? x : y;
+    double* vl = isx ? xl : yl;
+    double* vm = isx ? xm : ym;
+    const double tmp = s.refl_tmp, inv = s.refl_inv, e = s.refl_extra, eta = s.refl_eta, cum = s.refl_cum;
+    const double cur = v[j];
+    const double nv = tmp * ((1.0 + e) * cur - e * vl[j]) + inv * cur;
+    vm[j] = (vm[j] * cum + nv * eta) / (cum + eta);
+    v[j] = nv;
+    vl[j] = nv;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The batched solver.
+// ---------------------------------------------------------------------------
+class BatchSolver : public Solver {
+ public:
+  BatchSolver(int64_t K, const pdcs_problem* probs, const pdcs_options* o)
+      : Solver(probs, o), K_(K), probs_(probs) {}
+  ~BatchSolver() override {
+    if (bgraph_exec_) cudaGraphExecDestroy(bgraph_exec_);
+    if (bgraph_) cudaGraphDestroy(bgraph_);
+    if (pin_) cudaFreeHost(pin_);
+  }
+  int run_batch(pdcs_result* res, pdcs_batch_info* info);
+
+ private:
+  int64_t K_;
+  const pdcs_problem* probs_;
+  // merged host problem
+  std::vector<int32_t> h_rp_, h_ci_;
+  std::vector<double> h_v_, h_c_, h_h_, h_bl_, h_bu_;
+  std::vector<int64_t> h_socx_, h_rsocx_, h_socG_, h_rsocG_;
+  // per instance: offsets of its runs in the merged vectors and local starts
+  std::vector<int64_t> xrun_start_, xrun_len_, yrun_start_, yrun_len_;  // K * kMaxRuns
+  std::vector<int64_t> xloc_, yloc_;                                    // K * kMaxRuns local starts
+  std::vector<int32_t> h_ix_, h_iy_;
+  // device
+  int32_t *ix_ = nullptr, *iy_ = nullptr;
+  RunTable rx_{}, ry_{};
+  PdhgState* sts_ = nullptr;
+  double *ps_ = nullptr, *ds_ = nullptr;
+  uint8_t* live_ = nullptr;
+  int32_t* live_cnt_ = nullptr;  // [0..1] live counts of alternating attempts, [2] accumulator
+  uint32_t* done_ctas_ = nullptr;
+  uint8_t* mask_ = nullptr;
+  double *s0_ = nullptr, *s1_ = nullptr;
+  double *cx_ = nullptr, *cy_ = nullptr;  // contributions: 8 x n, 8 x m
+  double *dxsq_ = nullptr, *dysq_ = nullptr, *dgdy_ = nullptr;
+  double* seg_out_ = nullptr;  // K * 20
+  cudaGraph_t bgraph_ = nullptr;
+  cudaGraphExec_t bgraph_exec_ = nullptr;
+  // pinned staging (reset at every synchronisation)
+  char* pin_ = nullptr;
+  size_t pin_cap_ = 0, pin_off_ = 0;
+  std::vector<Inst> inst_;
+  int64_t rounds_ = 0;
+
+  int validate_batch();
+  void merge();
+  void setup_batch();
+  void capture_batch_graph();
+  template <class T>
+  T* stage(size_t count);
+  void sync_reset() {
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    pin_off_ = 0;
+  }
+  uint8_t* upload_mask(const std::vector<Inst*>& g);
+  void seg_launch(const uint8_t* mask, const SegSide& X, const SegSide& Y, int stride);
+  const double* seg_fetch(int stride);
+  void exec_group(std::vector<Inst*>& g);
+  void exec_iterate(std::vector<Inst*>& its);
+  void resume(Inst& I) {
+    auto h = I.waiting;
+    I.waiting = nullptr;
+    h.resume();
+    I.task.rethrow();
+  }
+  void schedule();
+
+  // ---- requests (set the payload, suspend) ----
+  DevAwait post(Inst& I, const ReqPayload& p, double s0 = 0.0, double s1 = 0.0) {
+    I.req.key = p;
+    I.req.hash = fnv1a(&I.req.key, sizeof(ReqPayload));
+    I.req.s0 = s0;
+    I.req.s1 = s1;
+    return DevAwait{&I};
+  }
+  static ReqPayload payload(int32_t type) {
+    ReqPayload p;
+    std::memset(&p, 0, sizeof(p));  // padding takes part in the comparison
+    p.type = type;
+    return p;
+  }
+  struct Lin {
+    double* dst;
+    double a;
+    const double* u;
+    double b;
+    const double* v;
+    int side;
+  };
+  Co<> lin(Inst& I, std::vector<Lin> ops);
+  Co<> converge_info(Inst& I, const double* xs, const double* ys, Converge& C, double* gxs, double* atys);
+  Co<> exit_check(Inst& I);
+  Co<double> mnorm(Inst& I, const double* dx, const double* dy, double ta, double si);
+  Co<double> binary_search(Inst& I, double r, const double* px, const double* py, double ta, double si);
+  Co<double> approx(Inst& I, const ReqPayload& pr, double ta, double si, double& h1dx, double& h2dy, double t);
+  Co<> restart_threshold(Inst& I, bool dgap);
+  Co<bool> restart_check(Inst& I, bool dgap);
+  Co<> omega_update(Inst& I, const double* xds, const double* yds);
+  Co<> iterate(Inst& I);
+  Co<> main_task(Inst& I);
+  double kkt_error_i(const Inst& I, const Converge& C) const {
+    const double om = I.S.omega;
+    return std::sqrt(om * om * C.l2_abs_p * C.l2_abs_p + C.l2_abs_d * C.l2_abs_d / (om * om) +
+                     C.abs_gap * C.abs_gap);
+  }
+};
+
+template <class T>
+T* BatchSolver::stage(size_t count) {
+  size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+  if (pin_off_ + bytes > pin_cap_) sync_reset();
+  if (bytes > pin_cap_) throw std::runtime_error("batch staging buffer too small");
+  T* p = reinterpret_cast<T*>(pin_ + pin_off_);
+  pin_off_ += bytes;
+  return p;
+}
+
+int BatchSolver::validate_batch() {
+  if (K_ < 1 || !probs_) return PDCS_ERR_INVALID;
+  for (int64_t k = 0; k < K_; ++k) {
+    const pdcs_problem& q = probs_[k];
+    if (q.on_device) return PDCS_ERR_UNSUPPORTED;  // the batch merges host data
+    Solver one(&q, &O);
+    int rc = one.validate_only();
+    if (rc != PDCS_OK) return rc;
+    int64_t nsum = q.nb + 3 * (q.exp_x + q.dual_exp_x);
+    for (int64_t i = 0; i < q.n_soc_x; ++i) nsum += q.soc_x[i];
+    for (int64_t i = 0; i < q.n_rsoc_x; ++i) nsum += q.rsoc_x[i];
+    if (nsum != q.n) return PDCS_ERR_N_MISMATCH;  // every variable belongs to a cone
+    if (O.warm_start) return PDCS_ERR_UNSUPPORTED;
+  }
+  return PDCS_OK;
+}
+
+// Build the merged, type-ordered program on the host (parallel over instances).
+void BatchSolver::merge() {
+  const int64_t K = K_;
+  std::vector<std::array<int64_t, kMaxRuns>> xs(K), ys(K);  // sizes per type
+  for (int64_t k = 0; k < K; ++k) {
+    const pdcs_problem& q = probs_[k];
+    int64_t soc = 0, rsoc = 0, socg = 0, rsocg = 0;
+    for (int64_t i = 0; i < q.n_soc_x; ++i) soc += q.soc_x[i];
+    for (int64_t i = 0; i < q.n_rsoc_x; ++i) rsoc += q.rsoc_x[i];
+    for (int64_t i = 0; i < q.n_socG; ++i) socg += q.socG[i];
+    for (int64_t i = 0; i < q.n_rsocG; ++i) rsocg += q.rsocG[i];
+    xs[k] = {q.nb, soc, rsoc, 3 * q.exp_x, 3 * q.dual_exp_x, 0};
+    ys[k] = {q.mGzero, q.mGnonnegative, socg, rsocg, 3 * q.expG, 3 * q.dual_expG};
+  }
+  // region offsets and per-instance offsets inside each region
+  xrun_start_.assign(K * kMaxRuns, 0);
+  xrun_len_.assign(K * kMaxRuns, 0);
+  yrun_start_.assign(K * kMaxRuns, 0);
+  yrun_len_.assign(K * kMaxRuns, 0);
+  xloc_.assign(K * kMaxRuns, 0);
+  yloc_.assign(K * kMaxRuns, 0);
+  int64_t N = 0, M = 0;
+  for (int t = 0; t < kMaxRuns; ++t) {
+    for (int64_t k = 0; k < K; ++k) {
+      xrun_start_[k * kMaxRuns + t] = N;
+      xrun_len_[k * kMaxRuns + t] = xs[k][t];
+      N += xs[k][t];
+      yrun_start_[k * kMaxRuns + t] = M;
+      yrun_len_[k * kMaxRuns + t] = ys[k][t];
+      M += ys[k][t];
+    }
+  }
+  for (int64_t k = 0; k < K; ++k) {
+    int64_t a = 0, b = 0;
+    for (int t = 0; t < kMaxRuns; ++t) {
+      xloc_[k * kMaxRuns + t] = a;
+      a += xs[k][t];
+      yloc_[k * kMaxRuns + t] = b;
+      b += ys[k][t];
+    }
+  }
+  // row lengths in merged order, then the merged CSR
+  std::vector<int64_t> nnz_off(K + 1, 0);
+  for (int64_t k = 0; k < K; ++k) nnz_off[k + 1] = nnz_off[k] + probs_[k].nnz;
+  if (N > INT32_MAX || M > INT32_MAX || nnz_off[K] > INT32_MAX) throw std::invalid_argument("batch too large");
+  h_rp_.assign(M + 1, 0);
+  h_ci_.resize(nnz_off[K]);
+  h_v_.resize(nnz_off[K]);
+  h_c_.resize(N);
+  h_h_.resize(M);
+  h_ix_.resize(N);
+  h_iy_.resize(M);
+  int64_t NB = 0;
+  for (int64_t k = 0; k < K; ++k) NB += probs_[k].nb;
+  h_bl_.resize(NB);
+  h_bu_.resize(NB);
+  auto posx = [&](int64_t k, int64_t j) {
+    int t = kMaxRuns - 1;
+    while (t > 0 && j < xloc_[k * kMaxRuns + t]) --t;
+    return xrun_start_[k * kMaxRuns + t] + (j - xloc_[k * kMaxRuns + t]);
+  };
+  auto posy = [&](int64_t k, int64_t i) {
+    int t = kMaxRuns - 1;
+    while (t > 0 && i < yloc_[k * kMaxRuns + t]) --t;
+    return yrun_start_[k * kMaxRuns + t] + (i - yloc_[k * kMaxRuns + t]);
+  };
+  const unsigned nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  auto parallel = [&](auto&& fn) {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nth; ++t)
+      th.emplace_back([&, t]() {
+        for (int64_t k = t; k < K; k += nth) fn(k);
+      });
+    for (auto& x : th) x.join();
+  };
+  parallel([&](int64_t k) {
+    const pdcs_problem& q = probs_[k];
+    for (int64_t i = 0; i < q.m; ++i) h_rp_[posy(k, i) + 1] = q.G_rowptr[i + 1] - q.G_rowptr[i];
+    for (int64_t j = 0; j < q.n; ++j) {
+      const int64_t p = posx(k, j);
+      h_c_[p] = q.c[j];
+      h_ix_[p] = (int32_t)k;
+    }
+    for (int64_t i = 0; i < q.m; ++i) {
+      const int64_t p = posy(k, i);
+      h_h_[p] = q.h[i];
+      h_iy_[p] = (int32_t)k;
+    }
+    for (int64_t j = 0; j < q.nb; ++j) {
+      h_bl_[xrun_start_[k * kMaxRuns] + j] = q.bl[j];
+      h_bu_[xrun_start_[k * kMaxRuns] + j] = q.bu[j];
+    }
+  });
+  for (int64_t i = 0; i < M; ++i) h_rp_[i + 1] += h_rp_[i];
+  parallel([&](int64_t k) {
+    const pdcs_problem& q = probs_[k];
+    // local column -> merged column, run by run
+    for (int64_t i = 0; i < q.m; ++i) {
+      int64_t dst = h_rp_[posy(k, i)];
+      for (int64_t e = q.G_rowptr[i]; e < q.G_rowptr[i + 1]; ++e, ++dst) {
+        h_ci_[dst] = (int32_t)posx(k, q.G_colind[e]);
+        h_v_[dst] = q.G_val[e];
+      }
+    }
+  });
+  for (int64_t k = 0; k < K; ++k) {
+    const pdcs_problem& q = probs_[k];
+    h_socx_.insert(h_socx_.end(), q.soc_x, q.soc_x + q.n_soc_x);
+    h_socG_.insert(h_socG_.end(), q.socG, q.socG + q.n_socG);
+  }
+  for (int64_t k = 0; k < K; ++k) {
+    const pdcs_problem& q = probs_[k];
+    h_rsocx_.insert(h_rsocx_.end(), q.rsoc_x, q.rsoc_x + q.n_rsoc_x);
+    h_rsocG_.insert(h_rsocG_.end(), q.rsocG, q.rsocG + q.n_rsocG);
+  }
+  pdcs_problem mp;
+  std::memset(&mp, 0, sizeof(mp));
+  mp.n = N;
+  mp.m = M;
+  mp.nb = NB;
+  mp.nnz = nnz_off[K];
+  mp.G_rowptr = h_rp_.data();
+  mp.G_colind = h_ci_.data();
+  mp.G_val = h_v_.data();
+  mp.c = h_c_.data();
+  mp.h = h_h_.data();
+  mp.bl = h_bl_.data();
+  mp.bu = h_bu_.data();
+  for (int64_t k = 0; k < K; ++k) {
+    mp.mGzero += probs_[k].mGzero;
+    mp.mGnonnegative += probs_[k].mGnonnegative;
+    mp.expG += probs_[k].expG;
+    mp.dual_expG += probs_[k].dual_expG;
+    mp.exp_x += probs_[k].exp_x;
+    mp.dual_exp_x += probs_[k].dual_exp_x;
+  }
+  mp.socG = h_socG_.data();
+  mp.n_socG = (int64_t)h_socG_.size();
+  mp.rsocG = h_rsocG_.data();
+  mp.n_rsocG = (int64_t)h_rsocG_.size();
+  mp.soc_x = h_socx_.data();
+  mp.n_soc_x = (int64_t)h_socx_.size();
+  mp.rsoc_x = h_rsocx_.data();
+  mp.n_rsoc_x = (int64_t)h_rsocx_.size();
+  mp.on_device = 0;
+  P = mp;
+}
+
+void BatchSolver::setup_batch() {
+  const int64_t K = K_;
+  auto up = [&](auto* dst, const auto& v) {
+    if (!v.empty()) PDCS_CUDA(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, s_));
+  };
+  ix_ = A.alloc<int32_t>(n_);
+  iy_ = A.alloc<int32_t>(m_);
+  up(ix_, h_ix_);
+  up(iy_, h_iy_);
+  int64_t* rxs = A.alloc<int64_t>(K * kMaxRuns);
+  int64_t* rxl = A.alloc<int64_t>(K * kMaxRuns);
+  int64_t* rys = A.alloc<int64_t>(K * kMaxRuns);
+  int64_t* ryl = A.alloc<int64_t>(K * kMaxRuns);
+  up(rxs, xrun_start_);
+  up(rxl, xrun_len_);
+  up(rys, yrun_start_);
+  up(ryl, yrun_len_);
+  rx_ = RunTable{rxs, rxl};
+  ry_ = RunTable{rys, ryl};
+  sts_ = A.alloc<PdhgState>(K);
+  ps_ = A.alloc<double>(K);
+  ds_ = A.alloc<double>(K);
+  live_ = A.alloc<uint8_t>(K);
+  live_cnt_ = A.alloc<int32_t>(4);
+  done_ctas_ = A.alloc<uint32_t>(1);
+  mask_ = A.alloc<uint8_t>(K);
+  s0_ = A.alloc<double>(K);
+  s1_ = A.alloc<double>(K);
+  cx_ = A.alloc<double>(8 * std::max<int64_t>(n_, 1));
+  cy_ = A.alloc<double>(8 * std::max<int64_t>(m_, 1));
+  dxsq_ = A.alloc<double>(n_);
+  dysq_ = A.alloc<double>(m_);
+  dgdy_ = A.alloc<double>(m_);
+  seg_out_ = A.alloc<double>(K * 20);
+  PDCS_CUDA(cudaMemsetAsync(live_cnt_, 0, 4 * sizeof(int32_t), s_));
+  PDCS_CUDA(cudaMemsetAsync(done_ctas_, 0, sizeof(uint32_t), s_));
+  PDCS_CUDA(cudaMemsetAsync(live_, 0, K, s_));
+  pin_cap_ = std::max<size_t>(size_t(1) << 20, (size_t)K * (20 * sizeof(double) + sizeof(PdhgState)) * 4 + 4096);
+  PDCS_CUDA(cudaMallocHost(&pin_, pin_cap_));
+  inst_.resize(K);
+  for (int64_t k = 0; k < K; ++k) inst_[k].k = k;
+  // per-instance constants: raw norms (cal_constant), ginf, initial primal weight
+  {
+    SegSide X{}, Y{};
+    X.a[0] = c_raw; X.kind[0] = SK_SUMABS;
+    X.a[1] = c_raw; X.kind[1] = SK_MAXABS;
+    X.a[2] = c_s; X.kind[2] = SK_DOT;
+    X.count = 3;
+    double* rowmax = tm[0];
+    row_absstat_kernel<false><<<warp_grid(m_), kThreads, 0, s_>>>(m_, G_.rp, G_.v, nullptr, rowmax);
+    Y.a[0] = h_raw; Y.kind[0] = SK_SUMABS;
+    Y.a[1] = h_raw; Y.kind[1] = SK_MAXABS;
+    Y.a[2] = h_s; Y.kind[2] = SK_DOT;
+    Y.a[3] = rowmax; Y.kind[3] = SK_MAX;
+    Y.count = 4;
+    seg_launch(nullptr, X, Y, 7);
+    const double* r = seg_fetch(7);
+    for (int64_t k = 0; k < K; ++k) {
+      Inst& I = inst_[k];
+      const double* q = r + k * 7;
+      I.cNrm1 = q[0];
+      I.cNrmInf = q[1];
+      I.hNrm1 = q[3];
+      I.hNrmInf = q[4];
+      I.ginf = q[6];
+      const double cn = std::sqrt(q[2]), hn = std::sqrt(q[5]);
+      I.omega0 = (hn > 1e-10 && cn > 1e-10) ? cn / hn : 1.0;
+    }
+  }
+  attempts_per_graph_ = (attempts_per_graph_ + 1) & ~1;  // even: live-count slots alternate
+}
+
+uint8_t* BatchSolver::upload_mask(const std::vector<Inst*>& g) {
+  uint8_t* h = stage<uint8_t>(K_);
+  std::memset(h, 0, K_);
+  for (Inst* I : g) h[I->k] = 1;
+  PDCS_CUDA(cudaMemcpyAsync(mask_, h, K_, cudaMemcpyHostToDevice, s_));
+  return mask_;
+}
+
+void BatchSolver::seg_launch(const uint8_t* mask, const SegSide& X, const SegSide& Y, int stride) {
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((K_ * 32 + kThreads - 1) / kThreads, 148 * 16));
+  seg_reduce_kernel<<<grid, kThreads, 0, s_>>>(K_, mask, rx_, X, ry_, Y, seg_out_, stride);
+  kernels_++;
+}
+
+const double* BatchSolver::seg_fetch(int stride) {
+  double* h = stage<double>((size_t)K_ * stride);
+  PDCS_CUDA(cudaMemcpyAsync(h, seg_out_, sizeof(double) * K_ * stride, cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  // the staged copy stays valid until the next stage() call wraps around
+  return h;
+}
+
+void BatchSolver::capture_batch_graph() {
+  PDCS_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+  const int ctl_grid = (int)std::max<int64_t>(1, std::min<int64_t>((K_ * 32 + kThreads - 1) / kThreads, 148 * 16));
+  for (int a = 0; a < attempts_per_graph_; ++a) {
+    int32_t* cur = live_cnt_ + (a & 1);
+    int32_t* nxt = live_cnt_ + ((a + 1) & 1);
+    spmv_binned_kernel<1, true><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, yl, nullptr, aty, nullptr, cur, nullptr,
+                                                                      ix_, live_);
+    OpPrimalStepB op1{xl, aty, c_s, x, ix_, live_, ps_, dxsq_};
+    update_project_kernel<OpPrimalStepB><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, cur);
+    spmv_binned_kernel<2, true><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, x, xl, gx, gxl, cur, nullptr, iy_, live_);
+    OpDualStepB op2{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_};
+    update_project_kernel<OpDualStepB><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, cur);
+    BatchCtl ctl{sts_, ps_, ds_, live_, rx_, ry_, dxsq_, dysq_, dgdy_, cur, nxt, done_ctas_, live_cnt_ + 2};
+    batch_control_kernel<<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
+    batch_reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, x, xl, xm, n_, y, yl, ym, m_);
+  }
+  PDCS_CUDA(cudaStreamEndCapture(s_, &bgraph_));
+  PDCS_CUDA(cudaGraphInstantiate(&bgraph_exec_, bgraph_, 0));
+}
+
+// Run one batched operation for a group of instances with identical requests.
+void BatchSolver::exec_group(std::vector<Inst*>& g) {
+  const ReqPayload& q = g[0]->req.key;
+  rounds_++;
+  const uint8_t* mask = upload_mask(g);
+  auto kresid_side = [&](SegSide& S, double* contrib, int64_t stride) {
+    const int32_t kinds[7] = {SK_SUM, SK_MAX, SK_MAX, SK_SUM, SK_MAX, SK_SUM, SK_SUM};  // OpResidual's kResid7
+    for (int r = 0; r < 7; ++r) {
+      S.a[r] = contrib + r * stride;
+      S.kind[r] = kinds[r];
+    }
+  };
+  switch (q.type) {
+    case RQ_LIN: {
+      LinList L{};
+      for (int i = 0; i < q.count; ++i) L.op[i] = q.lin[i];
+      L.count = q.count;
+      masked_lin_kernel<<<grid_for(std::max(n_, m_)), kThreads, 0, s_>>>(L, ix_, iy_, mask, n_, m_);
+      kernels_++;
+      break;
+    }
+    case RQ_SPMV: {
+      const CsrDev& M = q.side ? Gt_ : G_;
+      spmv_binned_kernel<1, true><<<M.cta0[kBins], kThreads, 0, s_>>>(M, q.p[0], nullptr, const_cast<double*>(q.p[1]),
+                                                                      nullptr, nullptr, nullptr, q.side ? ix_ : iy_,
+                                                                      mask);
+      kernels_++;
+      break;
+    }
+    case RQ_REFLECT: {
+      PdhgState* h = stage<PdhgState>(K_);
+      for (int64_t k = 0; k < K_; ++k) h[k] = inst_[k].S;
+      PDCS_CUDA(cudaMemcpyAsync(sts_, h, sizeof(PdhgState) * K_, cudaMemcpyHostToDevice, s_));
+      masked_reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(sts_, ix_, iy_, mask, x, xl, xm, n_, y, yl, ym, m_);
+      kernels_++;
+      break;
+    }
+    case RQ_CONVERGE: {
+      const double *xs = q.p[0], *ys = q.p[1];
+      double *gxs = const_cast<double*>(q.p[2]), *atys = const_cast<double*>(q.p[3]);
+      if (q.side == 0) {  // side 1: the products G xs, G' ys are given
+        spmv_binned_kernel<1, true><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, xs, nullptr, gxs, nullptr, nullptr,
+                                                                        nullptr, iy_, mask);
+        spmv_binned_kernel<1, true><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, ys, nullptr, atys, nullptr, nullptr,
+                                                                          nullptr, ix_, mask);
+        kernels_ += 2;
+      }
+      PerElem<OpResidual> opp{OpResidual{gxs, Dl, 1.0, nullptr, 0.0, h_raw, tm[5], bl_fin, bu_fin, 0}, tm[5], cy_, m_,
+                              iy_, mask};
+      update_project(opp, CON, part_a);
+      PerElem<OpResidual> opd{OpResidual{atys, Dr, -1.0, c_raw, 1.0, nullptr, tn[5], bl_fin, bu_fin, nb_}, tn[5], cx_,
+                              n_, ix_, mask};
+      update_project(opd, SLK, part_b);
+      SegSide X{}, Y{};
+      kresid_side(X, cx_, n_);
+      X.a[7] = c_raw; X.b[7] = xs; X.sa[7] = Dr; X.kind[7] = SK_DOT;
+      X.count = 8;
+      kresid_side(Y, cy_, m_);
+      Y.a[7] = h_raw; Y.b[7] = ys; Y.sa[7] = Dl; Y.kind[7] = SK_DOT;
+      Y.count = 8;
+      seg_launch(mask, X, Y, 16);
+      const double* r = seg_fetch(16);
+      for (Inst* I : g) {
+        const double* v = r + I->k * 16;
+        // single-solver layout: [0..6] primal residual (y side), [7..13] dual (x side), 14 c'x, 15 h'y
+        for (int i = 0; i < 7; ++i) {
+          I->req.out[i] = v[8 + i];
+          I->req.out[7 + i] = v[i];
+        }
+        I->req.out[14] = v[7];
+        I->req.out[15] = v[15];
+      }
+      break;
+    }
+    case RQ_PROBE: {
+      // p: px, py, h1, h2, gpx, xs, ys, gxs; s0 / s1: per-instance steps
+      double* a0 = stage<double>(K_);
+      double* a1 = stage<double>(K_);
+      for (Inst* I : g) {
+        a0[I->k] = I->req.s0;
+        a1[I->k] = I->req.s1;
+      }
+      PDCS_CUDA(cudaMemcpyAsync(s0_, a0, sizeof(double) * K_, cudaMemcpyHostToDevice, s_));
+      PDCS_CUDA(cudaMemcpyAsync(s1_, a1, sizeof(double) * K_, cudaMemcpyHostToDevice, s_));
+      double *xs = const_cast<double*>(q.p[5]), *ys = const_cast<double*>(q.p[6]);
+      double* gxs = const_cast<double*>(q.p[7]);
+      PerElem<OpAxpyProjB> ox{OpAxpyProjB{q.p[0], q.p[2], s0_, xs, nullptr, nullptr, ix_}, xs, cx_, n_, ix_, mask};
+      update_project(ox, XI, part_a);
+      spmv_binned_kernel<1, true><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, xs, nullptr, gxs, nullptr, nullptr, nullptr,
+                                                                      iy_, mask);
+      PerElem<OpAxpyProjB> oy{OpAxpyProjB{q.p[1], q.p[3], s1_, ys, gxs, q.p[4], iy_}, ys, cy_, m_, iy_, mask};
+      update_project(oy, YI, part_b);
+      kernels_ += 1;
+      SegSide X{}, Y{};
+      X.a[0] = cx_; X.kind[0] = SK_SUM;
+      X.a[1] = cx_ + n_; X.kind[1] = SK_SUM;
+      X.count = 2;
+      Y.a[0] = cy_; Y.kind[0] = SK_SUM;
+      Y.a[1] = cy_ + m_; Y.kind[1] = SK_SUM;
+      Y.a[2] = cy_ + 2 * m_; Y.kind[2] = SK_SUM;
+      Y.count = 3;
+      seg_launch(mask, X, Y, 5);
+      const double* r = seg_fetch(5);
+      for (Inst* I : g) {
+        const double* v = r + I->k * 5;
+        I->req.out[0] = v[0];
+        I->req.out[1] = v[1];
+        I->req.out[3] = v[2];
+        I->req.out[4] = v[3];
+        I->req.out[5] = v[4];
+      }
+      break;
+    }
+    case RQ_MNORM: {
+      double* gdx = const_cast<double*>(q.p[2]);
+      spmv_binned_kernel<1, true><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, q.p[0], nullptr, gdx, nullptr, nullptr,
+                                                                      nullptr, iy_, mask);
+      kernels_++;
+      SegSide X{}, Y{};
+      X.a[0] = q.p[0]; X.kind[0] = SK_DOT;
+      X.count = 1;
+      Y.a[0] = q.p[1]; Y.b[0] = gdx; Y.kind[0] = SK_DOT;
+      Y.a[1] = q.p[1]; Y.kind[1] = SK_DOT;
+      Y.count = 2;
+      seg_launch(mask, X, Y, 3);
+      const double* r = seg_fetch(3);
+      for (Inst* I : g) {
+        const double* v = r + I->k * 3;
+        I->req.out[0] = v[1];
+        I->req.out[1] = v[2];
+        I->req.out[2] = v[0];
+      }
+      break;
+    }
+    case RQ_SEG: {
+      const int stride = q.X.count + q.Y.count;
+      seg_launch(mask, q.X, q.Y, stride);
+      const double* r = seg_fetch(stride);
+      for (Inst* I : g)
+        for (int i = 0; i < stride; ++i) I->req.out[i] = r[I->k * stride + i];
+      break;
+    }
+    default:
+      throw std::logic_error("unknown batch request");
+  }
+}
+
+// Run shared graphs of PDHG attempts until some iterating instance halts.
+void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
+  Timer tm_(t_iter_);
+  if (!bgraph_exec_) capture_batch_graph();
+  std::vector<uint8_t> iterating(K_, 0);
+  for (Inst* I : its) iterating[I->k] = 1;
+  PdhgState* hs = stage<PdhgState>(K_);
+  double* hps = stage<double>(K_);
+  double* hds = stage<double>(K_);
+  uint8_t* hl = stage<uint8_t>(K_);
+  int32_t* hc = stage<int32_t>(4);
+  int64_t to_check = 1 << 20;
+  for (int64_t k = 0; k < K_; ++k) {
+    PdhgState s = inst_[k].S;
+    s.active = iterating[k] ? 1 : 0;
+    s.do_reflect = 0;
+    hs[k] = s;
+    hps[k] = s.ps;
+    hds[k] = s.ds;
+    hl[k] = (uint8_t)s.active;
+    if (iterating[k] && s.check_freq > 0) to_check = std::min<int64_t>(to_check, s.check_freq - (s.iter % s.check_freq));
+  }
+  hc[0] = (int32_t)its.size();
+  hc[1] = 0;
+  hc[2] = 0;
+  hc[3] = 0;
+  PDCS_CUDA(cudaMemcpyAsync(sts_, hs, sizeof(PdhgState) * K_, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(ps_, hps, sizeof(double) * K_, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(ds_, hds, sizeof(double) * K_, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(live_, hl, K_, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(live_cnt_, hc, 4 * sizeof(int32_t), cudaMemcpyHostToDevice, s_));
+  int64_t graphs = (to_check + attempts_per_graph_ - 1) / attempts_per_graph_;
+  graphs = std::max<int64_t>(1, std::min<int64_t>(graphs, 4));
+  for (int64_t gi = 0; gi < graphs; ++gi) {
+    PDCS_CUDA(cudaGraphLaunch(bgraph_exec_, s_));
+    graphs_++;
+    kernels_ += 6LL * attempts_per_graph_;
+  }
+  PdhgState* back = stage<PdhgState>(K_);
+  PDCS_CUDA(cudaMemcpyAsync(back, sts_, sizeof(PdhgState) * K_, cudaMemcpyDeviceToHost, s_));
+  sync_reset();  // `back` stays readable: nothing is staged before the loop below ends
+  const bool timeout = O.time_limit > 0 && now_s() - t_start_ > O.time_limit;
+  std::vector<Inst*> halted;
+  for (Inst* I : its) {
+    I->S = back[I->k];
+    I->S.do_reflect = 0;  // applied by the graph's reflection kernel
+    I->S.done_ctas = 0;
+    if (!I->S.active || timeout) halted.push_back(I);
+  }
+  for (Inst* I : halted) resume(*I);
+}
+
+void BatchSolver::schedule() {
+  for (auto& I : inst_) I.task = main_task(I);
+  for (auto& I : inst_) {
+    I.task.start();
+    I.task.rethrow();
+  }
+  std::vector<Inst*> svc, its;
+  while (true) {
+    svc.clear();
+    its.clear();
+    for (auto& I : inst_) {
+      if (I.task.done()) continue;
+      if (I.req.key.type == RQ_ITERATE) its.push_back(&I);
+      else svc.push_back(&I);
+    }
+    if (svc.empty() && its.empty()) break;
+    if (!svc.empty()) {
+      // group identical requests (hash buckets, verified byte-wise)
+      std::unordered_map<uint64_t, std::vector<std::vector<Inst*>>> buckets;
+      std::vector<std::vector<Inst*>*> order;
+      for (Inst* I : svc) {
+        auto& lists = buckets[I->req.hash];
+        bool placed = false;
+        for (auto& l : lists)
+          if (std::memcmp(&l[0]->req.key, &I->req.key, sizeof(ReqPayload)) == 0) {
+            l.push_back(I);
+            placed = true;
+            break;
+          }
+        if (!placed) lists.push_back({I});
+      }
+      for (auto& kv : buckets)
+        for (auto& l : kv.second) order.push_back(&l);
+      std::sort(order.begin(), order.end(), [](auto* a, auto* b) { return (*a)[0]->k < (*b)[0]->k; });
+      for (auto* l : order) {
+        exec_group(*l);
+        for (Inst* I : *l) resume(*I);
+      }
+      continue;
+    }
+    exec_iterate(its);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per-instance algorithm: the single solver's main loop with device work
+// expressed as requests.
+// ---------------------------------------------------------------------------
+Co<> BatchSolver::lin(Inst& I, std::vector<Lin> ops) {
+  ReqPayload p = payload(RQ_LIN);
+  for (const Lin& o : ops) {
+    if (p.count == 6) {
+      co_await post(I, p);
+      p = payload(RQ_LIN);
+    }
+    LinOp& l = p.lin[p.count++];
+    l.dst = o.dst;
+    l.a = o.a;
+    l.u = o.u;
+    l.b = o.b;
+    l.v = o.v;
+    l.side = o.side;
+  }
+  if (p.count) co_await post(I, p);
+}
+
+Co<> BatchSolver::converge_info(Inst& I, const double* xs, const double* ys, Converge& C, double* gxs,
+                                double* atys) {
+  ReqPayload p = payload(RQ_CONVERGE);
+  p.p[0] = xs;
+  p.p[1] = ys;
+  p.p[2] = gxs;
+  p.p[3] = atys;
+  co_await post(I, p);
+  const double* r = I.req.out;
+  const double *rp = r, *rd = r + 7;
+  double pobj = r[14], hy = r[15];
+  double dobj = hy + rd[6];
+  C.pobj = pobj;
+  C.dobj = dobj;
+  C.abs_gap = std::fabs(pobj - dobj);
+  C.rel_gap = C.abs_gap / (1.0 + std::max(std::fabs(pobj), std::fabs(dobj)));
+  double l2p = std::sqrt(rp[0]), linfp = rp[1], axinf = rp[4], axnrm1 = rp[5];
+  double l2d = std::sqrt(rd[0]), linfd = rd[1], sinf = rd[2], snrm1 = rd[3], atyinf = rd[4], atynrm1 = rd[5];
+  C.l2_abs_p = l2p;
+  C.linf_abs_p = linfp;
+  C.l2_abs_d = l2d;
+  C.linf_abs_d = linfd;
+  C.l2_rel_p = l2p / (1.0 + std::max(snrm1, std::max(I.hNrm1, axnrm1)));
+  C.linf_rel_p = linfp / (1.0 + std::max(sinf, std::max(I.hNrmInf, axinf)));
+  C.l2_rel_d = l2d / (1.0 + std::max(I.cNrm1, atynrm1));
+  C.linf_rel_d = linfd / (1.0 + std::max(I.cNrmInf, atyinf));
+}
+
+// exit_condition_check_diagonal! (rpdhg_alg_gpu_gen_scaling.jl:309-352) with the
+// infeasibility information (:185-248), as Solver::exit_check
+// the reference pushes the objective trends with probability 1/4
+static void push_trend(const Inst& I, Infea& F) {
+  if (I.check_count % 4 == 1) {
+    F.ptrend.push_back(I.ci[0].pobj);
+    F.dtrend.push_back(I.ci[0].dobj);
+    if (F.ptrend.size() > 20) F.ptrend.erase(F.ptrend.begin());
+    if (F.dtrend.size() > 20) F.dtrend.erase(F.dtrend.begin());
+  }
+}
+
+Co<> BatchSolver::exit_check(Inst& I) {
+  double *gxc = tm[0], *gxm = tm[1], *atc = tn[0], *atm = tn[1];
+  co_await converge_info(I, x, y, I.ci[0], gxc, atc);
+  co_await converge_info(I, xm, ym, I.ci[1], gxm, atm);
+  I.check_count++;
+  // ray = current - average; G and G' of the difference by linearity
+  double *dxs = tn[2], *dys = tm[2], *gd = tm[3], *ad = tn[3];
+  co_await lin(I, {{dxs, 1.0, x, -1.0, xm, 0}, {dys, 1.0, y, -1.0, ym, 1}, {gd, 1.0, gxc, -1.0, gxm, 1},
+                   {ad, 1.0, atc, -1.0, atm, 0}});
+  double nr[4];
+  {
+    // |x/Dr|_inf, |dx/Dr|_inf; |y/Dl|_inf, |dy/Dl|_inf
+    ReqPayload s = payload(RQ_SEG);
+    s.X.a[0] = x; s.X.sa[0] = Dr; s.X.kind[0] = SK_MAXABS;
+    s.X.a[1] = dxs; s.X.sa[1] = Dr; s.X.kind[1] = SK_MAXABS;
+    s.X.count = 2;
+    s.Y.a[0] = y; s.Y.sa[0] = Dl; s.Y.kind[0] = SK_MAXABS;
+    s.Y.a[1] = dys; s.Y.sa[1] = Dl; s.Y.kind[1] = SK_MAXABS;
+    s.Y.count = 2;
+    co_await post(I, s);
+    for (int i = 0; i < 4; ++i) nr[i] = I.req.out[i];
+  }
+  {
+    // residuals of the ray with its products given (gd = G dx, ad = G' dy)
+    ReqPayload q = payload(RQ_CONVERGE);
+    q.p[0] = dxs;
+    q.p[1] = dys;
+    q.p[2] = gd;
+    q.p[3] = ad;
+    q.side = 1;
+    co_await post(I, q);
+  }
+  const double* r = I.req.out;
+  {
+    Infea& F = I.ii[0];
+    F.primal_ray_obj = I.ci[0].pobj;
+    F.dual_ray_obj = I.ci[0].dobj;
+    F.max_primal_ray_inf = (I.ci[0].pobj < 0.0) ? I.ci[0].linf_abs_p : 1e10;
+    F.max_dual_ray_inf = (I.ci[0].dobj > 0.0) ? I.ci[0].linf_abs_d : 1e10;
+    F.primal_ray_norm = nr[0];
+    F.dual_ray_norm = nr[2];
+    push_trend(I, F);
+  }
+  {
+    Infea& F = I.ii[1];
+    double pobj = r[14];
+    double dobj = r[15] + r[7 + 6];
+    F.primal_ray_obj = pobj;
+    F.dual_ray_obj = dobj;
+    F.max_primal_ray_inf = (pobj < 0.0) ? r[1] : 1e10;
+    F.max_dual_ray_inf = (dobj > 0.0) ? r[7 + 1] : 1e10;
+    F.primal_ray_norm = nr[1];
+    F.dual_ray_norm = nr[3];
+    push_trend(I, F);
+  }
+  termination_check(I.ci, I.ii, I.S.iter, O, now_s() - t_start_, I.exit_code, I.pobj, I.dobj, I.returned_seq);
+}
+
+Co<double> BatchSolver::mnorm(Inst& I, const double* dx, const double* dy, double ta, double si) {
+  ReqPayload p = payload(RQ_MNORM);
+  p.p[0] = dx;
+  p.p[1] = dy;
+  p.p[2] = tm[4];
+  co_await post(I, p);
+  const double* r = I.req.out;
+  co_return r[2] / ta - 2.0 * r[0] + r[1] / si;
+}
+
+Co<double> BatchSolver::binary_search(Inst& I, double r, const double* px, const double* py, double ta,
+                                      double si) {
+  double *h1 = tn[2], *h2 = tm[2], *xs = tn[3], *ys = tm[3], *gpx = tm[1], *gxs = tm[4];
+  {
+    ReqPayload a = payload(RQ_SPMV);
+    a.side = 1;
+    a.p[0] = py;
+    a.p[1] = h1;
+    co_await post(I, a);
+    ReqPayload b = payload(RQ_SPMV);
+    b.side = 0;
+    b.p[0] = px;
+    b.p[1] = gpx;
+    co_await post(I, b);
+  }
+  co_await lin(I, {{h1, 1.0, h1, -1.0, c_s, 0}, {h2, -1.0, gpx, 1.0, h_s, 1}});
+  double last_h1dx = 0.0, last_h2dy = 0.0;
+  ReqPayload pr = payload(RQ_PROBE);
+  pr.p[0] = px;
+  pr.p[1] = py;
+  pr.p[2] = h1;
+  pr.p[3] = h2;
+  pr.p[4] = gpx;
+  pr.p[5] = xs;
+  pr.p[6] = ys;
+  pr.p[7] = gxs;
+  double t = I.bs_t0, tR = t, tL = 0.0;
+  for (int k = 1; k <= 1000; ++k) {
+    double val = co_await approx(I, pr, ta, si, last_h1dx, last_h2dy, t);
+    if (val > r && val < r + 1e-6) {
+      tR = t;
+      tL = std::max(t - 0.01, 0.0);
+      val = co_await approx(I, pr, ta, si, last_h1dx, last_h2dy, tL);
+      if (val < r) break;
+    }
+    if (val < r && val > r - 1e-6) {
+      tL = t;
+      tR = t + 0.01;
+      val = co_await approx(I, pr, ta, si, last_h1dx, last_h2dy, tR);
+      if (val > r) break;
+    }
+    if (val > r) break;
+    t *= 2;
+  }
+  double tM = 0.5 * (tR + tL);
+  int64_t count = 0;
+  while (tR - tL > 1e-6) {
+    tM = 0.5 * (tR + tL);
+    const double v = co_await approx(I, pr, ta, si, last_h1dx, last_h2dy, tM);
+    if (v < r) tL = tM;
+    else tR = tM;
+    if (++count > 1000000) break;
+  }
+  I.bs_t0 = tM;
+  co_return (last_h1dx + last_h2dy) / r;
+}
+
+// one evaluation of the binary search at t (approx of Solver::binary_search)
+Co<double> BatchSolver::approx(Inst& I, const ReqPayload& pr, double ta, double si, double& h1dx, double& h2dy,
+                               double t) {
+  I.probes++;
+  probes_++;
+  co_await post(I, pr, t * ta / 2, t * si / 2);
+  const double* q = I.req.out;
+  h1dx = q[1];
+  h2dy = q[4];
+  co_return q[0] / ta - 2.0 * q[5] + q[3] / si;
+}
+
+Co<> BatchSolver::restart_threshold(Inst& I, bool dgap) {
+  if (dgap) {
+    double *dx = tn[4], *dy = tm[5];
+    co_await lin(I, {{dx, 1.0, x0, -1.0, x0l, 0}, {dy, 1.0, y0, -1.0, y0l, 1}});
+    double r = co_await mnorm(I, dx, dy, I.S.tau, I.S.sigma);
+    I.ndg_r = r;
+    I.ndg_thr = co_await binary_search(I, r, x0, y0, I.S.tau, I.S.sigma);
+    if (I.ndg_thr < 0) I.dgap_flag = false;
+  } else {
+    co_await converge_info(I, x, y, I.ci[0], tm[0], tn[0]);
+    I.kkt_thr = kkt_error_i(I, I.ci[0]);
+  }
+}
+
+Co<bool> BatchSolver::restart_check(Inst& I, bool dgap) {
+  if (dgap) {
+    double *dx = tn[4], *dy = tm[5];
+    co_await lin(I, {{dx, 1.0, x, -1.0, x0, 0}, {dy, 1.0, y, -1.0, y0, 1}});
+    double rl = co_await mnorm(I, dx, dy, I.S.tau, I.S.sigma);
+    double rho = co_await binary_search(I, rl, x, y, I.S.tau, I.S.sigma);
+    double rho_m = co_await binary_search(I, rl, xm, ym, I.S.tau, I.S.sigma);
+    I.ndg[0] = rho;
+    I.ndg[1] = rho_m;
+    const double betas[2] = {0.4, 0.8};
+    for (int bi = 0; bi < 2; ++bi) {
+      const double beta = betas[bi];
+      if (rho < beta * I.ndg_thr || rho_m < beta * I.ndg_thr) {
+        I.restart_used++;
+        if (I.ndg[0] < I.ndg[1] && I.dgap_flag) co_await lin(I, {{xm, 1.0, x, 0.0, nullptr, 0}, {ym, 1.0, y, 0.0, nullptr, 1}});
+        co_return true;
+      }
+    }
+  } else {
+    co_await converge_info(I, x, y, I.ci[0], tm[0], tn[0]);
+    co_await converge_info(I, xm, ym, I.ci[1], tm[1], tn[1]);
+    double lag0 = I.kkt_err[0], lag1 = I.kkt_err[1];
+    double e0 = kkt_error_i(I, I.ci[0]), e1 = kkt_error_i(I, I.ci[1]);
+    I.kkt_err[0] = e0;
+    I.kkt_err[1] = e1;
+    bool c1 = e0 < 0.4 * I.kkt_thr || e1 < 0.4 * I.kkt_thr;
+    bool c2 = (e0 < 0.8 * I.kkt_thr && e0 > lag0) || (e1 < 0.8 * I.kkt_thr && e1 > lag1);
+    if (c1 || c2) {
+      I.restart_used++;
+      if (I.kkt_err[0] < I.kkt_err[1]) co_await lin(I, {{xm, 1.0, x, 0.0, nullptr, 0}, {ym, 1.0, y, 0.0, nullptr, 1}});
+      co_return true;
+    }
+  }
+  if ((double)I.S.inner >= (double)I.S.iter * 0.223 && I.S.iter > 100000) {
+    I.restart_used++;
+    co_return true;
+  }
+  co_return false;
+}
+
+Co<> BatchSolver::omega_update(Inst& I, const double* xds, const double* yds) {
+  ReqPayload p = payload(RQ_SEG);
+  p.X.a[0] = xds; p.X.b[0] = x; p.X.kind[0] = SK_DIFF2;
+  p.X.count = 1;
+  p.Y.a[0] = yds; p.Y.b[0] = y; p.Y.kind[0] = SK_DIFF2;
+  p.Y.count = 1;
+  co_await post(I, p);
+  double xn = std::sqrt(I.req.out[0]), yn = std::sqrt(I.req.out[1]), om = I.S.omega;
+  const int64_t ru = I.restart_used;
+  if ((om > 1e4 || om < 1e-4) && ru % 20 == 0 && ru != 0) I.S.omega = I.omega0;
+  else if ((om > 3e4 || om < 1.0 / 3e4) && ru % 10 == 0 && ru != 0) I.S.omega = I.omega0;
+  else if (xn > 1e-10 && yn > 1e-10) I.S.omega = std::exp(0.5 * std::log(yn / xn) + 0.5 * std::log(om));
+}
+
+Co<> BatchSolver::iterate(Inst& I) {
+  ReqPayload p = payload(RQ_ITERATE);
+  co_await post(I, p);
+}
+
+Co<> BatchSolver::main_task(Inst& I) {
+  PdhgState& S = I.S;
+  co_await converge_info(I, x, y, I.ci[0], tm[0], tn[0]);  // rpdhg_alg_gpu_gen.jl:1865-1881
+  co_await lin(I, {{x0, 1.0, x, 0.0, nullptr, 0}, {y0, 1.0, y, 0.0, nullptr, 1},
+                   {x0l, 1.0, x, 0.0, nullptr, 0}, {y0l, 1.0, y, 0.0, nullptr, 1}});
+  S = PdhgState{};
+  S.omega = I.omega0;
+  S.eta_p = 1.0 / I.ginf;
+  S.tau = 0.9;
+  S.sigma = 0.9;
+  S.check_freq = O.check_terminate_freq;
+  S.attempt_limit = O.attempt_limit;
+  int64_t rf = 0;
+  if (O.use_duality_gap_restart) rf = O.duality_gap_restart_freq;
+  if (O.use_kkt_restart) rf = rf ? std::min(rf, O.kkt_restart_freq) : O.kkt_restart_freq;
+  S.restart_freq = rf;
+  S.restart_enabled = rf > 0;
+  for (int64_t outer = 1; outer <= O.max_outer_iter; ++outer) {
+    const bool bx = I.ci[0].l2_rel_p < I.pres_best, by = I.ci[0].l2_rel_d < I.dres_best;
+    if (bx) I.pres_best = I.ci[0].l2_rel_p;
+    if (by) I.dres_best = I.ci[0].l2_rel_d;
+    if (bx && by) co_await lin(I, {{xbest, 1.0, x, 0.0, nullptr, 0}, {ybest, 1.0, y, 0.0, nullptr, 1}});
+    else if (bx) co_await lin(I, {{xbest, 1.0, x, 0.0, nullptr, 0}});
+    else if (by) co_await lin(I, {{ybest, 1.0, y, 0.0, nullptr, 1}});
+    I.max_kkt = std::max(std::max(I.ci[0].l2_rel_p, I.ci[0].l2_rel_d), I.ci[0].rel_gap);
+    I.min_kkt = std::min(std::min(std::min(I.ci[0].l2_rel_p, I.ci[0].l2_rel_d), I.ci[0].rel_gap), I.min_kkt);
+    double extra = -0.1 * std::log10(I.max_kkt) + 0.2;
+    co_await lin(I, {{x0l, 1.0, x0, 0.0, nullptr, 0}, {y0l, 1.0, y0, 0.0, nullptr, 1},
+                     {x0, 1.0, xm, 0.0, nullptr, 0}, {y0, 1.0, ym, 0.0, nullptr, 1},
+                     {x, 1.0, xm, 0.0, nullptr, 0}, {y, 1.0, ym, 0.0, nullptr, 1}});
+    if (O.use_kkt_restart) co_await restart_threshold(I, false);
+    else co_await restart_threshold(I, I.dgap_flag);
+    {
+      double pd = I.ci[0].l2_rel_p / I.ci[0].l2_rel_d;
+      bool f1 = outer > 10 && I.max_kkt > 1e5;
+      bool f2 = outer > 80 && (pd > 1e10 || pd < 1e-10);
+      bool f3 = outer > 10 && S.tau < 1e-6 && S.sigma < 1e-6;
+      bool f4 = S.iter > 1000000 && I.ci[0].rel_gap > 0.98 && I.ci[0].l2_rel_p > 1.0 && I.ci[0].l2_rel_d > 1.0;
+      if (f1 || f2 || f3 || f4 || O.force_resolving) {
+        I.needs_single = true;  // resolving fallback: the instance is re-solved on its own
+        co_return;
+      }
+    }
+    co_await lin(I, {{xl, 1.0, x, 0.0, nullptr, 0}, {yl, 1.0, y, 0.0, nullptr, 1},
+                     {xds_, 1.0, x, 0.0, nullptr, 0}, {yds_, 1.0, y, 0.0, nullptr, 1}});
+    S.inner = 0;
+    S.eta_cum = 0.0;
+    S.extra = extra;
+    S.dec = std::min(0.9 + 0.1 * std::log10(I.max_kkt * 1e5), 1.0);
+    S.dec_next = S.dec;
+    S.eta = std::max(S.eta_p, 1e-6);
+    S.reject_count = 0;
+    S.ps = (S.eta / S.omega) * S.dec;
+    S.ds = (S.eta * S.omega) * S.dec;
+    S.active = 1;
+    S.halt_reason = HALT_NONE;
+    S.do_reflect = 0;
+    bool restart = false;
+    while (!restart) {
+      co_await iterate(I);
+      if (O.time_limit > 0 && now_s() - t_start_ > O.time_limit && S.active) {
+        I.exit_code = PDCS_EXIT_TIME_LIMIT;
+        co_return;
+      }
+      int reason = S.halt_reason;
+      S.halt_reason = HALT_NONE;
+      if (reason == HALT_LIMIT) {
+        I.exit_code = PDCS_EXIT_ATTEMPT_LIMIT;
+        co_return;
+      }
+      if (reason == HALT_CHECK) {
+        co_await exit_check(I);
+        I.max_kkt = std::max(std::max(I.ci[0].l2_rel_p, I.ci[0].l2_rel_d), I.ci[0].rel_gap);
+        S.dec_next = std::min(0.9 + 0.1 * std::log10(I.max_kkt * 1e5), 1.0);
+        if (I.exit_code != PDCS_EXIT_CONTINUE) co_return;
+        if (S.attempt_limit > 0 && S.iter >= S.attempt_limit) {
+          I.exit_code = PDCS_EXIT_ATTEMPT_LIMIT;
+          co_return;
+        }
+        if (S.accepted) {
+          post_accept(S, false);
+        } else {
+          after_reject(S);
+          if (S.reject_count > 1000000) {
+            S.eta = S.eta_p;
+            post_accept(S, true);
+          }
+        }
+        if (S.do_reflect) {
+          co_await post(I, payload(RQ_REFLECT));
+          S.do_reflect = 0;
+        }
+        reason = S.halt_reason;
+        S.halt_reason = HALT_NONE;
+        if (reason == HALT_NONE) {
+          S.active = 1;
+          continue;
+        }
+      }
+      if (reason == HALT_ARTIFICIAL) {
+        I.restart_used++;
+        restart = true;
+        break;
+      }
+      if (reason == HALT_RESTART_CHECK) {
+        bool brk = false;
+        if (O.use_kkt_restart && O.kkt_restart_freq > 0 && S.iter % O.kkt_restart_freq == 0) {
+          const bool rs = co_await restart_check(I, false);
+          if (rs || outer == 1) brk = true;
+        }
+        if (!brk && O.use_duality_gap_restart && O.duality_gap_restart_freq > 0 &&
+            S.iter % O.duality_gap_restart_freq == 0) {
+          const bool rs = co_await restart_check(I, I.dgap_flag);
+          if (rs || outer == 1) brk = true;
+        }
+        if (brk) {
+          restart = true;
+          break;
+        }
+        S.active = 1;
+        continue;
+      }
+    }
+    co_await omega_update(I, xds_, yds_);
+  }
+  I.exit_code = PDCS_EXIT_MAX_ITER;
+}
+
+int BatchSolver::run_batch(pdcs_result* res, pdcs_batch_info* info) {
+  int rc = validate_batch();
+  if (rc != PDCS_OK) return rc;
+  const double t0 = now_s();
+  merge();
+  rc = validate();
+  if (rc != PDCS_OK) return rc;
+  setup();
+  setup_batch();
+  t_start_ = now_s();
+  schedule();
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  // outputs: unscaled current or averaged iterate per instance, scattered to the callers' buffers
+  uint8_t* hpick = stage<uint8_t>(K_);
+  for (int64_t k = 0; k < K_; ++k) {
+    const Inst& I = inst_[k];
+    hpick[k] = (I.exit_code == PDCS_EXIT_OPTIMAL && I.returned_seq == 1) ? 1 : 0;
+  }
+  PDCS_CUDA(cudaMemcpyAsync(mask_, hpick, K_, cudaMemcpyHostToDevice, s_));
+  double* xo = tn[0];
+  double* yo = tm[0];
+  batch_output_kernel<<<grid_for(n_), kThreads, 0, s_>>>(xo, x, xm, Dr, ix_, mask_, n_);
+  batch_output_kernel<<<grid_for(m_), kThreads, 0, s_>>>(yo, y, ym, Dl, iy_, mask_, m_);
+  std::vector<double> hx(n_), hy(m_);
+  PDCS_CUDA(cudaMemcpyAsync(hx.data(), xo, sizeof(double) * n_, cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaMemcpyAsync(hy.data(), yo, sizeof(double) * m_, cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  const double solve_time = now_s() - t_start_;
+  int64_t fallbacks = 0;
+  for (int64_t k = 0; k < K_; ++k) {
+    const Inst& I = inst_[k];
+    pdcs_result& R = res[k];
+    if (I.needs_single) {
+      // resolving fallback (power method + fixed-step PDHG): the single solver
+      // replays this instance's trajectory and continues with the fallback
+      fallbacks++;
+      pdcs_options o1 = O;
+      o1.stream = nullptr;
+      Solver one(&probs_[k], &o1);
+      int r1 = one.run(&R);
+      if (r1 != PDCS_OK) return r1;
+      continue;
+    }
+    for (int t = 0; t < kMaxRuns; ++t) {
+      const int64_t L = xrun_len_[k * kMaxRuns + t];
+      if (L && R.x)
+        std::memcpy(R.x + xloc_[k * kMaxRuns + t], hx.data() + xrun_start_[k * kMaxRuns + t], sizeof(double) * L);
+      const int64_t Ly = yrun_len_[k * kMaxRuns + t];
+      if (Ly && R.y)
+        std::memcpy(R.y + yloc_[k * kMaxRuns + t], hy.data() + yrun_start_[k * kMaxRuns + t], sizeof(double) * Ly);
+    }
+    const bool mean = hpick[k] != 0;
+    const Converge& C = I.ci[mean ? 1 : 0];
+    const int ec = I.exit_code;
+    R.exit_code = ec;
+    R.returned_sequence = mean ? 1 : 0;
+    R.pObj = (ec == PDCS_EXIT_OPTIMAL || ec == PDCS_EXIT_MAX_ITER) ? C.pobj : I.pobj;
+    R.dObj = (ec == PDCS_EXIT_OPTIMAL || ec == PDCS_EXIT_MAX_ITER) ? C.dobj : I.dobj;
+    R.iter = I.S.iter;
+    R.restart_used = I.restart_used;
+    R.l_inf_rel_primal_res = C.linf_rel_p;
+    R.l_inf_rel_dual_res = C.linf_rel_d;
+    R.rel_gap = C.rel_gap;
+    R.l_2_rel_primal_res = C.l2_rel_p;
+    R.l_2_rel_dual_res = C.l2_rel_d;
+    R.l_inf_abs_primal_res = C.linf_abs_p;
+    R.l_inf_abs_dual_res = C.linf_abs_d;
+    R.abs_gap = C.abs_gap;
+    R.time = solve_time;
+    R.setup_time = t_start_ - t0;
+    R.kernel_launches = kernels_;
+    R.graph_launches = graphs_;
+    R.restart_probes = I.probes;
+  }
+  if (info) {
+    info->setup_time = t_start_ - t0;
+    info->solve_time = solve_time;
+    info->kernel_launches = kernels_;
+    info->graph_launches = graphs_;
+    info->service_rounds = rounds_;
+    info->single_fallbacks = fallbacks;
+    info->time_iterations = t_iter_;
+  }
+  return PDCS_OK;
+}
+
+}  // namespace pdcs

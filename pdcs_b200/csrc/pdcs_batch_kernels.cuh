@@ -1,0 +1,318 @@
+// pdcs_batch_kernels.cuh -- kernels of the batched solver.
+//
+// K independent instances are merged into one block-diagonal program whose
+// vectors are ordered by cone type across instances (all box parts, then all
+// SOC blocks, ...), so the single-instance cone tables, SpMV and projection
+// kernels apply unchanged.  What differs per instance -- step sizes, the
+// eta_bar test, restarts, termination -- lives in an array of PdhgState and in
+// per-instance scalar arrays indexed through per-element instance ids.
+//
+// Every kernel here touches only the elements of the instances selected by a
+// per-instance mask, so requests of different instances (at different points
+// of their own control flow) never disturb each other's data.
+//
+// Reductions are per instance and deterministic: kernels write per-element
+// contributions, and a warp per instance sums its (at most kMaxRuns)
+// contiguous runs in a fixed order.
+#pragma once
+#include "pdcs_kernels.cuh"
+
+namespace pdcs {
+
+// x runs: box, SOC, RSOC, exp, dual-exp; y runs: zero, nonneg, SOC, RSOC, exp, dual-exp
+constexpr int kMaxRuns = 6;
+
+struct RunTable {
+  const int64_t* start;  // K * kMaxRuns
+  const int64_t* len;
+};
+
+// x = P(x_lag + ps[k] (aty - c)); contribution (x - x_lag)^2
+struct OpPrimalStepB {
+  static constexpr int NACC = 1;
+  static constexpr bool kFusedControl = false;
+  __device__ static const int32_t* kinds() { return kSum1; }
+  const double* xl;
+  const double* aty;
+  const double* c;
+  double* out;
+  const int32_t* inst;
+  const uint8_t* mask;
+  const double* ps;
+  double* dxsq;
+  __device__ void load() {}
+  __device__ bool live(int64_t j) const { return mask[inst[j]] != 0; }
+  __device__ double z(int64_t j) const { return xl[j] + ps[inst[j]] * (aty[j] - c[j]); }
+  __device__ void fin(int64_t j, double, double p, double*) const {
+    out[j] = p;
+    const double d = p - xl[j];
+    dxsq[j] = d * d;
+  }
+};
+
+// y = P(y_lag - ds[k] (2 gx - gxl - h)); contributions (y - y_lag)^2, (y - y_lag)(gx - gxl)
+struct OpDualStepB {
+  static constexpr int NACC = 1;
+  static constexpr bool kFusedControl = false;
+  __device__ static const int32_t* kinds() { return kSum1; }
+  const double* yl;
+  const double* gx;
+  const double* gxl;
+  const double* h;
+  double* out;
+  const int32_t* inst;
+  const uint8_t* mask;
+  const double* ds;
+  double* dysq;
+  double* dgdy;
+  __device__ void load() {}
+  __device__ bool live(int64_t i) const { return mask[inst[i]] != 0; }
+  __device__ double z(int64_t i) const { return yl[i] - ds[inst[i]] * ((2.0 * gx[i] - gxl[i]) - h[i]); }
+  __device__ void fin(int64_t i, double, double p, double*) const {
+    out[i] = p;
+    const double d = p - yl[i];
+    dysq[i] = d * d;
+    dgdy[i] = d * (gx[i] - gxl[i]);
+  }
+};
+
+// OpAxpyProj with a per-instance step: out = P(base + alpha[k] dir)
+struct OpAxpyProjB {
+  static constexpr int NACC = 3;
+  static constexpr bool kFusedControl = false;
+  __device__ static const int32_t* kinds() { return kSum3; }
+  const double* base;
+  const double* dir;
+  const double* alpha;
+  double* out;
+  const double* g1;
+  const double* g0;
+  const int32_t* inst;
+  __device__ void load() {}
+  __device__ double z(int64_t j) const { return base[j] + alpha[inst[j]] * dir[j]; }
+  __device__ void fin(int64_t j, double, double p, double* acc) const {
+    out[j] = p;
+    double d = p - base[j];
+    acc[0] = fma(d, d, acc[0]);
+    acc[1] = fma(dir[j], d, acc[1]);
+    if (g1) acc[2] = fma(d, g1[j] - g0[j], acc[2]);
+  }
+};
+
+// Adapter: runs a single-instance op on the masked instances and stores each
+// element's accumulator values (what the op would add for that element) as
+// contributions contrib[r * stride + j], reduced per instance afterwards.
+template <class Op>
+struct PerElem {
+  static constexpr int NACC = 1;
+  static constexpr bool kFusedControl = false;
+  __device__ static const int32_t* kinds() { return kSum1; }
+  Op op;
+  double* out;  // the op's output (scratch of the large-SOC path)
+  double* contrib;
+  int64_t stride;
+  const int32_t* inst;
+  const uint8_t* mask;
+  __device__ void load() { op.load(); }
+  __device__ bool live(int64_t j) const { return mask[inst[j]] != 0; }
+  __device__ double z(int64_t j) const { return op.z(j); }
+  __device__ void fin(int64_t j, double z, double p, double*) const {
+    double a[Op::NACC];
+#pragma unroll
+    for (int r = 0; r < Op::NACC; ++r) a[r] = 0.0;
+    op.fin(j, z, p, a);
+#pragma unroll
+    for (int r = 0; r < Op::NACC; ++r) contrib[r * stride + j] = a[r];
+  }
+};
+
+// Per-instance reductions.  Kinds 0-3 follow dots_kernel (DOT, MAXABS,
+// SUMABS, DIFF2 with the optional divisor sa); SUM / MAX reduce contributions.
+enum SegKind : int32_t { SK_DOT = 0, SK_MAXABS = 1, SK_SUMABS = 2, SK_DIFF2 = 3, SK_SUM = 4, SK_MAX = 5 };
+constexpr int kSegMax = 8;
+
+struct SegSide {
+  const double* a[kSegMax];
+  const double* b[kSegMax];
+  const double* sa[kSegMax];
+  int32_t kind[kSegMax];
+  int32_t count;
+};
+
+__device__ __forceinline__ void seg_side(const SegSide& sp, RunTable rt, int64_t k, int lane, double* out) {
+  double acc[kSegMax];
+#pragma unroll
+  for (int r = 0; r < kSegMax; ++r) acc[r] = 0.0;
+  for (int q = 0; q < kMaxRuns; ++q) {
+    const int64_t s0 = rt.start[k * kMaxRuns + q], L = rt.len[k * kMaxRuns + q];
+    for (int64_t i = s0 + lane; i < s0 + L; i += 32) {
+#pragma unroll
+      for (int r = 0; r < kSegMax; ++r) {
+        if (r >= sp.count) break;
+        double a = sp.a[r][i];
+        if (sp.sa[r]) a /= sp.sa[r][i];
+        switch (sp.kind[r]) {
+          case SK_DOT: acc[r] = fma(a, sp.b[r] ? sp.b[r][i] : a, acc[r]); break;
+          case SK_MAXABS: acc[r] = fmax(acc[r], fabs(a)); break;
+          case SK_SUMABS: acc[r] += fabs(a); break;
+          case SK_DIFF2: { double d = a - sp.b[r][i]; acc[r] = fma(d, d, acc[r]); } break;
+          case SK_SUM: acc[r] += a; break;
+          default: acc[r] = fmax(acc[r], a); break;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kSegMax; ++r) {
+    if (r >= sp.count) break;
+    const bool mx = sp.kind[r] == SK_MAXABS || sp.kind[r] == SK_MAX;
+    double v = acc[r];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double w = __shfl_down_sync(kFull, v, o);
+      v = mx ? fmax(v, w) : v + w;
+    }
+    if (lane == 0) out[r] = v;
+  }
+}
+
+// out[k * stride + r]: x-side results r < X.count, then y-side results
+__global__ void __launch_bounds__(kThreads) seg_reduce_kernel(int64_t K, const uint8_t* __restrict__ mask,
+                                                             RunTable rx, SegSide X, RunTable ry, SegSide Y,
+                                                             double* __restrict__ out, int stride) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < K; k += wstride) {
+    if (mask && !mask[k]) continue;
+    if (X.count) seg_side(X, rx, k, lane, out + k * stride);
+    if (Y.count) seg_side(Y, ry, k, lane, out + k * stride + X.count);
+  }
+}
+
+// Control of one batched attempt.  live_cur / live_next: the number of live
+// instances at the start of this attempt and of the next one (two slots used
+// alternately by consecutive attempts of a graph).  A warp per instance sums
+// its contributions in a fixed order and runs the shared control_step.
+struct BatchCtl {
+  PdhgState* sts;
+  double* ps;
+  double* ds;
+  uint8_t* live;
+  RunTable rx, ry;
+  const double* dxsq;
+  const double* dysq;
+  const double* dgdy;
+  int32_t* live_cur;
+  int32_t* live_next;
+  uint32_t* done_ctas;
+  int32_t* live_accum;
+};
+
+__global__ void __launch_bounds__(kThreads) batch_control_kernel(int64_t K, BatchCtl c) {
+  if (*c.live_cur == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *c.live_next = 0;
+    return;
+  }
+  const int lane = threadIdx.x & 31;
+  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  int nlive = 0;
+  for (int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < K; k += wstride) {
+    if (!c.live[k]) {
+      // no step ran for this instance: nothing to reflect
+      if (lane == 0) c.sts[k].do_reflect = 0;
+      continue;
+    }
+    double a = 0.0, b = 0.0, d = 0.0;
+    for (int q = 0; q < kMaxRuns; ++q) {
+      const int64_t s0 = c.rx.start[k * kMaxRuns + q], L = c.rx.len[k * kMaxRuns + q];
+      for (int64_t i = s0 + lane; i < s0 + L; i += 32) a += c.dxsq[i];
+      const int64_t t0 = c.ry.start[k * kMaxRuns + q], M = c.ry.len[k * kMaxRuns + q];
+      for (int64_t i = t0 + lane; i < t0 + M; i += 32) {
+        b += c.dysq[i];
+        d += c.dgdy[i];
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(kFull, a, o);
+      b += __shfl_down_sync(kFull, b, o);
+      d += __shfl_down_sync(kFull, d, o);
+    }
+    if (lane == 0) {
+      PdhgState s = c.sts[k];
+      control_step(s, a, b, d);
+      c.sts[k] = s;
+      c.ps[k] = s.ps;
+      c.ds[k] = s.ds;
+      c.live[k] = s.active ? 1 : 0;
+      nlive += s.active ? 1 : 0;
+    }
+  }
+  // count the instances still live; the last CTA publishes the count
+  __shared__ int sh[kWarps];
+  for (int o = 16; o > 0; o >>= 1) nlive += __shfl_down_sync(kFull, nlive, o);
+  if (lane == 0) sh[threadIdx.x >> 5] = nlive;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < kWarps; ++w) t += sh[w];
+    atomicAdd(c.live_accum, t);
+    __threadfence();
+    if (atomicAdd(c.done_ctas, 1u) == gridDim.x - 1) {
+      __threadfence();
+      *c.live_next = atomicExch(c.live_accum, 0);
+      *c.done_ctas = 0;
+    }
+  }
+}
+
+// Reflection + eta-weighted averaging with per-instance coefficients
+// (reflect_kernel per instance); runs when the attempt's control step ran.
+__global__ void __launch_bounds__(kThreads) batch_reflect_kernel(const int32_t* __restrict__ live_cur,
+                                                                const PdhgState* __restrict__ sts,
+                                                                const int32_t* __restrict__ ix,
+                                                                const int32_t* __restrict__ iy,
+                                                                double* __restrict__ x, double* __restrict__ xl,
+                                                                double* __restrict__ xm, int64_t n,
+                                                                double* __restrict__ y, double* __restrict__ yl,
+                                                                double* __restrict__ ym, int64_t m) {
+  if (live_cur && *live_cur == 0) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += stride) {
+    const bool isx = i < n;
+    const int64_t j = isx ? i : i - n;
+    const PdhgState& s = sts[isx ? ix[j] : iy[j]];
+    if (!s.do_reflect) continue;
+    double* v = isx ? x : y;
+    double* vl = isx ? xl : yl;
+    double* vm = isx ? xm : ym;
+    const double tmp = s.refl_tmp, inv = s.refl_inv, e = s.refl_extra, eta = s.refl_eta, cum = s.refl_cum;
+    const double cur = v[j];
+    const double nv = tmp * ((1.0 + e) * cur - e * vl[j]) + inv * cur;
+    vm[j] = (vm[j] * cum + nv * eta) / (cum + eta);
+    v[j] = nv;
+    vl[j] = nv;
+  }
+}
+
+// out = a[k] u + b[k] v on the elements of masked instances (v may be NULL)
+__global__ void masked_axpby_kernel(double* __restrict__ out, const double* __restrict__ a,
+                                    const double* __restrict__ u, const double* __restrict__ b,
+                                    const double* __restrict__ v, const int32_t* __restrict__ inst,
+                                    const uint8_t* __restrict__ mask, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int32_t k = inst[i];
+    if (!mask[k]) continue;
+    out[i] = a[k] * u[i] + (v ? b[k] * v[i] : 0.0);
+  }
+}
+
+// unscaled output: out = (pick[k] ? vm : v) / D
+__global__ void batch_output_kernel(double* __restrict__ out, const double* __restrict__ v,
+                                    const double* __restrict__ vm, const double* __restrict__ D,
+                                    const int32_t* __restrict__ inst, const uint8_t* __restrict__ pick, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    out[i] = (pick[inst[i]] ? vm[i] : v[i]) / D[i];
+}
+
+}  // namespace pdcs

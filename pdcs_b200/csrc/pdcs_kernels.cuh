@@ -101,12 +101,15 @@ struct CsrDev {
   int32_t cta0[kBins + 1];   // first CTA of each bin, cta0[kBins] = grid size
 };
 
-template <int NV>
+// MASK: rows whose instance (row_inst) has imask == 0 are skipped (batched solver).
+template <int NV, bool MASK = false>
 __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const double* __restrict__ x0,
                                                               const double* __restrict__ x1,
                                                               double* __restrict__ y0, double* __restrict__ y1,
                                                               const int32_t* __restrict__ active,
-                                                              int32_t* __restrict__ clear_flag = nullptr) {
+                                                              int32_t* __restrict__ clear_flag = nullptr,
+                                                              const int32_t* __restrict__ row_inst = nullptr,
+                                                              const uint8_t* __restrict__ imask = nullptr) {
   // first kernel of a PDHG attempt: the previous attempt's reflection (if any)
   // has run by now, so its flag is cleared here, before the halt check
   if (clear_flag && blockIdx.x == 0 && threadIdx.x == 0) *clear_flag = 0;
@@ -127,8 +130,9 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const d
     const int64_t warp_first = r0 + (int64_t)lcta * rows_per_cta + (threadIdx.x >> 5) * (32 / g);
     for (int64_t qb = warp_first; qb < r1; qb += (int64_t)ncta * rows_per_cta) {
       const int64_t q = qb + (threadIdx.x & 31) / g;
-      const bool valid = q < r1;
+      bool valid = q < r1;
       const int32_t row = valid ? A.perm[q] : 0;
+      if (MASK && valid) valid = imask[row_inst[row]] != 0;
       const int32_t kb = valid ? A.rp[row] : 0, ke = valid ? A.rp[row + 1] : 0;
       double s0 = 0.0, s1 = 0.0, t0 = 0.0, t1 = 0.0;
       int32_t k = kb + lane_g;
@@ -163,6 +167,7 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const d
     __shared__ double red0[kWarps], red1[kWarps];
     for (int64_t q = r0 + lcta; q < r1; q += ncta) {
       const int32_t row = A.perm[q];
+      if (MASK && !imask[row_inst[row]]) continue;  // CTA-uniform
       const int32_t kb = A.rp[row], ke = A.rp[row + 1];
       double s0 = 0.0, s1 = 0.0;
       for (int32_t k = kb + threadIdx.x; k < ke; k += kThreads) {
@@ -251,35 +256,14 @@ __device__ inline void block_reduce_store(double (&acc)[N], const int32_t* kinds
   }
 }
 
-// The control step of one PDHG attempt (rpdhg_alg_gpu_gen_scaling.jl:711-765):
-// reduce the step's partial sums (fixed order), form eta_bar and eta', decide
-// accept / retry / halt.  Run by one CTA of kThreads threads.
-__device__ inline void control_block(PdhgState* st, const double* px, int nbx, const double* py, int nby) {
-  __shared__ double sh[3][kThreads];
-  double a = 0.0, b = 0.0, c = 0.0;
-  for (int i = threadIdx.x; i < nbx; i += kThreads) a += __ldcg(px + i);
-  for (int i = threadIdx.x; i < nby; i += kThreads) {
-    b += __ldcg(py + i);
-    c += __ldcg(py + nby + i);
-  }
-  sh[0][threadIdx.x] = a;
-  sh[1][threadIdx.x] = b;
-  sh[2][threadIdx.x] = c;
-  __syncthreads();
-  for (int s2 = kThreads / 2; s2 > 0; s2 >>= 1) {
-    if (threadIdx.x < s2) {
-      sh[0][threadIdx.x] += sh[0][threadIdx.x + s2];
-      sh[1][threadIdx.x] += sh[1][threadIdx.x + s2];
-      sh[2][threadIdx.x] += sh[2][threadIdx.x + s2];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x != 0) return;
-  PdhgState s = *st;
-  s.done_ctas = 0;
-  s.sum_dx2 = sh[0][0];
-  s.sum_dy2 = sh[1][0];
-  s.sum_dgdy = sh[2][0];
+// The control step of one PDHG attempt (rpdhg_alg_gpu_gen_scaling.jl:711-765)
+// given the step's sums a = |dx|^2, b = |dy|^2, c = dy'(G x - G x_lag): form
+// eta_bar and eta', decide accept / retry / halt.  Shared by the single-
+// instance control block and the per-instance control of the batched solver.
+__device__ inline void control_step(PdhgState& s, double a, double b, double c) {
+  s.sum_dx2 = a;
+  s.sum_dy2 = b;
+  s.sum_dgdy = c;
   s.do_reflect = 0;
   double num = s.omega * s.sum_dx2 + s.sum_dy2 / s.omega;
   double den = 2.0 * fabs(s.sum_dgdy);
@@ -308,7 +292,6 @@ __device__ inline void control_block(PdhgState* st, const double* px, int nbx, c
       s.halt_reason = HALT_LIMIT;
       s.active = 0;
     }
-    *st = s;
     return;
   }
   s.tau = s.eta / s.omega;
@@ -329,8 +312,40 @@ __device__ inline void control_block(PdhgState* st, const double* px, int nbx, c
       post_accept(s, true);
     }
   }
+}
+
+// Reduce the step's partial sums (fixed order) and run control_step; one CTA of kThreads threads.
+__device__ inline void control_block(PdhgState* st, const double* px, int nbx, const double* py, int nby) {
+  __shared__ double sh[3][kThreads];
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int i = threadIdx.x; i < nbx; i += kThreads) a += __ldcg(px + i);
+  for (int i = threadIdx.x; i < nby; i += kThreads) {
+    b += __ldcg(py + i);
+    c += __ldcg(py + nby + i);
+  }
+  sh[0][threadIdx.x] = a;
+  sh[1][threadIdx.x] = b;
+  sh[2][threadIdx.x] = c;
+  __syncthreads();
+  for (int s2 = kThreads / 2; s2 > 0; s2 >>= 1) {
+    if (threadIdx.x < s2) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + s2];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + s2];
+      sh[2][threadIdx.x] += sh[2][threadIdx.x + s2];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  PdhgState s = *st;
+  s.done_ctas = 0;
+  control_step(s, sh[0][0], sh[1][0], sh[2][0]);
   *st = s;
 }
+
+// Ops of the batched solver restrict work to the elements of selected
+// instances: live(j) is false for elements that must not be read or written.
+template <class Op>
+concept MaskedOp = requires(const Op& o) { o.live(int64_t(0)); };
 
 // Generic update + projection.  Op supplies:
 //   NACC, kinds[] (ACC_SUM / ACC_MAX), double* out (result / scratch, length T.len),
@@ -351,6 +366,9 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
       const int64_t j0 = T.seg_start[s], j1 = j0 + T.seg_len[s];
       const int32_t kind = T.seg_kind[s];
       for (int64_t j = j0 + (int64_t)b * kThreads + threadIdx.x; j < j1; j += stride) {
+        if constexpr (MaskedOp<Op>) {
+          if (!op.live(j)) continue;
+        }
         double z = op.z(j);
         double p = elem_proj(kind, z, j, T);
         op.fin(j, z, p, acc);
@@ -361,6 +379,9 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
     const int64_t wstride = (int64_t)T.ctaB * kWarps;
     for (int64_t k = (int64_t)(b - T.ctaA) * kWarps + (threadIdx.x >> 5); k < T.nwc; k += wstride) {
       const int64_t st = T.wc_start[k];
+      if constexpr (MaskedOp<Op>) {
+        if (!op.live(st)) continue;  // warp-uniform: a cone belongs to one instance
+      }
       const int32_t d = T.wc_len[k];
       const bool rsoc = T.wc_kind[k] == PK_RSOC;
       const double* S = T.S ? T.S + st : nullptr;
@@ -429,6 +450,9 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
     for (int64_t k = (int64_t)(b - T.ctaA - T.ctaB) * kThreads + threadIdx.x; k < total; k += tstride) {
       const bool first = k < T.exp_count;
       const int64_t j = first ? T.exp_base + 3 * k : T.dexp_base + 3 * (k - T.exp_count);
+      if constexpr (MaskedOp<Op>) {
+        if (!op.live(j)) continue;
+      }
       const int32_t kind = first ? T.exp_kind : T.dexp_kind;
       double z0 = op.z(j), z1 = op.z(j + 1), z2 = op.z(j + 2);
       double r = z0, s = z1, t = z2;

@@ -354,7 +354,7 @@ struct Infea {
 class Solver {
  public:
   Solver(const pdcs_problem* p, const pdcs_options* o) : P(*p), O(*o) {}
-  ~Solver() {
+  virtual ~Solver() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (graph_) cudaGraphDestroy(graph_);
     if (host_state_) cudaFreeHost(host_state_);
@@ -362,8 +362,9 @@ class Solver {
     if (own_stream_) cudaStreamDestroy(s_);
   }
   int run(pdcs_result* res);
+  int validate_only() { return validate(); }
 
- private:
+ protected:
   pdcs_problem P;
   pdcs_options O;
   Arena A;
@@ -1031,8 +1032,12 @@ void Solver::exit_check() {
   check_termination();
 }
 
-// check_termination_criteria (src/pdcs_gpu/termination.jl:74-260)
-void Solver::check_termination() {
+// check_termination_criteria (src/pdcs_gpu/termination.jl:74-260) on the
+// current (ci[0], ii[0]) and averaged (ci[1], ii[1]) sequences; sets
+// exit_code (PDCS_EXIT_CONTINUE while running), the reported objectives and
+// which sequence is returned.
+static void termination_check(Converge (&ci)[2], Infea (&ii)[2], int64_t iter, const pdcs_options& O,
+                              double elapsed, int& exit_code_, double& pobj_, double& dobj_, int& returned_seq_) {
   auto mono = [](const std::vector<double>& b, bool inc) {
     if (b.size() < 20) return false;
     for (size_t i = 1; i < 20; ++i)
@@ -1071,7 +1076,7 @@ void Solver::check_termination() {
         if (mono(I.dtrend, true)) I.status = PDCS_EXIT_PRIMAL_INFEASIBLE_LOW_ACC;
       }
     }
-    if ((I.status == 2 && S.iter > 2000) || (I.status == 3 && S.iter > 500)) {
+    if ((I.status == 2 && iter > 2000) || (I.status == 3 && iter > 500)) {
       exit_code_ = I.status;
       pobj_ = I.primal_ray_obj;
       dobj_ = I.dual_ray_obj;
@@ -1089,24 +1094,28 @@ void Solver::check_termination() {
         if (mono(I.ptrend, false)) I.status = PDCS_EXIT_DUAL_INFEASIBLE_LOW_ACC;
       }
     }
-    if ((I.status == 4 && S.iter > 2000) || (I.status == 5 && S.iter > 500)) {
+    if ((I.status == 4 && iter > 2000) || (I.status == 5 && iter > 500)) {
       exit_code_ = I.status;
       pobj_ = I.primal_ray_obj;
       dobj_ = I.dual_ray_obj;
       return;
     }
   }
-  if ((double)S.iter >= (double)O.max_outer_iter * (double)O.max_inner_iter) {
+  if ((double)iter >= (double)O.max_outer_iter * (double)O.max_inner_iter) {
     exit_code_ = PDCS_EXIT_MAX_ITER;
     pobj_ = ci[0].pobj;
     dobj_ = ci[0].dobj;
     return;
   }
-  if (O.time_limit > 0 && now_s() - t_start_ > O.time_limit) {
+  if (O.time_limit > 0 && elapsed > O.time_limit) {
     exit_code_ = PDCS_EXIT_TIME_LIMIT;
     return;
   }
   exit_code_ = PDCS_EXIT_CONTINUE;
+}
+
+void Solver::check_termination() {
+  termination_check(ci, ii, S.iter, O, now_s() - t_start_, exit_code_, pobj_, dobj_, returned_seq_);
 }
 
 // Mnorm (rpdhg_alg_gpu_gen.jl:133-138)
@@ -1583,6 +1592,8 @@ int Solver::run(pdcs_result* res) {
 
 }  // namespace pdcs
 
+#include "pdcs_batch.cuh"
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -1639,6 +1650,28 @@ int pdcs_solve(const pdcs_problem* prob, const pdcs_options* opts, pdcs_result* 
     return PDCS_ERR_BOUNDS;
   } catch (const std::exception& e) {
     std::fprintf(stderr, "pdcs_solve: %s\n", e.what());
+    return PDCS_ERR_INVALID;
+  }
+}
+
+int pdcs_solve_batch(int64_t count, const pdcs_problem* problems, const pdcs_options* opts, pdcs_result* results,
+                     pdcs_batch_info* info) {
+  if (count < 1 || !problems || !results) return PDCS_ERR_INVALID;
+  pdcs_options o;
+  if (opts) o = *opts;
+  else pdcs_default_options(&o);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PDCS_ERR_NO_DEVICE;
+  try {
+    pdcs::BatchSolver b(count, problems, &o);
+    return b.run_batch(results, info);
+  } catch (const pdcs::CudaError& e) {
+    std::fprintf(stderr, "pdcs_solve_batch: %s\n", e.what());
+    return PDCS_ERR_CUDA;
+  } catch (const std::domain_error&) {
+    return PDCS_ERR_BOUNDS;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "pdcs_solve_batch: %s\n", e.what());
     return PDCS_ERR_INVALID;
   }
 }

@@ -108,32 +108,13 @@ class _Holder:
         return a.ctypes.data if a.size else None
 
 
-def rpdhg_gpu_solve(*, n: int, m: int, nb: int, c, G, h, mGzero: int, mGnonnegative: int,
-                    socG: Sequence[int], rsocG: Sequence[int], expG: int, dual_expG: int,
-                    bl, bu, soc_x: Sequence[int], rsoc_x: Sequence[int], exp_x: int = 0,
-                    dual_exp_x: int = 0, Dl=None, Dr=None,
-                    rescaling_method: str = "ruiz_pock_chambolle", use_preconditioner: bool = True,
-                    use_adaptive_restart: bool = True, use_adaptive_step_size_weight: bool = True,
-                    use_aggressive: bool = True, use_accelerated: bool = False,
-                    use_resolving: bool = True, primal_sol=None, dual_sol=None,
-                    warm_start: bool = False, max_outer_iter: int = 10000,
-                    max_inner_iter: int = 500000, abs_tol: float = 1e-6, rel_tol: float = 1e-6,
-                    eps_primal_infeasible_low_acc: float = 1e-12,
-                    eps_dual_infeasible_low_acc: float = 1e-12,
-                    eps_primal_infeasible_high_acc: float = 1e-16,
-                    eps_dual_infeasible_high_acc: float = 1e-16, print_freq: int = 2000,
-                    check_terminate_freq: int = 2000, verbose: int = 0,
-                    time_limit: float = math.inf, method: str = "average",
-                    logfile_name: Optional[str] = None, use_kkt_restart: bool = False,
-                    kkt_restart_freq: int = 2000, use_duality_gap_restart: bool = True,
-                    duality_gap_restart_freq: int = 2000, attempt_limit: int = 0,
-                    attempts_per_graph: int = 32, stream=None, device_output: bool = False,
-                    force_resolving: bool = False) -> Solution:
-    """Solve min c'x s.t. Gx - h in K_d, bl <= x[:nb] <= bu, x[nb:] in K_p on the GPU."""
-    if method not in ("average", "halpern"):
-        raise ValueError("method only available for :average and :halpern")
-    if method == "halpern":
-        raise NotImplementedError("method=:halpern is not wired into the reference GPU module either")
+_PROBLEM_KEYS = ("n", "m", "nb", "c", "G", "h", "mGzero", "mGnonnegative", "socG", "rsocG", "expG",
+                 "dual_expG", "bl", "bu", "soc_x", "rsoc_x", "exp_x", "dual_exp_x", "Dl", "Dr")
+
+
+def _problem_struct(hold: _Holder, *, n, m, nb, c, G, h, mGzero, mGnonnegative, socG, rsocG, expG, dual_expG,
+                    bl, bu, soc_x, rsoc_x, exp_x=0, dual_exp_x=0, Dl=None, Dr=None):
+    """Validate like the reference (rpdhg_alg_gpu_gen.jl:1331-1375, :84, :94) and fill a PdcsProblem."""
     on_device = _is_torch_cuda(c)
     if not on_device:
         G = sp.csr_matrix(G)
@@ -162,11 +143,6 @@ def rpdhg_gpu_solve(*, n: int, m: int, nb: int, c, G, h, mGzero: int, mGnonnegat
     for q in list(rsocG) + list(rsoc_x):
         if q < 3:
             raise ValueError("The size of the rotated SOC must be greater than 2")
-    if warm_start and (primal_sol is None or dual_sol is None or len(primal_sol) != n or len(dual_sol) != m):
-        raise ValueError("Warmstart doesn't match the problem size")
-
-    L = capi.load()
-    hold = _Holder()
     P = capi.PdcsProblem()
     P.n, P.m, P.nb, P.nnz = n, m, nb, nnz
     P.G_rowptr, P.G_colind, P.G_val = hold.i32(rowptr), hold.i32(colind), hold.f64(val)
@@ -179,7 +155,29 @@ def rpdhg_gpu_solve(*, n: int, m: int, nb: int, c, G, h, mGzero: int, mGnonnegat
     P.rsoc_x, P.n_rsoc_x = hold.i64(rsoc_x), len(rsoc_x)
     P.exp_x, P.dual_exp_x = exp_x, dual_exp_x
     P.on_device = 1 if on_device else 0
+    return P
 
+
+def _options_struct(L, hold: _Holder, *, n=0, m=0, rescaling_method: str = "ruiz_pock_chambolle",
+                    use_preconditioner: bool = True, use_adaptive_restart: bool = True,
+                    use_adaptive_step_size_weight: bool = True, use_aggressive: bool = True,
+                    use_accelerated: bool = False, use_resolving: bool = True, primal_sol=None, dual_sol=None,
+                    warm_start: bool = False, max_outer_iter: int = 10000, max_inner_iter: int = 500000,
+                    abs_tol: float = 1e-6, rel_tol: float = 1e-6, eps_primal_infeasible_low_acc: float = 1e-12,
+                    eps_dual_infeasible_low_acc: float = 1e-12, eps_primal_infeasible_high_acc: float = 1e-16,
+                    eps_dual_infeasible_high_acc: float = 1e-16, print_freq: int = 2000,
+                    check_terminate_freq: int = 2000, verbose: int = 0, time_limit: float = math.inf,
+                    method: str = "average", logfile_name: Optional[str] = None, use_kkt_restart: bool = False,
+                    kkt_restart_freq: int = 2000, use_duality_gap_restart: bool = True,
+                    duality_gap_restart_freq: int = 2000, attempt_limit: int = 0, attempts_per_graph: int = 32,
+                    stream=None, force_resolving: bool = False):
+    """Fill a PdcsOptions from the reference's keyword arguments (rpdhg_alg_gpu_gen.jl:1219-1268)."""
+    if method not in ("average", "halpern"):
+        raise ValueError("method only available for :average and :halpern")
+    if method == "halpern":
+        raise NotImplementedError("method=:halpern is not wired into the reference GPU module either")
+    if warm_start and (primal_sol is None or dual_sol is None or len(primal_sol) != n or len(dual_sol) != m):
+        raise ValueError("Warmstart doesn't match the problem size")
     O = capi.PdcsOptions()
     L.pdcs_default_options(C.byref(O))
     O.rescaling_method = _RESCALING[rescaling_method.lstrip(":")]
@@ -210,7 +208,34 @@ def rpdhg_gpu_solve(*, n: int, m: int, nb: int, c, G, h, mGzero: int, mGnonnegat
     O.attempts_per_graph = attempts_per_graph
     O.force_resolving = int(force_resolving)
     O.stream = stream
+    return O
 
+
+def _info(R) -> Info:
+    return Info(exit_status=capi.EXIT_STATUS.get(R.exit_code, str(R.exit_code)),
+                exit_code=R.exit_code, pObj=R.pObj, dObj=R.dObj, iter=R.iter, time=R.time,
+                setup_time=R.setup_time, restart_used=R.restart_used,
+                l_inf_rel_primal_res=R.l_inf_rel_primal_res,
+                l_inf_rel_dual_res=R.l_inf_rel_dual_res, rel_gap=R.rel_gap,
+                l_2_rel_primal_res=R.l_2_rel_primal_res, l_2_rel_dual_res=R.l_2_rel_dual_res,
+                l_inf_abs_primal_res=R.l_inf_abs_primal_res,
+                l_inf_abs_dual_res=R.l_inf_abs_dual_res, abs_gap=R.abs_gap,
+                returned_sequence=R.returned_sequence, kernel_launches=R.kernel_launches,
+                graph_launches=R.graph_launches, time_iterations=R.time_iterations,
+                time_exit_checks=R.time_exit_checks, time_restarts=R.time_restarts,
+                restart_probes=R.restart_probes)
+
+
+def rpdhg_gpu_solve(*, device_output: bool = False, **kw) -> Solution:
+    """Solve min c'x s.t. Gx - h in K_d, bl <= x[:nb] <= bu, x[nb:] in K_p on the GPU.
+
+    Keywords: the reference's problem data and options (rpdhg_alg_gpu_gen.jl:1219-1268), plus
+    attempt_limit, attempts_per_graph, stream, force_resolving and device_output."""
+    L = capi.load()
+    hold = _Holder()
+    P = _problem_struct(hold, **{k: v for k, v in kw.items() if k in _PROBLEM_KEYS})
+    O = _options_struct(L, hold, **{k: v for k, v in kw.items() if k not in _PROBLEM_KEYS or k in ("n", "m")})
+    n, m = P.n, P.m
     R = capi.PdcsResult()
     if device_output:
         import torch
@@ -223,19 +248,52 @@ def rpdhg_gpu_solve(*, n: int, m: int, nb: int, c, G, h, mGzero: int, mGnonnegat
         R.x, R.y = (xo.ctypes.data if n else None), (yo.ctypes.data if m else None)
     rc = L.pdcs_solve(C.byref(P), C.byref(O), C.byref(R))
     capi.check(rc, "pdcs_solve")
-    info = Info(exit_status=capi.EXIT_STATUS.get(R.exit_code, str(R.exit_code)),
-                exit_code=R.exit_code, pObj=R.pObj, dObj=R.dObj, iter=R.iter, time=R.time,
-                setup_time=R.setup_time, restart_used=R.restart_used,
-                l_inf_rel_primal_res=R.l_inf_rel_primal_res,
-                l_inf_rel_dual_res=R.l_inf_rel_dual_res, rel_gap=R.rel_gap,
-                l_2_rel_primal_res=R.l_2_rel_primal_res, l_2_rel_dual_res=R.l_2_rel_dual_res,
-                l_inf_abs_primal_res=R.l_inf_abs_primal_res,
-                l_inf_abs_dual_res=R.l_inf_abs_dual_res, abs_gap=R.abs_gap,
-                returned_sequence=R.returned_sequence, kernel_launches=R.kernel_launches,
-                graph_launches=R.graph_launches, time_iterations=R.time_iterations,
-                time_exit_checks=R.time_exit_checks, time_restarts=R.time_restarts,
-                restart_probes=R.restart_probes)
-    return Solution(xo, yo, info)
+    return Solution(xo, yo, _info(R))
+
+
+@dataclasses.dataclass
+class BatchInfo:
+    setup_time: float
+    solve_time: float
+    time_iterations: float
+    kernel_launches: int
+    graph_launches: int
+    service_rounds: int
+    single_fallbacks: int
+
+
+def rpdhg_gpu_solve_batch(problems, **options):
+    """Solve many independent programs in one batched run (pdcs_solve_batch).
+
+    problems: sequence of dicts of rpdhg_gpu_solve's problem keywords (n, m, nb, c, G, h, cones, bl, bu)
+    or objects with a ``kwargs()`` method.  options: rpdhg_gpu_solve's option keywords, shared by all
+    instances.  Returns (list of Solution, BatchInfo)."""
+    L = capi.load()
+    hold = _Holder()
+    probs = [p.kwargs() if hasattr(p, "kwargs") else dict(p) for p in problems]
+    if not probs:
+        raise ValueError("empty batch")
+    Ps = (capi.PdcsProblem * len(probs))()
+    for i, kw in enumerate(probs):
+        Ps[i] = _problem_struct(hold, **{k: v for k, v in kw.items() if k in _PROBLEM_KEYS})
+        if Ps[i].on_device:
+            raise ValueError("pdcs_solve_batch takes host data")
+    O = _options_struct(L, hold, **options)
+    Rs = (capi.PdcsResult * len(probs))()
+    outs = []
+    for i, kw in enumerate(probs):
+        xo, yo = np.zeros(Ps[i].n), np.zeros(Ps[i].m)
+        outs.append((xo, yo))
+        Rs[i].x = xo.ctypes.data if Ps[i].n else None
+        Rs[i].y = yo.ctypes.data if Ps[i].m else None
+    B = capi.PdcsBatchInfo()
+    rc = L.pdcs_solve_batch(len(probs), Ps, C.byref(O), Rs, C.byref(B))
+    capi.check(rc, "pdcs_solve_batch")
+    sols = [Solution(outs[i][0], outs[i][1], _info(Rs[i])) for i in range(len(probs))]
+    info = BatchInfo(setup_time=B.setup_time, solve_time=B.solve_time, time_iterations=B.time_iterations,
+                     kernel_launches=B.kernel_launches, graph_launches=B.graph_launches,
+                     service_rounds=B.service_rounds, single_fallbacks=B.single_fallbacks)
+    return sols, info
 
 
 def solve_problem(prob, **kw) -> Solution:

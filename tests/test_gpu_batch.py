@@ -1,0 +1,111 @@
+"""Batched solver (pdcs_solve_batch): every instance follows the single-instance
+algorithm with its own step sizes, restarts and termination.
+
+Parity: (1) after a fixed number of attempts each instance's iterates equal the
+oracle's to rounding; (2) solved to 1e-6, each instance matches the
+single-instance GPU solve (status, objective) and the oracle's evaluator."""
+import numpy as np
+import pytest
+
+from oracle import binding as B
+from pdcs_b200 import problems, solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed_batch():
+    return [
+        problems.mixed_small(seed=7),
+        problems.batch_socp_c3(count=3, seed=11, nmin=50, nmax=400)[0],
+        problems.logreg_exp_c1(samples=120, features=12, density=0.3),
+        problems.mixed_small(seed=9, scale=2),
+        problems.socp_c0(n_box=60, n_soc=60, m=90, density=0.08, seed=5),
+    ]
+
+
+@pytest.mark.parametrize("attempts", [1, 7, 60])
+def test_batch_first_attempts_track_oracle(cuda, attempts):
+    batch = _mixed_batch()
+    sols, info = solver.rpdhg_gpu_solve_batch(batch, attempt_limit=attempts)
+    assert info.single_fallbacks == 0
+    for p, g in zip(batch, sols):
+        o = B.solve(p, threads=1, attempt_limit=attempts)
+        assert g.info.exit_code == 10 and o["exit_code"] == 10
+        assert g.info.iter == o["iter"] == attempts
+        for a, b in ((g.primal, o["x"]), (g.dual, o["y"])):
+            scale = max(1.0, np.abs(b).max())
+            assert np.abs(a - b).max() <= 1e-9 * scale, (p.name, attempts, np.abs(a - b).max())
+
+
+def test_batch_matches_single_solves(cuda):
+    batch = _mixed_batch() + problems.batch_socp_c3(count=6, seed=23, nmin=50, nmax=600)
+    sols, info = solver.rpdhg_gpu_solve_batch(batch, time_limit=300)
+    assert info.graph_launches > 0 and info.service_rounds > 0
+    for p, g in zip(batch, sols):
+        s = solver.solve_problem(p, time_limit=120)
+        assert g.info.exit_status == s.info.exit_status == "optimal", (p.name, g, s)
+        e = B.evaluate(p, g.primal, g.dual)
+        assert max(e["primal_res_gpu_form"], e["dual_res"], e["rel_gap"]) < 1.05e-6, (p.name, e)
+        assert abs(g.info.pObj - e["pobj"]) <= 1e-9 * (1 + abs(e["pobj"]))
+        rel = abs(g.info.pObj - s.info.pObj) / (1 + abs(s.info.pObj))
+        assert rel <= 2e-6, (p.name, g.info.pObj, s.info.pObj)
+        # same algorithm; only the order of floating-point sums differs, which can move
+        # convergence across one exit check (every 2000 attempts) or a restart
+        assert abs(g.info.iter - s.info.iter) <= 2000 + 0.25 * s.info.iter, (p.name, g.info.iter, s.info.iter)
+
+
+def test_batch_oracle_solution_parity(cuda):
+    batch = problems.batch_socp_c3(count=4, seed=31, nmin=80, nmax=300)
+    sols, _ = solver.rpdhg_gpu_solve_batch(batch, time_limit=300)
+    for p, g in zip(batch, sols):
+        o = B.solve(p, threads=2)
+        assert g.info.exit_status == "optimal" and o["exit_code"] == 0
+        eg = B.evaluate(p, g.primal, g.dual)
+        eo = B.evaluate(p, o["x"], o["y"])
+        assert abs(eg["pobj"] - eo["pobj"]) / (1 + abs(eo["pobj"])) <= 2e-6
+
+
+def test_batch_infeasible_members_keep_their_status(cuda):
+    batch = [problems.primal_infeasible_lp(), problems.mixed_small(seed=7), problems.dual_infeasible_lp()]
+    sols, _ = solver.rpdhg_gpu_solve_batch(batch, time_limit=300)
+    single = [solver.solve_problem(p, time_limit=120) for p in batch]
+    cls = lambda c: {2: "p", 3: "p", 4: "d", 5: "d"}.get(c, c)
+    for g, s in zip(sols, single):
+        assert cls(g.info.exit_code) == cls(s.info.exit_code), (g, s)
+    assert sols[1].info.exit_status == "optimal"
+
+
+def test_batch_kkt_restart_variant(cuda):
+    batch = _mixed_batch()[:3]
+    kw = dict(time_limit=300, use_kkt_restart=True, use_duality_gap_restart=False)
+    sols, _ = solver.rpdhg_gpu_solve_batch(batch, **kw)
+    for p, g in zip(batch, sols):
+        s = solver.solve_problem(p, **kw)
+        assert g.info.exit_status == s.info.exit_status == "optimal"
+        assert abs(g.info.pObj - s.info.pObj) / (1 + abs(s.info.pObj)) <= 2e-6
+
+
+def test_batch_resolving_fallback_is_the_single_solve(cuda):
+    batch = _mixed_batch()[:2]
+    sols, info = solver.rpdhg_gpu_solve_batch(batch, time_limit=300, force_resolving=True)
+    assert info.single_fallbacks == 2
+    for p, g in zip(batch, sols):
+        s = solver.solve_problem(p, time_limit=120, force_resolving=True)
+        assert g.info.exit_code == s.info.exit_code
+        assert g.info.iter == s.info.iter
+        assert np.array_equal(g.primal, s.primal)
+
+
+def test_batch_validation(cuda):
+    ok = problems.mixed_small().kwargs()
+    bad = dict(ok)
+    bad["mGzero"] = ok["mGzero"] + 1
+    with pytest.raises(ValueError):
+        solver.rpdhg_gpu_solve_batch([ok, bad])
+    extra = problems.random_feasible(n_box=5, soc_x=[3], mGnonnegative=4, density=0.5, seed=3).kwargs()
+    extra["n"] += 1  # a variable outside every cone
+    extra["c"] = np.append(extra["c"], 0.0)
+    import scipy.sparse as sp
+    extra["G"] = sp.hstack([sp.csr_matrix(extra["G"]), sp.csr_matrix((extra["m"], 1))]).tocsr()
+    with pytest.raises(RuntimeError, match="status -7"):
+        solver.rpdhg_gpu_solve_batch([ok, extra])
