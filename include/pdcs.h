@@ -100,7 +100,9 @@ typedef struct {
   double time_limit;             /* seconds; <= 0 means none */
   int64_t kkt_restart_freq;      /* 2000 */
   int32_t use_duality_gap_restart; /* 1 */
-  int32_t precision;             /* 0: FP64 throughout (the reference's arithmetic) */
+  int32_t precision;             /* 0: FP64 throughout (the reference's arithmetic); 1: FP32 matrices and
+                                    iterate deltas between FP64 anchors (FP64 projections, averages,
+                                    termination checks) */
   int64_t duality_gap_restart_freq; /* 2000 */
   int64_t attempt_limit;         /* > 0: stop after this many PDHG attempts (sampling) */
   void* stream;                  /* cudaStream_t to run on; NULL = an internal stream */
@@ -161,6 +163,18 @@ typedef struct {
  * be NULL.  Returns PDCS_OK or the first validation error. */
 int pdcs_solve_batch(int64_t count, const pdcs_problem* problems, const pdcs_options* opts,
                      pdcs_result* results, pdcs_batch_info* info);
+
+/* A prepared batch: merged, uploaded and preconditioned once, solved any number
+ * of times from a cold start (to time solves with the data resident in device
+ * memory, or to solve again after a forward pass).  No counterpart in the
+ * reference.  The problems' host arrays must stay valid until
+ * pdcs_batch_destroy (an instance that enters the resolving fallback is
+ * re-solved alone from them).  Not thread-safe: one call at a time per handle. */
+typedef struct pdcs_batch pdcs_batch;
+int pdcs_batch_create(int64_t count, const pdcs_problem* problems, const pdcs_options* opts, pdcs_batch** out);
+/* attempt_limit > 0 overrides the option for this solve. */
+int pdcs_batch_solve(pdcs_batch* batch, int64_t attempt_limit, pdcs_result* results, pdcs_batch_info* info);
+void pdcs_batch_destroy(pdcs_batch* batch);
 
 /* Block projections on device memory.  Replaces the projection entry points
  * few_block_proj (cuda/few_block_proj.cu:414-432, bound by gpu_kernel.jl:377-406)

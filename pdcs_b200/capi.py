@@ -89,8 +89,8 @@ class PdcsBatchInfo(C.Structure):
 
 
 # every symbol declared in include/pdcs.h
-EXPORTS = ["pdcs_default_options", "pdcs_solve", "pdcs_solve_batch", "pdcs_block_proj", "pdcs_spmv_csr",
-           "pdcs_spmv_csr_noalloc", "pdcs_version"]
+EXPORTS = ["pdcs_default_options", "pdcs_solve", "pdcs_solve_batch", "pdcs_batch_create", "pdcs_batch_solve",
+           "pdcs_batch_destroy", "pdcs_block_proj", "pdcs_spmv_csr", "pdcs_spmv_csr_noalloc", "pdcs_version"]
 
 _lib = None
 
@@ -110,6 +110,12 @@ def load():
     L.pdcs_solve.restype = C.c_int
     L.pdcs_solve_batch.argtypes = [C.c_int64, _P(PdcsProblem), _P(PdcsOptions), _P(PdcsResult), _P(PdcsBatchInfo)]
     L.pdcs_solve_batch.restype = C.c_int
+    L.pdcs_batch_create.argtypes = [C.c_int64, _P(PdcsProblem), _P(PdcsOptions), _P(_vp)]
+    L.pdcs_batch_create.restype = C.c_int
+    L.pdcs_batch_solve.argtypes = [_vp, C.c_int64, _P(PdcsResult), _P(PdcsBatchInfo)]
+    L.pdcs_batch_solve.restype = C.c_int
+    L.pdcs_batch_destroy.argtypes = [_vp]
+    L.pdcs_batch_destroy.restype = None
     L.pdcs_block_proj.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]
     L.pdcs_block_proj.restype = C.c_int
     L.pdcs_spmv_csr.argtypes = [C.c_int64, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp]

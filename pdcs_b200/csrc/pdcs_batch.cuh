@@ -151,6 +151,7 @@ struct Inst {
   int64_t restart_used = 0, check_count = 0, probes = 0;
   double hNrm1 = 0, hNrmInf = 0, cNrm1 = 0, cNrmInf = 0, ginf = 1, omega0 = 1;
   bool needs_single = false;  // resolving fallback: re-solved alone after the batch
+  bool anchored = false;      // FP32 mode: deltas live (from the start of iterating to the halt)
   double t_done = 0;
   Req req;
   std::coroutine_handle<> waiting;
@@ -232,9 +233,24 @@ class BatchSolver : public Solver {
     if (bgraph_) cudaGraphDestroy(bgraph_);
     if (pin_) cudaFreeHost(pin_);
   }
-  int run_batch(pdcs_result* res, pdcs_batch_info* info);
+  // merge, upload and precondition once (the problems must stay valid until destruction:
+  // the resolving fallback re-solves an instance from them)
+  int prepare();
+  // cold-start solve of the prepared batch; attempt_limit > 0 overrides the option
+  int solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_limit);
+  int run_batch(pdcs_result* res, pdcs_batch_info* info) {
+    int rc = prepare();
+    return rc != PDCS_OK ? rc : solve(res, info, 0);
+  }
 
  private:
+  struct InstConst {
+    double hNrm1, hNrmInf, cNrm1, cNrmInf, ginf, omega0;
+  };
+  std::vector<InstConst> consts_;
+  double setup_time_ = 0.0;
+  bool prepared_ = false;
+  void reset_state();
   int64_t K_;
   const pdcs_problem* probs_;
   // merged host problem
@@ -260,6 +276,20 @@ class BatchSolver : public Solver {
   double* seg_out_ = nullptr;  // K * 20
   cudaGraph_t bgraph_ = nullptr;
   cudaGraphExec_t bgraph_exec_ = nullptr;
+  // active-row lists of G (0) and G' (1) for the iteration graph
+  struct Compact {
+    int4* rows = nullptr;
+    int64_t* cbin = nullptr;
+    int64_t* full_bin = nullptr;
+    int32_t* flag = nullptr;
+    int32_t* pos = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+  } cmp_[2];
+  CsrDev Gc_{}, Gtc_{};
+  CsrT<float> G32c_{}, Gt32c_{};
+  void setup_compaction();
+  void compact(const uint8_t* mask);
   // pinned staging (reset at every synchronisation)
   char* pin_ = nullptr;
   size_t pin_cap_ = 0, pin_off_ = 0;
@@ -543,8 +573,7 @@ void BatchSolver::setup_batch() {
   PDCS_CUDA(cudaMemsetAsync(live_, 0, K, s_));
   pin_cap_ = std::max<size_t>(size_t(1) << 20, (size_t)K * (20 * sizeof(double) + sizeof(PdhgState)) * 4 + 4096);
   PDCS_CUDA(cudaMallocHost(&pin_, pin_cap_));
-  inst_.resize(K);
-  for (int64_t k = 0; k < K; ++k) inst_[k].k = k;
+  consts_.resize(K);
   // per-instance constants: raw norms (cal_constant), ginf, initial primal weight
   {
     SegSide X{}, Y{};
@@ -562,7 +591,7 @@ void BatchSolver::setup_batch() {
     seg_launch(nullptr, X, Y, 7);
     const double* r = seg_fetch(7);
     for (int64_t k = 0; k < K; ++k) {
-      Inst& I = inst_[k];
+      InstConst& I = consts_[k];
       const double* q = r + k * 7;
       I.cNrm1 = q[0];
       I.cNrmInf = q[1];
@@ -598,17 +627,76 @@ const double* BatchSolver::seg_fetch(int stride) {
   return h;
 }
 
+void BatchSolver::setup_compaction() {
+  const CsrDev* full[2] = {&G_, &Gt_};
+  CsrDev* view[2] = {&Gc_, &Gtc_};
+  for (int w = 0; w < 2; ++w) {
+    Compact& c = cmp_[w];
+    const CsrDev& F = *full[w];
+    const int64_t R = F.bin_off[kBins];
+    c.rows = A.alloc<int4>(std::max<int64_t>(R, 1));
+    c.cbin = A.alloc<int64_t>(kBins + 1);
+    c.full_bin = A.alloc<int64_t>(kBins + 1);
+    c.flag = A.alloc<int32_t>(R + 1);
+    c.pos = A.alloc<int32_t>(R + 1);
+    PDCS_CUDA(cudaMemcpyAsync(c.full_bin, F.bin_off, sizeof(int64_t) * (kBins + 1), cudaMemcpyHostToDevice, s_));
+    PDCS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c.tmp_bytes, c.flag, c.pos, (int)(R + 1), s_));
+    c.tmp = A.alloc<char>(std::max<size_t>(c.tmp_bytes, 1));
+    *view[w] = F;
+    view[w]->rows = c.rows;
+    view[w]->dbin = c.cbin;
+  }
+  PDCS_CUDA(cudaStreamSynchronize(s_));  // the bin offsets were copied from the host structs
+  if (fp32_) {
+    G32c_ = G32_;
+    G32c_.rows = cmp_[0].rows;
+    G32c_.dbin = cmp_[0].cbin;
+    Gt32c_ = Gt32_;
+    Gt32c_.rows = cmp_[1].rows;
+    Gt32c_.dbin = cmp_[1].cbin;
+  }
+}
+
+// Rebuild the iteration graph's row lists from the rows of the masked instances.
+void BatchSolver::compact(const uint8_t* mask) {
+  const CsrDev* full[2] = {&G_, &Gt_};
+  for (int w = 0; w < 2; ++w) {
+    Compact& c = cmp_[w];
+    const int64_t R = full[w]->bin_off[kBins];
+    row_flags_kernel<<<grid_for(R + 1), kThreads, 0, s_>>>(full[w]->rows, R, mask, c.flag);
+    PDCS_CUDA(cub::DeviceScan::ExclusiveSum(c.tmp, c.tmp_bytes, c.flag, c.pos, (int)(R + 1), s_));
+    row_compact_kernel<<<grid_for(R), kThreads, 0, s_>>>(full[w]->rows, R, c.flag, c.pos, c.rows, c.full_bin,
+                                                         c.cbin);
+    kernels_ += 3;
+  }
+}
+
 void BatchSolver::capture_batch_graph() {
   PDCS_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
   const int ctl_grid = (int)std::max<int64_t>(1, std::min<int64_t>((K_ * 32 + kThreads - 1) / kThreads, 148 * 16));
-  for (int a = 0; a < attempts_per_graph_; ++a) {
+  for (int a = 0; a < attempts_per_graph_ && fp32_; ++a) {
     int32_t* cur = live_cnt_ + (a & 1);
     int32_t* nxt = live_cnt_ + ((a + 1) & 1);
-    spmv_binned_kernel<1, true><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, yl, nullptr, aty, nullptr, cur, nullptr,
-                                                                      ix_, live_);
+    spmv_binned_kernel<1, false, float><<<Gt32c_.cta0[kBins], kThreads, 0, s_>>>(Gt32c_, dyl32_, nullptr, aty32_,
+                                                                               nullptr, cur);
+    OpPrimalStep32B op1{xa_, dxl32_, qa_, aty32_, dx32_, x, ix_, live_, ps_, dxsq_};
+    update_project_kernel<OpPrimalStep32B><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, cur);
+    spmv_binned_kernel<2, false, float><<<G32c_.cta0[kBins], kThreads, 0, s_>>>(G32c_, dx32_, dxl32_, gx32_,
+                                                                              gxl32_, cur);
+    OpDualStep32B op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_};
+    update_project_kernel<OpDualStep32B><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, cur);
+    BatchCtl ctl{sts_, ps_, ds_, live_, rx_, ry_, dxsq_, dysq_, dgdy_, cur, nxt, done_ctas_, live_cnt_ + 2};
+    batch_control_kernel<<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
+    batch_reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dx32_, dxl32_, dxm_, n_, dy32_,
+                                                               dyl32_, dym_, m_);
+  }
+  for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
+    int32_t* cur = live_cnt_ + (a & 1);
+    int32_t* nxt = live_cnt_ + ((a + 1) & 1);
+    spmv_binned_kernel<1><<<Gtc_.cta0[kBins], kThreads, 0, s_>>>(Gtc_, yl, nullptr, aty, nullptr, cur);
     OpPrimalStepB op1{xl, aty, c_s, x, ix_, live_, ps_, dxsq_};
     update_project_kernel<OpPrimalStepB><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, cur);
-    spmv_binned_kernel<2, true><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, x, xl, gx, gxl, cur, nullptr, iy_, live_);
+    spmv_binned_kernel<2><<<Gc_.cta0[kBins], kThreads, 0, s_>>>(Gc_, x, xl, gx, gxl, cur);
     OpDualStepB op2{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_};
     update_project_kernel<OpDualStepB><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, cur);
     BatchCtl ctl{sts_, ps_, ds_, live_, rx_, ry_, dxsq_, dysq_, dgdy_, cur, nxt, done_ctas_, live_cnt_ + 2};
@@ -641,11 +729,7 @@ void BatchSolver::exec_group(std::vector<Inst*>& g) {
       break;
     }
     case RQ_SPMV: {
-      const CsrDev& M = q.side ? Gt_ : G_;
-      spmv_binned_kernel<1, true><<<M.cta0[kBins], kThreads, 0, s_>>>(M, q.p[0], nullptr, const_cast<double*>(q.p[1]),
-                                                                      nullptr, nullptr, nullptr, q.side ? ix_ : iy_,
-                                                                      mask);
-      kernels_++;
+      spmv_masked(q.side ? Gt_ : G_, q.p[0], const_cast<double*>(q.p[1]), mask);
       break;
     }
     case RQ_REFLECT: {
@@ -660,11 +744,8 @@ void BatchSolver::exec_group(std::vector<Inst*>& g) {
       const double *xs = q.p[0], *ys = q.p[1];
       double *gxs = const_cast<double*>(q.p[2]), *atys = const_cast<double*>(q.p[3]);
       if (q.side == 0) {  // side 1: the products G xs, G' ys are given
-        spmv_binned_kernel<1, true><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, xs, nullptr, gxs, nullptr, nullptr,
-                                                                        nullptr, iy_, mask);
-        spmv_binned_kernel<1, true><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, ys, nullptr, atys, nullptr, nullptr,
-                                                                          nullptr, ix_, mask);
-        kernels_ += 2;
+        spmv_masked(G_, xs, gxs, mask);
+        spmv_masked(Gt_, ys, atys, mask);
       }
       PerElem<OpResidual> opp{OpResidual{gxs, Dl, 1.0, nullptr, 0.0, h_raw, tm[5], bl_fin, bu_fin, 0}, tm[5], cy_, m_,
                               iy_, mask};
@@ -707,11 +788,9 @@ void BatchSolver::exec_group(std::vector<Inst*>& g) {
       double* gxs = const_cast<double*>(q.p[7]);
       PerElem<OpAxpyProjB> ox{OpAxpyProjB{q.p[0], q.p[2], s0_, xs, nullptr, nullptr, ix_}, xs, cx_, n_, ix_, mask};
       update_project(ox, XI, part_a);
-      spmv_binned_kernel<1, true><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, xs, nullptr, gxs, nullptr, nullptr, nullptr,
-                                                                      iy_, mask);
+      spmv_masked(G_, xs, gxs, mask);
       PerElem<OpAxpyProjB> oy{OpAxpyProjB{q.p[1], q.p[3], s1_, ys, gxs, q.p[4], iy_}, ys, cy_, m_, iy_, mask};
       update_project(oy, YI, part_b);
-      kernels_ += 1;
       SegSide X{}, Y{};
       X.a[0] = cx_; X.kind[0] = SK_SUM;
       X.a[1] = cx_ + n_; X.kind[1] = SK_SUM;
@@ -734,9 +813,7 @@ void BatchSolver::exec_group(std::vector<Inst*>& g) {
     }
     case RQ_MNORM: {
       double* gdx = const_cast<double*>(q.p[2]);
-      spmv_binned_kernel<1, true><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, q.p[0], nullptr, gdx, nullptr, nullptr,
-                                                                      nullptr, iy_, mask);
-      kernels_++;
+      spmv_masked(G_, q.p[0], gdx, mask);
       SegSide X{}, Y{};
       X.a[0] = q.p[0]; X.kind[0] = SK_DOT;
       X.count = 1;
@@ -797,6 +874,21 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   PDCS_CUDA(cudaMemcpyAsync(ds_, hds, sizeof(double) * K_, cudaMemcpyHostToDevice, s_));
   PDCS_CUDA(cudaMemcpyAsync(live_, hl, K_, cudaMemcpyHostToDevice, s_));
   PDCS_CUDA(cudaMemcpyAsync(live_cnt_, hc, 4 * sizeof(int32_t), cudaMemcpyHostToDevice, s_));
+  // the graph's SpMVs run over the rows of the iterating instances only (rows of
+  // instances that halt during these graphs are still computed; their products
+  // are not read before the next attempt or anchor recomputes them)
+  compact(live_);
+  if (fp32_) {
+    // FP64 anchors at the current iterates: for instances that (re)start
+    // iterating, and every round for the others (refinement keeps the FP32
+    // deltas small: at most the movement of one round)
+    std::vector<Inst*> again;
+    for (Inst* I : its)
+      if (I->anchored) again.push_back(I);
+    if (!again.empty()) materialize(ix_, iy_, upload_mask(again));
+    for (Inst* I : its) I->anchored = true;
+    anchor(ix_, iy_, live_);
+  }
   int64_t graphs = (to_check + attempts_per_graph_ - 1) / attempts_per_graph_;
   graphs = std::max<int64_t>(1, std::min<int64_t>(graphs, 4));
   for (int64_t gi = 0; gi < graphs; ++gi) {
@@ -814,6 +906,10 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
     I->S.do_reflect = 0;  // applied by the graph's reflection kernel
     I->S.done_ctas = 0;
     if (!I->S.active || timeout) halted.push_back(I);
+  }
+  if (fp32_ && !halted.empty()) {  // their host requests work on the FP64 iterates
+    materialize(ix_, iy_, upload_mask(halted));
+    for (Inst* I : halted) I->anchored = false;
   }
   for (Inst* I : halted) resume(*I);
 }
@@ -1262,17 +1358,65 @@ Co<> BatchSolver::main_task(Inst& I) {
   I.exit_code = PDCS_EXIT_MAX_ITER;
 }
 
-int BatchSolver::run_batch(pdcs_result* res, pdcs_batch_info* info) {
+int BatchSolver::prepare() {
   int rc = validate_batch();
   if (rc != PDCS_OK) return rc;
   const double t0 = now_s();
   merge();
   rc = validate();
   if (rc != PDCS_OK) return rc;
+  inst_of_y_ = h_iy_.data();
+  inst_of_x_ = h_ix_.data();
   setup();
   setup_batch();
+  setup_compaction();
+  // the merged matrix lives on the device now
+  std::vector<int32_t>().swap(h_ci_);
+  std::vector<double>().swap(h_v_);
+  std::vector<int32_t>().swap(h_rp_);
+  P.G_rowptr = nullptr;
+  P.G_colind = nullptr;
+  P.G_val = nullptr;
+  setup_time_ = now_s() - t0;
+  prepared_ = true;
+  return PDCS_OK;
+}
+
+// iterates to the cold start, warm starts of the exponential-cone roots cleared,
+// fresh per-instance control state
+void BatchSolver::reset_state() {
+  for (double* v : {x, xl, xm, xbest}) PDCS_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * n_, s_));
+  for (double* v : {y, yl, ym, ybest}) PDCS_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * m_, s_));
+  const int64_t nxe = XI.exp_count + XI.dexp_count, nye = YI.exp_count + YI.dexp_count;
+  if (nxe) PDCS_CUDA(cudaMemsetAsync(XI.rho_ws, 0xff, sizeof(double) * nxe, s_));
+  if (nye) PDCS_CUDA(cudaMemsetAsync(YI.rho_ws, 0xff, sizeof(double) * nye, s_));
+  PDCS_CUDA(cudaMemsetAsync(live_cnt_, 0, 4 * sizeof(int32_t), s_));
+  PDCS_CUDA(cudaMemsetAsync(done_ctas_, 0, sizeof(uint32_t), s_));
+  inst_.clear();
+  inst_.resize(K_);
+  for (int64_t k = 0; k < K_; ++k) {
+    Inst& I = inst_[k];
+    const InstConst& c = consts_[k];
+    I.k = k;
+    I.hNrm1 = c.hNrm1;
+    I.hNrmInf = c.hNrmInf;
+    I.cNrm1 = c.cNrm1;
+    I.cNrmInf = c.cNrmInf;
+    I.ginf = c.ginf;
+    I.omega0 = c.omega0;
+  }
+  kernels_ = graphs_ = probes_ = rounds_ = 0;
+  t_iter_ = 0.0;
+}
+
+int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_limit) {
+  if (!prepared_) return PDCS_ERR_INVALID;
+  const int64_t limit0 = O.attempt_limit;
+  if (attempt_limit > 0) O.attempt_limit = attempt_limit;
+  reset_state();
   t_start_ = now_s();
   schedule();
+  O.attempt_limit = limit0;
   PDCS_CUDA(cudaStreamSynchronize(s_));
   // outputs: unscaled current or averaged iterate per instance, scattered to the callers' buffers
   uint8_t* hpick = stage<uint8_t>(K_);
@@ -1331,13 +1475,13 @@ int BatchSolver::run_batch(pdcs_result* res, pdcs_batch_info* info) {
     R.l_inf_abs_dual_res = C.linf_abs_d;
     R.abs_gap = C.abs_gap;
     R.time = solve_time;
-    R.setup_time = t_start_ - t0;
+    R.setup_time = setup_time_;
     R.kernel_launches = kernels_;
     R.graph_launches = graphs_;
     R.restart_probes = I.probes;
   }
   if (info) {
-    info->setup_time = t_start_ - t0;
+    info->setup_time = setup_time_;
     info->solve_time = solve_time;
     info->kernel_launches = kernels_;
     info->graph_launches = graphs_;

@@ -306,6 +306,26 @@ __global__ void masked_axpby_kernel(double* __restrict__ out, const double* __re
   }
 }
 
+// Active-row compaction of a bin-ordered row list: flag[q] = 1 for rows of
+// masked instances (flag[R] = 0 closes the scan).
+__global__ void row_flags_kernel(const int4* __restrict__ rows, int64_t R, const uint8_t* __restrict__ mask,
+                                 int32_t* __restrict__ flag) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q <= R; q += stride)
+    flag[q] = (q < R && mask[rows[q].w]) ? 1 : 0;
+}
+
+// out[pos[q]] = rows[q] for flagged rows (pos: exclusive scan of flag, so the
+// bins stay contiguous and in order); cbin[b] = pos[full_bin[b]]
+__global__ void row_compact_kernel(const int4* __restrict__ rows, int64_t R, const int32_t* __restrict__ flag,
+                                   const int32_t* __restrict__ pos, int4* __restrict__ out,
+                                   const int64_t* __restrict__ full_bin, int64_t* __restrict__ cbin) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < R; q += stride)
+    if (flag[q]) out[pos[q]] = rows[q];
+  if (blockIdx.x == 0 && threadIdx.x <= kBins) cbin[threadIdx.x] = pos[full_bin[threadIdx.x]];
+}
+
 // unscaled output: out = (pick[k] ? vm : v) / D
 __global__ void batch_output_kernel(double* __restrict__ out, const double* __restrict__ v,
                                     const double* __restrict__ vm, const double* __restrict__ D,

@@ -1,0 +1,227 @@
+// pdcs_fp32.cuh -- FP32-bulk PDHG attempts with FP64 anchors.
+//
+// Between two refinements the iterates are stored as FP32 deltas from FP64
+// anchors:
+//   x = xa + dx,  x_lag = xa + dxl,  x_avg = xa + dxm (dxm in FP64)
+//   y = ya + dy,  y_lag = ya + dyl,  y_avg = ya + dym
+// and the per-anchor products are precomputed in FP64:
+//   qa = G' ya - c,   ra = G xa - h.
+// One attempt then needs only FP32 SpMVs of the deltas (G and G' stored in
+// FP32): G' y_lag - c = qa + G' dyl,  2 G x - G x_lag - h = ra + 2 G dx - G dxl.
+// FP32 rounding is relative to the deltas (the distance moved since the
+// anchor), not to the iterates.  Projections -- the exponential-cone root
+// included -- the eta_bar sums and the averages are FP64.  The deltas are
+// folded back into the FP64 iterates (materialize) at every halt of the
+// device loop and the anchors move there (anchor) every round of graphs, so
+// the exit checks, restarts and KKT reductions run in FP64 on the FP64 matrix.
+#pragma once
+#include "pdcs_kernels.cuh"
+
+namespace pdcs {
+
+// ---- single instance ----
+
+// x = P(xa + dxl + ps (qa + aty)); dx = x - xa (FP32); acc: sum (dx - dxl)^2
+struct OpPrimalStep32 {
+  static constexpr int NACC = 1;
+  static constexpr bool kFusedControl = false;
+  __device__ static const int32_t* kinds() { return kSum1; }
+  const double* xa;
+  const float* dxl;
+  const double* qa;
+  const float* aty;
+  float* dx;
+  double* out;  // FP64 scratch of the large-SOC path
+  const PdhgState* st;
+  double ps;
+  __device__ void load() { ps = st->ps; }
+  __device__ double z(int64_t j) const { return xa[j] + (double)dxl[j] + ps * (qa[j] + (double)aty[j]); }
+  __device__ void fin(int64_t j, double, double p, double* acc) const {
+    const float d = (float)(p - xa[j]);
+    dx[j] = d;
+    const double s = (double)d - (double)dxl[j];
+    acc[0] = fma(s, s, acc[0]);
+  }
+};
+
+// y = P(ya + dyl - ds (ra + 2 gx - gxl)); dy = y - ya (FP32);
+// acc: sum (dy - dyl)^2, sum (dy - dyl)(gx - gxl); the last CTA runs the control step
+struct OpDualStep32 {
+  static constexpr int NACC = 2;
+  static constexpr bool kFusedControl = true;
+  __device__ static const int32_t* kinds() { return kSum2; }
+  const double* ya;
+  const float* dyl;
+  const double* ra;
+  const float* gx;
+  const float* gxl;
+  float* dy;
+  double* out;
+  PdhgState* st;
+  double ds;
+  const double* ctrl_px;
+  int ctrl_nbx;
+  __device__ void load() { ds = st->ds; }
+  __device__ double z(int64_t i) const {
+    return ya[i] + (double)dyl[i] - ds * (ra[i] + (2.0 * (double)gx[i] - (double)gxl[i]));
+  }
+  __device__ void fin(int64_t i, double, double p, double* acc) const {
+    const float d = (float)(p - ya[i]);
+    dy[i] = d;
+    const double s = (double)d - (double)dyl[i];
+    acc[0] = fma(s, s, acc[0]);
+    acc[1] = fma(s, (double)gx[i] - (double)gxl[i], acc[1]);
+  }
+};
+
+// ---- batched (per-instance steps, masked, per-element contributions) ----
+
+struct OpPrimalStep32B {
+  static constexpr int NACC = 1;
+  static constexpr bool kFusedControl = false;
+  __device__ static const int32_t* kinds() { return kSum1; }
+  const double* xa;
+  const float* dxl;
+  const double* qa;
+  const float* aty;
+  float* dx;
+  double* out;
+  const int32_t* inst;
+  const uint8_t* mask;
+  const double* ps;
+  double* dxsq;
+  __device__ void load() {}
+  __device__ bool live(int64_t j) const { return mask[inst[j]] != 0; }
+  __device__ double z(int64_t j) const {
+    return xa[j] + (double)dxl[j] + ps[inst[j]] * (qa[j] + (double)aty[j]);
+  }
+  __device__ void fin(int64_t j, double, double p, double*) const {
+    const float d = (float)(p - xa[j]);
+    dx[j] = d;
+    const double s = (double)d - (double)dxl[j];
+    dxsq[j] = s * s;
+  }
+};
+
+struct OpDualStep32B {
+  static constexpr int NACC = 1;
+  static constexpr bool kFusedControl = false;
+  __device__ static const int32_t* kinds() { return kSum1; }
+  const double* ya;
+  const float* dyl;
+  const double* ra;
+  const float* gx;
+  const float* gxl;
+  float* dy;
+  double* out;
+  const int32_t* inst;
+  const uint8_t* mask;
+  const double* ds;
+  double* dysq;
+  double* dgdy;
+  __device__ void load() {}
+  __device__ bool live(int64_t i) const { return mask[inst[i]] != 0; }
+  __device__ double z(int64_t i) const {
+    return ya[i] + (double)dyl[i] - ds[inst[i]] * (ra[i] + (2.0 * (double)gx[i] - (double)gxl[i]));
+  }
+  __device__ void fin(int64_t i, double, double p, double*) const {
+    const float d = (float)(p - ya[i]);
+    dy[i] = d;
+    const double s = (double)d - (double)dyl[i];
+    dysq[i] = s * s;
+    dgdy[i] = s * ((double)gx[i] - (double)gxl[i]);
+  }
+};
+
+// Reflection + averaging on the deltas (the anchor cancels: tmp + inv = 1).
+__device__ __forceinline__ void reflect32_elem(const PdhgState& s, float* d, float* dl, double* dm, int64_t j) {
+  const double tmp = s.refl_tmp, inv = s.refl_inv, e = s.refl_extra, eta = s.refl_eta, cum = s.refl_cum;
+  const double cur = (double)d[j];
+  const float nv = (float)(tmp * ((1.0 + e) * cur - e * (double)dl[j]) + inv * cur);
+  dm[j] = (dm[j] * cum + (double)nv * eta) / (cum + eta);
+  d[j] = nv;
+  dl[j] = nv;
+}
+
+__global__ void __launch_bounds__(kThreads) reflect32_kernel(const PdhgState* __restrict__ st,
+                                                            float* __restrict__ dx, float* __restrict__ dxl,
+                                                            double* __restrict__ dxm, int64_t n,
+                                                            float* __restrict__ dy, float* __restrict__ dyl,
+                                                            double* __restrict__ dym, int64_t m) {
+  if (!st->do_reflect) return;
+  const PdhgState s = *st;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += stride) {
+    if (i < n) reflect32_elem(s, dx, dxl, dxm, i);
+    else reflect32_elem(s, dy, dyl, dym, i - n);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) batch_reflect32_kernel(const int32_t* __restrict__ live_cur,
+                                                                  const PdhgState* __restrict__ sts,
+                                                                  const int32_t* __restrict__ ix,
+                                                                  const int32_t* __restrict__ iy,
+                                                                  float* __restrict__ dx, float* __restrict__ dxl,
+                                                                  double* __restrict__ dxm, int64_t n,
+                                                                  float* __restrict__ dy, float* __restrict__ dyl,
+                                                                  double* __restrict__ dym, int64_t m) {
+  if (*live_cur == 0) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += stride) {
+    const bool isx = i < n;
+    const int64_t j = isx ? i : i - n;
+    const PdhgState& s = sts[isx ? ix[j] : iy[j]];
+    if (!s.do_reflect) continue;
+    if (isx) reflect32_elem(s, dx, dxl, dxm, j);
+    else reflect32_elem(s, dy, dyl, dym, j);
+  }
+}
+
+// anchor: va = v, d = 0, dl = vl - v, dm = vm - v (elements of masked instances; mask NULL = all)
+__global__ void anchor_kernel(const double* __restrict__ v, const double* __restrict__ vl,
+                              const double* __restrict__ vm, double* __restrict__ va, float* __restrict__ d,
+                              float* __restrict__ dl, double* __restrict__ dm, const int32_t* __restrict__ inst,
+                              const uint8_t* __restrict__ mask, int64_t len) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride) {
+    if (mask && !mask[inst[i]]) continue;
+    const double a = v[i];
+    va[i] = a;
+    d[i] = 0.0f;
+    dl[i] = (float)(vl[i] - a);
+    dm[i] = vm[i] - a;
+  }
+}
+
+// materialize: v = va + d, vl = va + dl, vm = va + dm
+__global__ void materialize_kernel(double* __restrict__ v, double* __restrict__ vl, double* __restrict__ vm,
+                                   const double* __restrict__ va, const float* __restrict__ d,
+                                   const float* __restrict__ dl, const double* __restrict__ dm,
+                                   const int32_t* __restrict__ inst, const uint8_t* __restrict__ mask,
+                                   int64_t len) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride) {
+    if (mask && !mask[inst[i]]) continue;
+    const double a = va[i];
+    v[i] = a + (double)d[i];
+    vl[i] = a + (double)dl[i];
+    vm[i] = a + dm[i];
+  }
+}
+
+// out = u - w on the elements of masked instances (mask NULL = all)
+__global__ void masked_sub_kernel(double* __restrict__ out, const double* __restrict__ u, const double* __restrict__ w,
+                                  const int32_t* __restrict__ inst, const uint8_t* __restrict__ mask, int64_t len) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride) {
+    if (mask && !mask[inst[i]]) continue;
+    out[i] = u[i] - w[i];
+  }
+}
+
+__global__ void to_float_kernel(float* __restrict__ out, const double* __restrict__ in, int64_t len) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride) out[i] = (float)in[i];
+}
+
+}  // namespace pdcs

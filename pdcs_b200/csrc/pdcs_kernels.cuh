@@ -11,6 +11,8 @@
 // The reference's third SpMV (G' dy, :712) is replaced by the identity
 // dx' G' dy = dy' (G x - G x_lag), which the second pass provides for free.
 #pragma once
+#include <type_traits>
+
 #include "pdcs_device.cuh"
 
 namespace pdcs {
@@ -91,24 +93,46 @@ __host__ __device__ inline void after_reject(PdhgState& st) {
 // ---------------------------------------------------------------------------
 constexpr int kBins = 7;
 
-struct CsrDev {
+// rows[q] for the q-th row in bin order: {row, first nonzero, end, instance}
+template <class T>
+struct CsrT {
   int64_t m, n, nnz;
   const int32_t* rp;
   const int32_t* ci;
-  const double* v;
-  const int32_t* perm;       // rows ordered by bin
+  const T* v;
+  const int4* rows;          // row descriptors ordered by bin (one 16-byte load per row)
+  const int64_t* dbin;       // device bin offsets (a compacted row list) or NULL: bin_off
   int64_t bin_off[kBins + 1];
   int32_t cta0[kBins + 1];   // first CTA of each bin, cta0[kBins] = grid size
 };
+using CsrDev = CsrT<double>;
 
-// MASK: rows whose instance (row_inst) has imask == 0 are skipped (batched solver).
-template <int NV, bool MASK = false>
-__global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const double* __restrict__ x0,
-                                                              const double* __restrict__ x1,
-                                                              double* __restrict__ y0, double* __restrict__ y1,
+// Row sums in T.  FP32 rows use FP32 products and sums; the long-row bin
+// (rows of more than 128 nonzeros, one CTA each) adds with Kahan compensation.
+template <class T>
+struct RowAcc {
+  T s = T(0), c = T(0);
+  __device__ __forceinline__ void add(T v) {
+    if constexpr (std::is_same_v<T, float>) {
+      const float y = v - c;
+      const float t = s + y;
+      c = (t - s) - y;
+      s = t;
+    } else {
+      s += v;
+    }
+  }
+};
+
+// MASK: rows whose instance (rows[q].w) has imask == 0 are skipped (batched solver).
+template <int NV, bool MASK = false, class T = double>
+__global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
+                                                              const std::type_identity_t<T>* __restrict__ x0,
+                                                              const std::type_identity_t<T>* __restrict__ x1,
+                                                              std::type_identity_t<T>* __restrict__ y0,
+                                                              std::type_identity_t<T>* __restrict__ y1,
                                                               const int32_t* __restrict__ active,
                                                               int32_t* __restrict__ clear_flag = nullptr,
-                                                              const int32_t* __restrict__ row_inst = nullptr,
                                                               const uint8_t* __restrict__ imask = nullptr) {
   // first kernel of a PDHG attempt: the previous attempt's reflection (if any)
   // has run by now, so its flag is cleared here, before the halt check
@@ -119,7 +143,7 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const d
 #pragma unroll
   for (int b = 1; b < kBins; ++b)
     if (cta >= A.cta0[b]) bin = b;
-  const int64_t r0 = A.bin_off[bin], r1 = A.bin_off[bin + 1];
+  const int64_t r0 = A.dbin ? A.dbin[bin] : A.bin_off[bin], r1 = A.dbin ? A.dbin[bin + 1] : A.bin_off[bin + 1];
   const int ncta = A.cta0[bin + 1] - A.cta0[bin];
   const int lcta = cta - A.cta0[bin];
   if (bin < kBins - 1) {
@@ -131,13 +155,14 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const d
     for (int64_t qb = warp_first; qb < r1; qb += (int64_t)ncta * rows_per_cta) {
       const int64_t q = qb + (threadIdx.x & 31) / g;
       bool valid = q < r1;
-      const int32_t row = valid ? A.perm[q] : 0;
-      if (MASK && valid) valid = imask[row_inst[row]] != 0;
-      const int32_t kb = valid ? A.rp[row] : 0, ke = valid ? A.rp[row + 1] : 0;
-      double s0 = 0.0, s1 = 0.0, t0 = 0.0, t1 = 0.0;
+      const int4 ri = valid ? __ldg(A.rows + q) : make_int4(0, 0, 0, 0);
+      const int32_t row = ri.x;
+      if (MASK && valid) valid = imask[ri.w] != 0;
+      const int32_t kb = valid ? ri.y : 0, ke = valid ? ri.z : 0;
+      T s0 = T(0), s1 = T(0), t0 = T(0), t1 = T(0);
       int32_t k = kb + lane_g;
       for (; k + g < ke; k += 2 * g) {  // two independent gathers in flight
-        const double a = A.v[k], b = A.v[k + g];
+        const T a = A.v[k], b = A.v[k + g];
         const int32_t ca = A.ci[k], cb = A.ci[k + g];
         s0 = fma(a, x0[ca], s0);
         t0 = fma(b, x0[cb], t0);
@@ -147,7 +172,7 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const d
         }
       }
       if (k < ke) {
-        const double a = A.v[k];
+        const T a = A.v[k];
         const int32_t ca = A.ci[k];
         s0 = fma(a, x0[ca], s0);
         if (NV == 2) s1 = fma(a, x1[ca], s1);
@@ -164,18 +189,20 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const d
       }
     }
   } else {
-    __shared__ double red0[kWarps], red1[kWarps];
+    __shared__ T red0[kWarps], red1[kWarps];
     for (int64_t q = r0 + lcta; q < r1; q += ncta) {
-      const int32_t row = A.perm[q];
-      if (MASK && !imask[row_inst[row]]) continue;  // CTA-uniform
-      const int32_t kb = A.rp[row], ke = A.rp[row + 1];
-      double s0 = 0.0, s1 = 0.0;
+      const int4 ri = __ldg(A.rows + q);
+      const int32_t row = ri.x;
+      if (MASK && !imask[ri.w]) continue;  // CTA-uniform
+      const int32_t kb = ri.y, ke = ri.z;
+      RowAcc<T> a0, a1;
       for (int32_t k = kb + threadIdx.x; k < ke; k += kThreads) {
-        const double a = A.v[k];
+        const T a = A.v[k];
         const int32_t col = A.ci[k];
-        s0 = fma(a, x0[col], s0);
-        if (NV == 2) s1 = fma(a, x1[col], s1);
+        a0.add(a * x0[col]);
+        if (NV == 2) a1.add(a * x1[col]);
       }
+      T s0 = a0.s, s1 = a1.s;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         s0 += __shfl_down_sync(kFull, s0, o);
@@ -188,13 +215,13 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrDev A, const d
       }
       __syncthreads();
       if (threadIdx.x == 0) {
-        double t0 = 0.0, t1 = 0.0;
+        RowAcc<T> t0, t1;
         for (int i = 0; i < kWarps; ++i) {
-          t0 += red0[i];
-          t1 += red1[i];
+          t0.add(red0[i]);
+          t1.add(red1[i]);
         }
-        y0[row] = t0;
-        if (NV == 2) y1[row] = t1;
+        y0[row] = t0.s;
+        if (NV == 2) y1[row] = t1.s;
       }
       __syncthreads();
     }

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/pdcs.h"
+#include "pdcs_fp32.cuh"
 #include "pdcs_kernels.cuh"
 #include "pdcs_preprocess.cuh"
 
@@ -380,6 +381,12 @@ class Solver {
          *ybest = nullptr;
   double *tn[6] = {}, *tm[6] = {};
   double *xds_ = nullptr, *yds_ = nullptr;  // iterates at the start of an outer iteration (omega update)
+  // FP32-bulk mode (precision 1): FP32 matrices and deltas, FP64 anchors and averages
+  bool fp32_ = false;
+  CsrT<float> G32_{}, Gt32_{};
+  float *dx32_ = nullptr, *dxl32_ = nullptr, *dy32_ = nullptr, *dyl32_ = nullptr;
+  float *aty32_ = nullptr, *gx32_ = nullptr, *gxl32_ = nullptr;
+  double *xa_ = nullptr, *ya_ = nullptr, *qa_ = nullptr, *ra_ = nullptr, *dxm_ = nullptr, *dym_ = nullptr;
   double *part_x = nullptr, *part_y = nullptr, *part_r = nullptr, *red_out = nullptr;
   double *part_a = nullptr, *part_b = nullptr;  // partials of host-driven (non-graph) reductions
   PdhgState* st_dev = nullptr;
@@ -418,7 +425,10 @@ class Solver {
   int validate();
   void setup();
   void build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
-                  const int32_t* d_ci, const double* d_v, CsrDev& D);
+                  const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst);
+  // instance of each row of G and of G' (batched solver; NULL: one instance)
+  const int32_t* inst_of_y_ = nullptr;
+  const int32_t* inst_of_x_ = nullptr;
   int warp_grid(int64_t rows) const {
     return (int)std::max<int64_t>(1, std::min<int64_t>((rows * 32 + kThreads - 1) / kThreads, 148 * 16));
   }
@@ -429,6 +439,12 @@ class Solver {
   // ---- device helpers ----
   void spmv(const CsrDev& M, const double* xin, double* yout) {
     spmv_binned_kernel<1><<<M.cta0[kBins], kThreads, 0, s_>>>(M, xin, nullptr, yout, nullptr, nullptr);
+    kernels_++;
+  }
+  // rows of the instances with mask[k] != 0 only (batched solver)
+  void spmv_masked(const CsrDev& M, const double* xin, double* yout, const uint8_t* mask) {
+    spmv_binned_kernel<1, true><<<M.cta0[kBins], kThreads, 0, s_>>>(M, xin, nullptr, yout, nullptr, nullptr, nullptr,
+                                                                    mask);
     kernels_++;
   }
   void axpby(double* out, double a, const double* u, double b, const double* v, int64_t len) {
@@ -539,6 +555,11 @@ class Solver {
     return (hn > 1e-10 && cn > 1e-10) ? cn / hn : 1.0;
   }
   void run_until_halt();
+  void setup_fp32();
+  // FP32 mode: fix FP64 anchors at the current iterates (mask: instances, NULL = all)
+  void anchor(const int32_t* ix, const int32_t* iy, const uint8_t* mask);
+  // FP32 mode: fold the deltas back into the FP64 iterates
+  void materialize(const int32_t* ix, const int32_t* iy, const uint8_t* mask);
   void main_loop();
   double power_method(bool* converged);
   void resolving();
@@ -566,19 +587,20 @@ int Solver::validate() {
   for (int64_t i = 0; i < P.n_rsoc_x; ++i) nsum += P.rsoc_x[i];
   if (nsum > P.n) return PDCS_ERR_N_MISMATCH;
   if (O.use_preconditioner == 0 || O.use_adaptive_restart == 0 || O.use_adaptive_step_size_weight == 0 ||
-      O.use_aggressive == 0 || O.use_accelerated != 0 || O.precision != 0)
+      O.use_aggressive == 0 || O.use_accelerated != 0 || (O.precision != 0 && O.precision != 1))
     return PDCS_ERR_UNSUPPORTED;  // only the reference GPU module's live main loop (rpdhg_alg_gpu_gen.jl:1886-1927)
   return PDCS_OK;
 }
 
 void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
-                        const int32_t* d_ci, const double* d_v, CsrDev& D) {
+                        const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst) {
   D.m = rows;
   D.n = cols;
   D.nnz = rp[rows];
   D.rp = d_rp;
   D.ci = d_ci;
   D.v = d_v;
+  D.dbin = nullptr;
   std::vector<std::vector<int32_t>> bins(kBins);
   for (int64_t i = 0; i < rows; ++i) {
     int64_t L = rp[i + 1] - rp[i];
@@ -594,8 +616,8 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
     }
     bins[b].push_back((int32_t)i);
   }
-  std::vector<int32_t> perm;
-  perm.reserve(rows);
+  std::vector<int4> desc;
+  desc.reserve(rows);
   int64_t off = 0;
   int32_t cta = 0;
   for (int b = 0; b < kBins; ++b) {
@@ -603,7 +625,7 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
     D.cta0[b] = cta;
     int64_t R = (int64_t)bins[b].size();
     off += R;
-    perm.insert(perm.end(), bins[b].begin(), bins[b].end());
+    for (int32_t r : bins[b]) desc.push_back(make_int4(r, rp[r], rp[r + 1], row_inst ? row_inst[r] : 0));
     if (R == 0) continue;
     if (b < kBins - 1) {
       int64_t rows_per_cta = kThreads >> b;
@@ -614,10 +636,11 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
   }
   D.bin_off[kBins] = off;
   D.cta0[kBins] = std::max(cta, 1);
-  int32_t* d_perm = A.alloc<int32_t>(perm.size());
-  if (!perm.empty())
-    PDCS_CUDA(cudaMemcpyAsync(d_perm, perm.data(), perm.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s_));
-  D.perm = d_perm;
+  int4* d_desc = A.alloc<int4>(std::max<size_t>(desc.size(), 1));
+  if (!desc.empty())
+    PDCS_CUDA(cudaMemcpyAsync(d_desc, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));  // the host vector is released on return
+  D.rows = d_desc;
 }
 
 void Solver::size_table(ConeTable& T) {
@@ -868,8 +891,8 @@ void Solver::setup() {
   PDCS_CUDA(cudaMemcpyAsync(rp_h.data(), g_rp, sizeof(int32_t) * (m_ + 1), cudaMemcpyDeviceToHost, s_));
   PDCS_CUDA(cudaMemcpyAsync(trp_h.data(), t_rp, sizeof(int32_t) * (n_ + 1), cudaMemcpyDeviceToHost, s_));
   PDCS_CUDA(cudaStreamSynchronize(s_));
-  build_bins(rp_h, m_, n_, g_rp, g_ci, g_v, G_);
-  build_bins(trp_h, n_, m_, t_rp, t_ci, t_v, Gt_);
+  build_bins(rp_h, m_, n_, g_rp, g_ci, g_v, G_, inst_of_y_);
+  build_bins(trp_h, n_, m_, t_rp, t_ci, t_v, Gt_, inst_of_x_);
   // ---- iterates and work vectors ----
   auto vecn = [&]() { return A.alloc<double>(n_); };
   auto vecm = [&]() { return A.alloc<double>(m_); };
@@ -905,13 +928,85 @@ void Solver::setup() {
   PDCS_CUDA(cudaMemsetAsync(st_dev, 0, sizeof(PdhgState), s_));
   grid_reflect_ = grid_for(std::max(n_, m_));
   attempts_per_graph_ = O.attempts_per_graph > 0 ? O.attempts_per_graph : 32;
+  if (O.precision == 1) setup_fp32();
   PDCS_CUDA(cudaStreamSynchronize(s_));
+}
+
+void Solver::setup_fp32() {
+  fp32_ = true;
+  float* gv = A.alloc<float>(nnz_);
+  float* tv = A.alloc<float>(nnz_);
+  to_float_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(gv, G_.v, nnz_);
+  to_float_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(tv, Gt_.v, nnz_);
+  auto narrow = [](const CsrDev& D, const float* v) {
+    CsrT<float> F;
+    F.m = D.m;
+    F.n = D.n;
+    F.nnz = D.nnz;
+    F.rp = D.rp;
+    F.ci = D.ci;
+    F.v = v;
+    F.rows = D.rows;
+    F.dbin = D.dbin;
+    for (int b = 0; b <= kBins; ++b) {
+      F.bin_off[b] = D.bin_off[b];
+      F.cta0[b] = D.cta0[b];
+    }
+    return F;
+  };
+  G32_ = narrow(G_, gv);
+  Gt32_ = narrow(Gt_, tv);
+  dx32_ = A.alloc<float>(n_);
+  dxl32_ = A.alloc<float>(n_);
+  aty32_ = A.alloc<float>(n_);
+  dy32_ = A.alloc<float>(m_);
+  dyl32_ = A.alloc<float>(m_);
+  gx32_ = A.alloc<float>(m_);
+  gxl32_ = A.alloc<float>(m_);
+  xa_ = A.alloc<double>(n_);
+  qa_ = A.alloc<double>(n_);
+  dxm_ = A.alloc<double>(n_);
+  ya_ = A.alloc<double>(m_);
+  ra_ = A.alloc<double>(m_);
+  dym_ = A.alloc<double>(m_);
+}
+
+void Solver::anchor(const int32_t* ix, const int32_t* iy, const uint8_t* mask) {
+  anchor_kernel<<<grid_for(n_), kThreads, 0, s_>>>(x, xl, xm, xa_, dx32_, dxl32_, dxm_, ix, mask, n_);
+  anchor_kernel<<<grid_for(m_), kThreads, 0, s_>>>(y, yl, ym, ya_, dy32_, dyl32_, dym_, iy, mask, m_);
+  if (mask) {
+    spmv_masked(Gt_, ya_, qa_, mask);
+    spmv_masked(G_, xa_, ra_, mask);
+  } else {
+    spmv(Gt_, ya_, qa_);
+    spmv(G_, xa_, ra_);
+  }
+  masked_sub_kernel<<<grid_for(n_), kThreads, 0, s_>>>(qa_, qa_, c_s, ix, mask, n_);
+  masked_sub_kernel<<<grid_for(m_), kThreads, 0, s_>>>(ra_, ra_, h_s, iy, mask, m_);
+  kernels_ += 4;
+}
+
+void Solver::materialize(const int32_t* ix, const int32_t* iy, const uint8_t* mask) {
+  materialize_kernel<<<grid_for(n_), kThreads, 0, s_>>>(x, xl, xm, xa_, dx32_, dxl32_, dxm_, ix, mask, n_);
+  materialize_kernel<<<grid_for(m_), kThreads, 0, s_>>>(y, yl, ym, ya_, dy32_, dyl32_, dym_, iy, mask, m_);
+  kernels_ += 2;
 }
 
 void Solver::capture_graph() {
   PDCS_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
   const int32_t* act = &st_dev->active;
-  for (int a = 0; a < attempts_per_graph_; ++a) {
+  for (int a = 0; a < attempts_per_graph_ && fp32_; ++a) {
+    spmv_binned_kernel<1, false, float><<<Gt32_.cta0[kBins], kThreads, 0, s_>>>(Gt32_, dyl32_, nullptr, aty32_,
+                                                                               nullptr, act, &st_dev->do_reflect);
+    OpPrimalStep32 op1{xa_, dxl32_, qa_, aty32_, dx32_, x, st_dev, 0.0};
+    update_project_kernel<OpPrimalStep32><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, act);
+    spmv_binned_kernel<2, false, float><<<G32_.cta0[kBins], kThreads, 0, s_>>>(G32_, dx32_, dxl32_, gx32_, gxl32_,
+                                                                             act);
+    OpDualStep32 op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, st_dev, 0.0, part_x, XI.ctaA + XI.ctaB + XI.ctaC};
+    update_project_kernel<OpDualStep32><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, act);
+    reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, dx32_, dxl32_, dxm_, n_, dy32_, dyl32_, dym_, m_);
+  }
+  for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
     spmv_binned_kernel<1><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, yl, nullptr, aty, nullptr, act,
                                                                 &st_dev->do_reflect);
     OpPrimalStep op1{xl, aty, c_s, x, st_dev, 0.0};
@@ -1259,6 +1354,7 @@ void Solver::run_until_halt() {
   Timer tm_(t_iter_);
   push_state();
   if (!graph_exec_) capture_graph();
+  if (fp32_) anchor(nullptr, nullptr, nullptr);
   while (true) {
     int64_t to_check = S.check_freq > 0 ? S.check_freq - (S.iter % S.check_freq) : 1 << 20;
     int64_t graphs = (to_check + attempts_per_graph_ - 1) / attempts_per_graph_;
@@ -1269,9 +1365,14 @@ void Solver::run_until_halt() {
       kernels_ += 5LL * attempts_per_graph_;
     }
     pull_state();
-    if (!S.active) return;
-    if (O.time_limit > 0 && now_s() - t_start_ > O.time_limit) return;
+    if (!S.active) break;
+    if (O.time_limit > 0 && now_s() - t_start_ > O.time_limit) break;
+    if (fp32_) {  // FP64 refinement: new anchors, so the FP32 deltas stay one round's movement
+      materialize(nullptr, nullptr, nullptr);
+      anchor(nullptr, nullptr, nullptr);
+    }
   }
+  if (fp32_) materialize(nullptr, nullptr, nullptr);  // the host works on the FP64 iterates
 }
 
 void Solver::log_progress() {
@@ -1674,6 +1775,61 @@ int pdcs_solve_batch(int64_t count, const pdcs_problem* problems, const pdcs_opt
     std::fprintf(stderr, "pdcs_solve_batch: %s\n", e.what());
     return PDCS_ERR_INVALID;
   }
+}
+
+struct pdcs_batch {
+  pdcs::BatchSolver* solver;
+};
+
+int pdcs_batch_create(int64_t count, const pdcs_problem* problems, const pdcs_options* opts, pdcs_batch** out) {
+  if (count < 1 || !problems || !out) return PDCS_ERR_INVALID;
+  *out = nullptr;
+  pdcs_options o;
+  if (opts) o = *opts;
+  else pdcs_default_options(&o);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PDCS_ERR_NO_DEVICE;
+  pdcs::BatchSolver* b = nullptr;
+  try {
+    b = new pdcs::BatchSolver(count, problems, &o);
+    int rc = b->prepare();
+    if (rc != PDCS_OK) {
+      delete b;
+      return rc;
+    }
+    *out = new pdcs_batch{b};
+    return PDCS_OK;
+  } catch (const pdcs::CudaError& e) {
+    std::fprintf(stderr, "pdcs_batch_create: %s\n", e.what());
+    delete b;
+    return PDCS_ERR_CUDA;
+  } catch (const std::domain_error&) {
+    delete b;
+    return PDCS_ERR_BOUNDS;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "pdcs_batch_create: %s\n", e.what());
+    delete b;
+    return PDCS_ERR_INVALID;
+  }
+}
+
+int pdcs_batch_solve(pdcs_batch* batch, int64_t attempt_limit, pdcs_result* results, pdcs_batch_info* info) {
+  if (!batch || !batch->solver || !results) return PDCS_ERR_INVALID;
+  try {
+    return batch->solver->solve(results, info, attempt_limit);
+  } catch (const pdcs::CudaError& e) {
+    std::fprintf(stderr, "pdcs_batch_solve: %s\n", e.what());
+    return PDCS_ERR_CUDA;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "pdcs_batch_solve: %s\n", e.what());
+    return PDCS_ERR_INVALID;
+  }
+}
+
+void pdcs_batch_destroy(pdcs_batch* batch) {
+  if (!batch) return;
+  delete batch->solver;
+  delete batch;
 }
 
 int pdcs_block_proj(double* arr, const double* bl, const double* bu, const double* S, const int64_t* head_start,

@@ -170,8 +170,11 @@ def _options_struct(L, hold: _Holder, *, n=0, m=0, rescaling_method: str = "ruiz
                     method: str = "average", logfile_name: Optional[str] = None, use_kkt_restart: bool = False,
                     kkt_restart_freq: int = 2000, use_duality_gap_restart: bool = True,
                     duality_gap_restart_freq: int = 2000, attempt_limit: int = 0, attempts_per_graph: int = 32,
-                    stream=None, force_resolving: bool = False):
-    """Fill a PdcsOptions from the reference's keyword arguments (rpdhg_alg_gpu_gen.jl:1219-1268)."""
+                    stream=None, force_resolving: bool = False, precision="fp64"):
+    """Fill a PdcsOptions from the reference's keyword arguments (rpdhg_alg_gpu_gen.jl:1219-1268).
+
+    precision: "fp64" (the reference's arithmetic) or "fp32" (FP32 matrices and iterate deltas
+    between FP64 anchors; FP64 projections, averages and termination checks)."""
     if method not in ("average", "halpern"):
         raise ValueError("method only available for :average and :halpern")
     if method == "halpern":
@@ -208,6 +211,10 @@ def _options_struct(L, hold: _Holder, *, n=0, m=0, rescaling_method: str = "ruiz
     O.attempts_per_graph = attempts_per_graph
     O.force_resolving = int(force_resolving)
     O.stream = stream
+    prec = {"fp64": 0, "fp32": 1, 0: 0, 1: 1}.get(precision)
+    if prec is None:
+        raise ValueError("precision must be 'fp64' or 'fp32'")
+    O.precision = prec
     return O
 
 
@@ -262,6 +269,68 @@ class BatchInfo:
     single_fallbacks: int
 
 
+class BatchHandle:
+    """A prepared batch (pdcs_batch_create): merged, uploaded and preconditioned once;
+    ``solve()`` runs a cold-start batched solve of it (pdcs_batch_solve)."""
+
+    def __init__(self, problems, **options):
+        self._L = capi.load()
+        self._hold = _Holder()
+        self._h = C.c_void_p()
+        probs = [p.kwargs() if hasattr(p, "kwargs") else dict(p) for p in problems]
+        if not probs:
+            raise ValueError("empty batch")
+        self._Ps = (capi.PdcsProblem * len(probs))()
+        for i, kw in enumerate(probs):
+            self._Ps[i] = _problem_struct(self._hold, **{k: v for k, v in kw.items() if k in _PROBLEM_KEYS})
+            if self._Ps[i].on_device:
+                raise ValueError("pdcs_batch_create takes host data")
+        self._O = _options_struct(self._L, self._hold, **options)
+        self.count = len(probs)
+        self.sizes = [(P.n, P.m) for P in self._Ps]
+        rc = self._L.pdcs_batch_create(self.count, self._Ps, C.byref(self._O), C.byref(self._h))
+        capi.check(rc, "pdcs_batch_create")
+
+    def solve(self, attempt_limit: int = 0):
+        """Returns (list of Solution, BatchInfo)."""
+        if not self._h:
+            raise RuntimeError("batch handle is closed")
+        Rs = (capi.PdcsResult * self.count)()
+        outs = []
+        for i, (n, m) in enumerate(self.sizes):
+            xo, yo = np.zeros(n), np.zeros(m)
+            outs.append((xo, yo))
+            Rs[i].x = xo.ctypes.data if n else None
+            Rs[i].y = yo.ctypes.data if m else None
+        B = capi.PdcsBatchInfo()
+        rc = self._L.pdcs_batch_solve(self._h, attempt_limit, Rs, C.byref(B))
+        capi.check(rc, "pdcs_batch_solve")
+        return [Solution(outs[i][0], outs[i][1], _info(Rs[i])) for i in range(self.count)], _batch_info(B)
+
+    def close(self):
+        if self._h:
+            self._L.pdcs_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _batch_info(B) -> "BatchInfo":
+    return BatchInfo(setup_time=B.setup_time, solve_time=B.solve_time, time_iterations=B.time_iterations,
+                     kernel_launches=B.kernel_launches, graph_launches=B.graph_launches,
+                     service_rounds=B.service_rounds, single_fallbacks=B.single_fallbacks)
+
+
 def rpdhg_gpu_solve_batch(problems, **options):
     """Solve many independent programs in one batched run (pdcs_solve_batch).
 
@@ -290,10 +359,7 @@ def rpdhg_gpu_solve_batch(problems, **options):
     rc = L.pdcs_solve_batch(len(probs), Ps, C.byref(O), Rs, C.byref(B))
     capi.check(rc, "pdcs_solve_batch")
     sols = [Solution(outs[i][0], outs[i][1], _info(Rs[i])) for i in range(len(probs))]
-    info = BatchInfo(setup_time=B.setup_time, solve_time=B.solve_time, time_iterations=B.time_iterations,
-                     kernel_launches=B.kernel_launches, graph_launches=B.graph_launches,
-                     service_rounds=B.service_rounds, single_fallbacks=B.single_fallbacks)
-    return sols, info
+    return sols, _batch_info(B)
 
 
 def solve_problem(prob, **kw) -> Solution:

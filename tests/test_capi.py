@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "pdcs.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pdcs_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char\*)\s+(pdcs_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_expected_entry_points():

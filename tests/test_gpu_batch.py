@@ -109,3 +109,16 @@ def test_batch_validation(cuda):
     extra["G"] = sp.hstack([sp.csr_matrix(extra["G"]), sp.csr_matrix((extra["m"], 1))]).tocsr()
     with pytest.raises(RuntimeError, match="status -7"):
         solver.rpdhg_gpu_solve_batch([ok, extra])
+
+
+def test_batch_handle_resolves_identically(cuda):
+    batch = _mixed_batch()[:3]
+    with solver.BatchHandle(batch) as h:
+        a, _ = h.solve(attempt_limit=50)
+        b, _ = h.solve(attempt_limit=50)
+        c, info = h.solve()
+    one, _ = solver.rpdhg_gpu_solve_batch(batch)
+    for x, y, z, w in zip(a, b, c, one):
+        assert np.array_equal(x.primal, y.primal) and x.info.iter == 50  # cold start each time
+        assert z.info.exit_status == w.info.exit_status == "optimal"
+        assert z.info.iter == w.info.iter and np.array_equal(z.primal, w.primal)

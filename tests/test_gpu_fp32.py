@@ -1,0 +1,72 @@
+"""FP32-bulk mode (precision="fp32"): FP32 matrices and iterate deltas between
+FP64 anchors.  Its iterates are not the oracle's bit for bit; the checks are
+(1) the first attempts stay within FP32 rounding of the oracle's FP64
+trajectory, (2) converged solutions meet the 1e-6 criteria under the oracle's
+FP64 evaluator and their objectives agree with the FP64 oracle's.  The
+measured errors are printed (pytest -s) for each instance."""
+import numpy as np
+import pytest
+
+from oracle import binding as B
+from pdcs_b200 import problems, solver
+
+pytestmark = pytest.mark.gpu
+
+INSTANCES = {
+    "socp_c0": lambda: problems.socp_c0(),
+    "mixed_small": lambda: problems.mixed_small(),
+    "mixed_medium": lambda: problems.mixed_small(seed=9, scale=6),
+    "logreg_small": lambda: problems.logreg_exp_c1(samples=300, features=30, density=0.2),
+}
+
+
+@pytest.mark.parametrize("name", ["socp_c0", "mixed_small", "logreg_small"])
+def test_fp32_first_attempts_near_oracle(cuda, name):
+    p = INSTANCES[name]()
+    # FP32 rounding is ~1e-7 relative; the adaptive step's accept / retry decisions
+    # then let two trajectories drift apart slowly, so later attempts get a looser bound
+    for attempts, tol in ((1, 2e-6), (7, 2e-6), (40, 1e-3)):
+        g = solver.solve_problem(p, attempt_limit=attempts, precision="fp32")
+        o = B.solve(p, threads=1, attempt_limit=attempts)
+        assert g.info.iter == o["iter"] == attempts
+        for a, b in ((g.primal, o["x"]), (g.dual, o["y"])):
+            err = np.abs(a - b).max() / max(1.0, np.abs(b).max())
+            print(f"{name} attempts={attempts} max rel err vs FP64 oracle {err:.2e}")
+            assert err <= tol, (name, attempts, err)
+
+
+@pytest.mark.parametrize("name", list(INSTANCES))
+def test_fp32_solution_meets_fp64_criteria(cuda, name):
+    p = INSTANCES[name]()
+    g = solver.solve_problem(p, time_limit=120, precision="fp32")
+    assert g.info.exit_status == "optimal", g
+    e = B.evaluate(p, g.primal, g.dual)
+    assert max(e["primal_res_gpu_form"], e["dual_res"], e["rel_gap"]) < 1.05e-6, e
+    o = B.solve(p, threads=4)
+    eo = B.evaluate(p, o["x"], o["y"])
+    rel = abs(e["pobj"] - eo["pobj"]) / (1 + abs(eo["pobj"]))
+    print(f"{name}: fp32 iters {g.info.iter} vs oracle {o['iter']}; objective rel err {rel:.2e}; "
+          f"criteria {e['primal_res_gpu_form']:.2e} {e['dual_res']:.2e} {e['rel_gap']:.2e}")
+    assert rel <= 2e-6, (e["pobj"], eo["pobj"])
+
+
+def test_fp32_batch(cuda):
+    batch = [problems.mixed_small(seed=7), problems.logreg_exp_c1(samples=120, features=12, density=0.3)] + \
+        problems.batch_socp_c3(count=5, seed=41, nmin=50, nmax=500)
+    sols, info = solver.rpdhg_gpu_solve_batch(batch, time_limit=300, precision="fp32")
+    ref, _ = solver.rpdhg_gpu_solve_batch(batch, time_limit=300)
+    for p, g, r in zip(batch, sols, ref):
+        assert g.info.exit_status == r.info.exit_status == "optimal", (p.name, g)
+        e = B.evaluate(p, g.primal, g.dual)
+        assert max(e["primal_res_gpu_form"], e["dual_res"], e["rel_gap"]) < 1.05e-6, (p.name, e)
+        rel = abs(g.info.pObj - r.info.pObj) / (1 + abs(r.info.pObj))
+        assert rel <= 2e-6, (p.name, g.info.pObj, r.info.pObj)
+
+
+def test_fp32_batch_first_attempts_match_single_fp32(cuda):
+    batch = [problems.mixed_small(seed=7), problems.socp_c0(n_box=60, n_soc=60, m=90, density=0.08, seed=5)]
+    sols, _ = solver.rpdhg_gpu_solve_batch(batch, attempt_limit=30, precision="fp32")
+    for p, g in zip(batch, sols):
+        s = solver.solve_problem(p, attempt_limit=30, precision="fp32")
+        scale = max(1.0, np.abs(s.primal).max())
+        assert np.abs(g.primal - s.primal).max() <= 1e-5 * scale
