@@ -108,6 +108,9 @@ typedef struct {
   void* stream;                  /* cudaStream_t to run on; NULL = an internal stream */
   int32_t attempts_per_graph;    /* PDHG attempts captured per CUDA graph (default 32) */
   int32_t force_resolving;       /* test hook: enter the resolving fallback at the first outer iteration */
+  int32_t spmv_lane_nnz;         /* SpMV schedule, nonzeros per lane of a row's lane group (power of two,
+                                    1..16); 0 (default) = autotuned per matrix at setup */
+  int32_t reserved_opt;
 } pdcs_options;
 
 typedef struct {
@@ -131,6 +134,8 @@ typedef struct {
   double time_exit_checks;   /* seconds in termination checks (every check_terminate_freq) */
   double time_restarts;      /* seconds in restart thresholds / restart checks    */
   int64_t restart_probes;    /* projections probes of the restart binary searches */
+  int32_t spmv_lane_nnz_G;   /* SpMV schedules used for G and G' (nonzeros per lane) */
+  int32_t spmv_lane_nnz_Gt;
 } pdcs_result;
 
 /* Fills *opts with the reference's defaults. */

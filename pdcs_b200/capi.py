@@ -64,7 +64,8 @@ class PdcsOptions(C.Structure):
                 ("time_limit", C.c_double), ("kkt_restart_freq", C.c_int64),
                 ("use_duality_gap_restart", C.c_int32), ("precision", C.c_int32),
                 ("duality_gap_restart_freq", C.c_int64), ("attempt_limit", C.c_int64),
-                ("stream", _vp), ("attempts_per_graph", C.c_int32), ("force_resolving", C.c_int32)]
+                ("stream", _vp), ("attempts_per_graph", C.c_int32), ("force_resolving", C.c_int32),
+                ("spmv_lane_nnz", C.c_int32), ("reserved_opt", C.c_int32)]
 
 
 class PdcsResult(C.Structure):
@@ -79,7 +80,8 @@ class PdcsResult(C.Structure):
                 ("l_inf_abs_dual_res", C.c_double), ("abs_gap", C.c_double),
                 ("kernel_launches", C.c_int64), ("graph_launches", C.c_int64),
                 ("time_iterations", C.c_double), ("time_exit_checks", C.c_double),
-                ("time_restarts", C.c_double), ("restart_probes", C.c_int64)]
+                ("time_restarts", C.c_double), ("restart_probes", C.c_int64),
+                ("spmv_lane_nnz_G", C.c_int32), ("spmv_lane_nnz_Gt", C.c_int32)]
 
 
 class PdcsBatchInfo(C.Structure):

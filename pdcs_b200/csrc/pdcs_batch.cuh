@@ -680,11 +680,11 @@ void BatchSolver::capture_batch_graph() {
     spmv_binned_kernel<1, false, float><<<Gt32c_.cta0[kBins], kThreads, 0, s_>>>(Gt32c_, dyl32_, nullptr, aty32_,
                                                                                nullptr, cur);
     OpPrimalStep32B op1{xa_, dxl32_, qa_, aty32_, dx32_, x, ix_, live_, ps_, dxsq_};
-    update_project_kernel<OpPrimalStep32B><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, cur);
+    launch_update_project(op1, XI, part_x, cur, s_);
     spmv_binned_kernel<2, false, float><<<G32c_.cta0[kBins], kThreads, 0, s_>>>(G32c_, dx32_, dxl32_, gx32_,
                                                                               gxl32_, cur);
     OpDualStep32B op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_};
-    update_project_kernel<OpDualStep32B><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, cur);
+    launch_update_project(op2, YI, part_y, cur, s_);
     BatchCtl ctl{sts_, ps_, ds_, live_, rx_, ry_, dxsq_, dysq_, dgdy_, cur, nxt, done_ctas_, live_cnt_ + 2};
     batch_control_kernel<<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
     batch_reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dx32_, dxl32_, dxm_, n_, dy32_,
@@ -695,10 +695,10 @@ void BatchSolver::capture_batch_graph() {
     int32_t* nxt = live_cnt_ + ((a + 1) & 1);
     spmv_binned_kernel<1><<<Gtc_.cta0[kBins], kThreads, 0, s_>>>(Gtc_, yl, nullptr, aty, nullptr, cur);
     OpPrimalStepB op1{xl, aty, c_s, x, ix_, live_, ps_, dxsq_};
-    update_project_kernel<OpPrimalStepB><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, cur);
+    launch_update_project(op1, XI, part_x, cur, s_);
     spmv_binned_kernel<2><<<Gc_.cta0[kBins], kThreads, 0, s_>>>(Gc_, x, xl, gx, gxl, cur);
     OpDualStepB op2{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_};
-    update_project_kernel<OpDualStepB><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, cur);
+    launch_update_project(op2, YI, part_y, cur, s_);
     BatchCtl ctl{sts_, ps_, ds_, live_, rx_, ry_, dxsq_, dysq_, dgdy_, cur, nxt, done_ctas_, live_cnt_ + 2};
     batch_control_kernel<<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
     batch_reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, x, xl, xm, n_, y, yl, ym, m_);
@@ -891,6 +891,7 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   }
   int64_t graphs = (to_check + attempts_per_graph_ - 1) / attempts_per_graph_;
   graphs = std::max<int64_t>(1, std::min<int64_t>(graphs, 4));
+  const double t_round = now_s();
   for (int64_t gi = 0; gi < graphs; ++gi) {
     PDCS_CUDA(cudaGraphLaunch(bgraph_exec_, s_));
     graphs_++;
@@ -899,6 +900,10 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   PdhgState* back = stage<PdhgState>(K_);
   PDCS_CUDA(cudaMemcpyAsync(back, sts_, sizeof(PdhgState) * K_, cudaMemcpyDeviceToHost, s_));
   sync_reset();  // `back` stays readable: nothing is staged before the loop below ends
+  if (O.verbose)
+    std::printf("[pdcs_b200 batch] %.3f s: %zu of %lld instances iterating, %lld attempts in %.3f ms\n",
+                now_s() - t_start_, its.size(), (long long)K_, (long long)(graphs * attempts_per_graph_),
+                1e3 * (now_s() - t_round));
   const bool timeout = O.time_limit > 0 && now_s() - t_start_ > O.time_limit;
   std::vector<Inst*> halted;
   for (Inst* I : its) {
@@ -1390,6 +1395,8 @@ void BatchSolver::reset_state() {
   const int64_t nxe = XI.exp_count + XI.dexp_count, nye = YI.exp_count + YI.dexp_count;
   if (nxe) PDCS_CUDA(cudaMemsetAsync(XI.rho_ws, 0xff, sizeof(double) * nxe, s_));
   if (nye) PDCS_CUDA(cudaMemsetAsync(YI.rho_ws, 0xff, sizeof(double) * nye, s_));
+  if (XI.nwc) PDCS_CUDA(cudaMemsetAsync(XI.soc_ws, 0xff, sizeof(double) * XI.nwc, s_));
+  if (YI.nwc) PDCS_CUDA(cudaMemsetAsync(YI.soc_ws, 0xff, sizeof(double) * YI.nwc, s_));
   PDCS_CUDA(cudaMemsetAsync(live_cnt_, 0, 4 * sizeof(int32_t), s_));
   PDCS_CUDA(cudaMemsetAsync(done_ctas_, 0, sizeof(uint32_t), s_));
   inst_.clear();
@@ -1479,6 +1486,8 @@ int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_
     R.kernel_launches = kernels_;
     R.graph_launches = graphs_;
     R.restart_probes = I.probes;
+    R.spmv_lane_nnz_G = lane_G_;
+    R.spmv_lane_nnz_Gt = lane_Gt_;
   }
   if (info) {
     info->setup_time = setup_time_;

@@ -106,6 +106,110 @@ __device__ inline void warp_soc_reg(double& v, double w, int d, bool weighted) {
   else if (act) v = v / (1.0 + mu * D * D);
 }
 
+// ---------------------------------------------------------------------------
+// Lane groups: g lanes (g = 2..32, a power of two) per block, 32 / g blocks per
+// warp.  Reductions are xor butterflies within the group followed by a
+// broadcast from the group's lane 0 (identical values in every lane).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double grp_sum(double v, int g) {
+  for (int o = g >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o, g);
+  return __shfl_sync(kFull, v, 0, g);
+}
+__device__ __forceinline__ double grp_max(double v, int g) {
+  for (int o = g >> 1; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o, g));
+  return __shfl_sync(kFull, v, 0, g);
+}
+__device__ __forceinline__ double grp_bcast(double v, int g) { return __shfl_sync(kFull, v, 0, g); }
+
+// warp_soc_reg for a lane group (block of d <= g elements, element i in group
+// lane i).  Every lane runs the same shuffles: groups whose block is inside,
+// polar, unweighted or converged idle through the remaining Newton steps.
+// ws: the block's warm start of the Newton root (s * scale from its previous
+// projection, NaN = none; NULL = no warm start).  Q is concave increasing, so
+// from a start above the root one Newton step lands at or below it; from
+// there the iterates climb monotonically as in warp_soc_reg.
+__device__ inline void group_soc_reg(double& v, double w, int d, bool weighted, int g, double* ws) {
+  const int gl = threadIdx.x & (g - 1);
+  const bool act = gl < d;
+  const double scale = grp_max(act ? fabs(v) : 0.0, g);
+  const bool trivial = scale == 0.0 || !isfinite(scale);
+  const double sc = trivial ? 1.0 : scale;
+  const double t = grp_bcast(v, g) / sc;
+  const double xi = (act && gl >= 1) ? v / sc : 0.0;
+  const double D = (act && gl >= 1) ? w : 1.0;
+  const double nDx = sqrt(grp_sum((D * xi) * (D * xi), g));
+  const double nxD = sqrt(grp_sum((xi / D) * (xi / D), g));
+  const bool inside = trivial || nDx <= t;
+  const bool polar = !inside && nxD <= -t;
+  const bool rest = !inside && !polar;
+  const bool zero_t = rest && weighted && t == 0.0;
+  const bool newton = rest && weighted && t != 0.0;
+  // t == 0: closed form (every lane computes it; only zero_t groups use it)
+  const double y0 = xi / (1.0 + D * D);
+  const double s_zero = sqrt(grp_sum((D * y0) * (D * y0), g));
+  const double c = D * D * xi * xi;
+  const double a = 1.0 + D * D;
+  const double s_lo = fmax(t, 0.0);
+  double s = s_lo;
+  double sw = (newton && ws && gl == 0) ? *ws : __longlong_as_double(0x7ff8000000000000ll);
+  sw = grp_bcast(sw, g) / sc;
+  bool first = newton && isfinite(sw) && sw > s_lo;
+  if (first) s = sw;
+  bool done = !newton;
+  for (int it = 0; it < 200; ++it) {
+    if (!__any_sync(kFull, !done)) break;
+    double S1 = 0.0, S2 = 0.0;
+    if (!done && c != 0.0) {
+      const double iu = 1.0 / (s * a - t * D * D);
+      S1 = c * iu * iu;
+      S2 = c * a * iu * iu * iu;
+    }
+    S1 = grp_sum(S1, g);
+    S2 = grp_sum(S2, g);
+    if (done) continue;
+    const double Q = 1.0 / sqrt(S1);
+    const double dQ = Q * Q * Q * S2;
+    const double step = (1.0 - Q) / dQ;
+    if (first) {
+      first = false;
+      if (step < 0.0) {  // warm start above the root
+        s = fmax(s + step, s_lo);
+        continue;
+      }
+    }
+    if (!(step > 0.0)) {
+      done = true;
+      continue;
+    }
+    const double sn = s + step;
+    if (!(sn > s)) {
+      done = true;
+      continue;
+    }
+    s = sn;
+    if (step <= 1e-17 * s) done = true;
+  }
+  if (inside) return;
+  if (polar) {
+    if (act) v = 0.0;
+    return;
+  }
+  if (!weighted) {
+    const double cc = 0.5 * (1.0 + t / nDx);
+    if (gl == 0) v = cc * nDx * sc;
+    else if (act) v *= cc;
+    return;
+  }
+  const double sf = zero_t ? s_zero : s;
+  const double mu = zero_t ? 1.0 : 1.0 - t / s;
+  if (gl == 0) {
+    v = sf * sc;
+    if (newton && ws) *ws = s * sc;
+  } else if (act) {
+    v = v / (1.0 + mu * D * D);
+  }
+}
+
 // Memory path for any d: block values in p[0..d), weights from wfun(i).
 template <class WF>
 __device__ inline void warp_soc_mem(double* p, int64_t d, WF wfun, bool weighted) {

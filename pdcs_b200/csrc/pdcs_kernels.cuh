@@ -88,8 +88,9 @@ __host__ __device__ inline void after_reject(PdhgState& st) {
 
 // ---------------------------------------------------------------------------
 // CSR SpMV with rows binned by length.  Bin b < 6 holds rows handled by a
-// group of g = 2^b lanes (rows of up to ~4g nonzeros); bin 6 holds long rows,
-// one CTA each.  One launch covers all bins: CTA ranges [cta0[b], cta0[b+1]).
+// group of g = 2^b lanes (rows of up to L g nonzeros for a schedule of L
+// nonzeros per lane, picked per matrix by the setup autotuner); bin 6 holds
+// longer rows, one CTA each.  One launch covers all bins: CTA ranges [cta0[b], cta0[b+1]).
 // ---------------------------------------------------------------------------
 constexpr int kBins = 7;
 
@@ -159,26 +160,30 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
       const int32_t row = ri.x;
       if (MASK && valid) valid = imask[ri.w] != 0;
       const int32_t kb = valid ? ri.y : 0, ke = valid ? ri.z : 0;
-      T s0 = T(0), s1 = T(0), t0 = T(0), t1 = T(0);
+      T s0 = T(0), s1 = T(0), t0 = T(0), t1 = T(0), u0 = T(0), u1 = T(0), w0 = T(0), w1 = T(0);
       int32_t k = kb + lane_g;
-      for (; k + g < ke; k += 2 * g) {  // two independent gathers in flight
-        const T a = A.v[k], b = A.v[k + g];
-        const int32_t ca = A.ci[k], cb = A.ci[k + g];
+      for (; k + 3 * g < ke; k += 4 * g) {  // four independent gathers in flight
+        const T a = A.v[k], b = A.v[k + g], c = A.v[k + 2 * g], d = A.v[k + 3 * g];
+        const int32_t ca = A.ci[k], cb = A.ci[k + g], cc = A.ci[k + 2 * g], cd = A.ci[k + 3 * g];
         s0 = fma(a, x0[ca], s0);
         t0 = fma(b, x0[cb], t0);
+        u0 = fma(c, x0[cc], u0);
+        w0 = fma(d, x0[cd], w0);
         if (NV == 2) {
           s1 = fma(a, x1[ca], s1);
           t1 = fma(b, x1[cb], t1);
+          u1 = fma(c, x1[cc], u1);
+          w1 = fma(d, x1[cd], w1);
         }
       }
-      if (k < ke) {
+      for (; k < ke; k += g) {
         const T a = A.v[k];
         const int32_t ca = A.ci[k];
         s0 = fma(a, x0[ca], s0);
         if (NV == 2) s1 = fma(a, x1[ca], s1);
       }
-      s0 += t0;
-      s1 += t1;
+      s0 = (s0 + t0) + (u0 + w0);
+      s1 = (s1 + t1) + (u1 + w1);
       for (int o = g >> 1; o > 0; o >>= 1) {
         s0 += __shfl_down_sync(kFull, s0, o, g);
         if (NV == 2) s1 += __shfl_down_sync(kFull, s1, o, g);
@@ -231,6 +236,8 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
 // ---------------------------------------------------------------------------
 // Block structure of one vector for projections.
 // ---------------------------------------------------------------------------
+constexpr int kCls = 6;
+
 struct ConeTable {
   int64_t len;
   int32_t nseg;
@@ -238,7 +245,7 @@ struct ConeTable {
   int64_t seg_start[3], seg_len[3];
   const double* lo;  // BOX bounds (global index)
   const double* hi;
-  int64_t nwc;               // SOC / RSOC blocks (one warp each)
+  int64_t nwc;               // SOC / RSOC blocks
   const int64_t* wc_start;
   const int32_t* wc_len;
   const int8_t* wc_kind;     // PK_SOC or PK_RSOC
@@ -248,6 +255,13 @@ struct ConeTable {
   int32_t dexp_kind;
   const double* S;           // scaling (NULL: unscaled)
   double* rho_ws;            // per exp/dual-exp cone warm start of the root (NULL: none)
+  // warp-cone schedule by size class: class c < kCls - 1 packs blocks of at
+  // most g = 2 << c elements, 32 / g per warp; the last class (> 32) takes a
+  // warp per block.  sched lists warp-cone indices class by class.
+  const int64_t* sched;
+  int64_t cls_off[kCls + 1];  // ranges of sched per class
+  int64_t task0[kCls + 1];    // first warp task of each class; task0[kCls] = tasks
+  double* soc_ws;             // per warp cone warm start of the weighted-SOC root (NULL: none)
   int64_t elem_total;        // sum of seg_len
   int32_t ctaA, ctaB, ctaC;  // CTAs for elementwise / warp cones / exp cones
 };
@@ -377,7 +391,9 @@ concept MaskedOp = requires(const Op& o) { o.live(int64_t(0)); };
 // Generic update + projection.  Op supplies:
 //   NACC, kinds[] (ACC_SUM / ACC_MAX), double* out (result / scratch, length T.len),
 //   load(): read scalars; z(j): value before projection; fin(j, z, p, acc): consume.
-template <class Op>
+// EXP: compile the exponential-cone path (its root solve sets the register
+// budget of the whole kernel; tables without exp cones use EXP = false).
+template <class Op, bool EXP = true>
 __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTable T, double* partials,
                                                                  const int32_t* active) {
   if (active && !*active) return;
@@ -404,45 +420,65 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
   } else if (b < T.ctaA + T.ctaB) {
     const int lane = threadIdx.x & 31;
     const int64_t wstride = (int64_t)T.ctaB * kWarps;
-    for (int64_t k = (int64_t)(b - T.ctaA) * kWarps + (threadIdx.x >> 5); k < T.nwc; k += wstride) {
-      const int64_t st = T.wc_start[k];
-      if constexpr (MaskedOp<Op>) {
-        if (!op.live(st)) continue;  // warp-uniform: a cone belongs to one instance
-      }
-      const int32_t d = T.wc_len[k];
-      const bool rsoc = T.wc_kind[k] == PK_RSOC;
-      const double* S = T.S ? T.S + st : nullptr;
-      const double r2 = 0.7071067811865476;
-      if (d <= 32) {
-        double z = (lane < d) ? op.z(st + lane) : 0.0;
+    const double r2 = 0.7071067811865476;
+    for (int64_t task = (int64_t)(b - T.ctaA) * kWarps + (threadIdx.x >> 5); task < T.task0[kCls];
+         task += wstride) {
+      int c = 0;
+#pragma unroll
+      for (int q = 1; q < kCls; ++q)
+        if (task >= T.task0[q]) c = q;
+      if (c < kCls - 1) {
+        // 32 / g blocks of at most g elements, one per lane group
+        const int g = 2 << c;
+        const int gl = lane & (g - 1);
+        const int64_t idx = T.cls_off[c] + (task - T.task0[c]) * (32 / g) + lane / g;
+        bool have = idx < T.cls_off[c + 1];
+        const int64_t k = have ? T.sched[idx] : 0;
+        const int64_t st = have ? T.wc_start[k] : 0;
+        if constexpr (MaskedOp<Op>) {
+          if (have && !op.live(st)) have = false;  // group-uniform: a block belongs to one instance
+        }
+        const int d = have ? T.wc_len[k] : 0;
+        const bool rsoc = have && T.wc_kind[k] == PK_RSOC;
+        const double* S = (T.S && have) ? T.S + st : nullptr;
+        const double z = (gl < d) ? op.z(st + gl) : 0.0;
         double v = z;
         double w = 1.0;
-        if (S && lane < d) {
-          if (rsoc) w = (lane >= 2) ? sqrt(S[0] * S[1]) / S[lane] : 1.0;
-          else w = (lane >= 1) ? S[0] / S[lane] : 1.0;
+        if (S && gl < d) {
+          if (rsoc) w = (gl >= 2) ? sqrt(S[0] * S[1]) / S[gl] : 1.0;
+          else w = (gl >= 1) ? S[0] / S[gl] : 1.0;
         }
-        bool weighted = __any_sync(kFull, w != 1.0);
-        if (rsoc) {
-          double p0 = __shfl_sync(kFull, v, 0), q0 = __shfl_sync(kFull, v, 1);
-          if (lane == 0) v = (p0 + q0) * r2;
-          if (lane == 1) v = (p0 - q0) * r2;
+        const bool weighted = grp_max(w != 1.0 ? 1.0 : 0.0, g) != 0.0;
+        {  // RSOC: rotate the first two elements to the SOC form (all lanes shuffle)
+          const double p0 = __shfl_sync(kFull, v, 0, g), q0 = __shfl_sync(kFull, v, 1, g);
+          if (rsoc && gl == 0) v = (p0 + q0) * r2;
+          if (rsoc && gl == 1) v = (p0 - q0) * r2;
         }
-        warp_soc_reg(v, w, d, weighted);
-        if (rsoc) {
-          double a0 = __shfl_sync(kFull, v, 0), b0 = __shfl_sync(kFull, v, 1);
-          if (lane == 0) v = (a0 + b0) * r2;
-          if (lane == 1) v = (a0 - b0) * r2;
+        group_soc_reg(v, w, d, weighted, g, (have && T.soc_ws) ? T.soc_ws + k : nullptr);
+        {
+          const double a0 = __shfl_sync(kFull, v, 0, g), b0 = __shfl_sync(kFull, v, 1, g);
+          if (rsoc && gl == 0) v = (a0 + b0) * r2;
+          if (rsoc && gl == 1) v = (a0 - b0) * r2;
         }
-        if (lane < d) op.fin(st + lane, z, v, acc);
+        if (gl < d) op.fin(st + gl, z, v, acc);
       } else {
+        // blocks of more than 32 elements: a warp each, values staged in op.out
+        const int64_t k = T.sched[T.cls_off[c] + (task - T.task0[c])];
+        const int64_t st = T.wc_start[k];
+        if constexpr (MaskedOp<Op>) {
+          if (!op.live(st)) continue;  // warp-uniform
+        }
+        const int32_t d = T.wc_len[k];
+        const bool rsoc = T.wc_kind[k] == PK_RSOC;
+        const double* S = T.S ? T.S + st : nullptr;
         double* p = op.out + st;
         for (int64_t i = lane; i < d; i += 32) p[i] = op.z(st + i);
         __syncwarp();
         bool weighted = false;
         if (S) {
-          double g = rsoc ? sqrt(S[0] * S[1]) : S[0];
+          double gw = rsoc ? sqrt(S[0] * S[1]) : S[0];
           bool any = false;
-          for (int64_t i = (rsoc ? 2 : 1) + lane; i < d; i += 32) any |= (g / S[i] != 1.0);
+          for (int64_t i = (rsoc ? 2 : 1) + lane; i < d; i += 32) any |= (gw / S[i] != 1.0);
           weighted = __any_sync(kFull, any);
         }
         if (rsoc) {
@@ -452,8 +488,8 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
             p[1] = (p0 - q0) * r2;
           }
           __syncwarp();
-          double g = S ? sqrt(S[0] * S[1]) : 1.0;
-          warp_soc_mem(p, d, [&](int64_t i) { return (i == 1 || !S) ? 1.0 : g / S[i]; }, weighted);
+          double gw = S ? sqrt(S[0] * S[1]) : 1.0;
+          warp_soc_mem(p, d, [&](int64_t i) { return (i == 1 || !S) ? 1.0 : gw / S[i]; }, weighted);
           __syncwarp();
           if (lane == 0) {
             double a0 = p[0], b0 = p[1];
@@ -471,7 +507,7 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
         __syncwarp();
       }
     }
-  } else {
+  } else if constexpr (EXP) {
     const int64_t tstride = (int64_t)T.ctaC * kThreads;
     const int64_t total = T.exp_count + T.dexp_count;
     for (int64_t k = (int64_t)(b - T.ctaA - T.ctaB) * kThreads + threadIdx.x; k < total; k += tstride) {
@@ -508,6 +544,15 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
     __syncthreads();
     if (last) control_block(op.st, op.ctrl_px, op.ctrl_nbx, partials, nblocks);
   }
+}
+
+// Launch update_project_kernel on table T, with the exp path only when T has exp cones.
+template <class Op>
+inline void launch_update_project(const Op& op, const ConeTable& T, double* partials, const int32_t* active,
+                                  cudaStream_t s) {
+  const int grid = T.ctaA + T.ctaB + T.ctaC;
+  if (T.exp_count + T.dexp_count > 0) update_project_kernel<Op, true><<<grid, kThreads, 0, s>>>(op, T, partials, active);
+  else update_project_kernel<Op, false><<<grid, kThreads, 0, s>>>(op, T, partials, active);
 }
 
 // ---------------------------------------------------------------------------

@@ -8,10 +8,12 @@
 // device-resident state, so the host only intervenes at the reference's
 // checkpoints (iter % check_terminate_freq, restart checks, artificial restarts).
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -324,18 +326,62 @@ static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// One stream-ordered memory pool per device, owned by the library: a solve's
+// workspace returns to it at the end and the next solve on that device reuses
+// it without driver allocations (cudaMalloc / cudaFree synchronise the device).
+// Up to kPoolKeep bytes stay cached across synchronisations.
+constexpr uint64_t kPoolKeep = 8ull << 30;
+
+static cudaMemPool_t library_pool() {
+  static std::mutex mu;
+  static std::vector<cudaMemPool_t> pools;
+  int dev = 0;
+  PDCS_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    PDCS_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = kPoolKeep;
+    PDCS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[dev] = pool;
+  }
+  return pools[dev];
+}
+
+// Device workspace of one solve, allocated in stream order on the solve's stream.
 struct Arena {
   std::vector<void*> ptrs;
+  cudaStream_t s = nullptr;
+  cudaMemPool_t pool = nullptr;
+  void bind(cudaStream_t stream) {
+    s = stream;
+    pool = library_pool();
+  }
   template <class T>
   T* alloc(size_t count) {
     void* p = nullptr;
-    PDCS_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    PDCS_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), pool, s));
     ptrs.push_back(p);
     return static_cast<T*>(p);
   }
-  ~Arena() {
-    for (void* p : ptrs) cudaFree(p);
+  void release() {
+    for (void* p : ptrs) cudaFreeAsync(p, s);
+    ptrs.clear();
   }
+  void drop(const void* p) {
+    for (size_t i = 0; i < ptrs.size(); ++i)
+      if (ptrs[i] == p) {
+        cudaFreeAsync(ptrs[i], s);
+        ptrs.erase(ptrs.begin() + i);
+        return;
+      }
+  }
+  ~Arena() { release(); }
 };
 
 struct Converge {
@@ -360,6 +406,7 @@ class Solver {
     if (graph_) cudaGraphDestroy(graph_);
     if (host_state_) cudaFreeHost(host_state_);
     if (host_red_) cudaFreeHost(host_red_);
+    A.release();  // back to the pool, in order on s_
     if (own_stream_) cudaStreamDestroy(s_);
   }
   int run(pdcs_result* res);
@@ -425,7 +472,10 @@ class Solver {
   int validate();
   void setup();
   void build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
-                  const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst);
+                  const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst, int lane_nnz);
+  int tune_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp, const int32_t* d_ci,
+                const double* d_v, CsrDev& D, const int32_t* row_inst, const double* xin, double* yout);
+  int lane_G_ = 4, lane_Gt_ = 4;  // SpMV schedules in use (nonzeros per lane)
   // instance of each row of G and of G' (batched solver; NULL: one instance)
   const int32_t* inst_of_y_ = nullptr;
   const int32_t* inst_of_x_ = nullptr;
@@ -457,7 +507,7 @@ class Solver {
   int grid_for(int64_t len) const { return (int)std::max<int64_t>(1, std::min<int64_t>((len + kThreads - 1) / kThreads, 148 * 8)); }
   template <class Op>
   void update_project(const Op& op, const ConeTable& T, double* partials) {
-    update_project_kernel<Op><<<T.ctaA + T.ctaB + T.ctaC, kThreads, 0, s_>>>(op, T, partials, nullptr);
+    launch_update_project(op, T, partials, nullptr, s_);
     kernels_++;
   }
   // reduce partials of the last kernel to host values
@@ -592,8 +642,11 @@ int Solver::validate() {
   return PDCS_OK;
 }
 
+// Rows binned by length for a schedule of lane_nnz nonzeros per lane: bin b < 6
+// takes rows of at most lane_nnz * 2^b nonzeros (g = 2^b lanes each), bin 6 the
+// longer rows (a CTA each).  Counting sort: rows keep their order inside a bin.
 void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
-                        const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst) {
+                        const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst, int lane_nnz) {
   D.m = rows;
   D.n = cols;
   D.nnz = rp[rows];
@@ -601,31 +654,24 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
   D.ci = d_ci;
   D.v = d_v;
   D.dbin = nullptr;
-  std::vector<std::vector<int32_t>> bins(kBins);
-  for (int64_t i = 0; i < rows; ++i) {
-    int64_t L = rp[i + 1] - rp[i];
-    int b;
-    if (L > 128) b = kBins - 1;  // CTA per row
-    else {
-      int g = 1;
-      b = 0;
-      while (g < 32 && (int64_t)g * 4 < L) {
-        g *= 2;
-        b++;
-      }
-    }
-    bins[b].push_back((int32_t)i);
-  }
-  std::vector<int4> desc;
-  desc.reserve(rows);
+  auto bin_of = [&](int64_t i) {
+    const int64_t L = rp[i + 1] - rp[i];
+    if (L > 32LL * lane_nnz) return kBins - 1;
+    int b = 0;
+    while (b < kBins - 2 && ((int64_t)lane_nnz << b) < L) ++b;
+    return b;
+  };
+  int64_t cnt[kBins] = {};
+  for (int64_t i = 0; i < rows; ++i) cnt[bin_of(i)]++;
   int64_t off = 0;
   int32_t cta = 0;
+  int64_t pos[kBins];
   for (int b = 0; b < kBins; ++b) {
     D.bin_off[b] = off;
     D.cta0[b] = cta;
-    int64_t R = (int64_t)bins[b].size();
+    pos[b] = off;
+    const int64_t R = cnt[b];
     off += R;
-    for (int32_t r : bins[b]) desc.push_back(make_int4(r, rp[r], rp[r + 1], row_inst ? row_inst[r] : 0));
     if (R == 0) continue;
     if (b < kBins - 1) {
       int64_t rows_per_cta = kThreads >> b;
@@ -636,6 +682,9 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
   }
   D.bin_off[kBins] = off;
   D.cta0[kBins] = std::max(cta, 1);
+  std::vector<int4> desc(rows);
+  for (int64_t i = 0; i < rows; ++i)
+    desc[pos[bin_of(i)]++] = make_int4((int32_t)i, rp[i], rp[i + 1], row_inst ? row_inst[i] : 0);
   int4* d_desc = A.alloc<int4>(std::max<size_t>(desc.size(), 1));
   if (!desc.empty())
     PDCS_CUDA(cudaMemcpyAsync(d_desc, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice, s_));
@@ -643,12 +692,83 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
   D.rows = d_desc;
 }
 
+// SpMV schedule autotuner: time each nonzeros-per-lane target on this matrix
+// (CUDA events, best of 3 after a warm-up) and keep the fastest, leaving the
+// default (4) only for a gain of 3% or more; a fixed target (spmv_lane_nnz > 0)
+// skips the search.  The choice is remembered per device and row structure
+// for the life of the process, so repeated solves of a matrix use the same
+// schedule (and give bit-identical results).  Returns the target used.
+int Solver::tune_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
+                      const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst, const double* xin,
+                      double* yout) {
+  if (O.spmv_lane_nnz > 0) {
+    build_bins(rp, rows, cols, d_rp, d_ci, d_v, D, row_inst, O.spmv_lane_nnz);
+    return O.spmv_lane_nnz;
+  }
+  static std::mutex mu;
+  static std::map<std::array<uint64_t, 4>, int> chosen;
+  int dev = 0;
+  PDCS_CUDA(cudaGetDevice(&dev));
+  uint64_t h = 1469598103934665603ull;
+  for (int64_t i = 0; i <= rows; ++i) {
+    h ^= (uint64_t)(uint32_t)rp[i];
+    h *= 1099511628211ull;
+  }
+  const std::array<uint64_t, 4> key{(uint64_t)dev, (uint64_t)rows, (uint64_t)cols, h};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = chosen.find(key);
+    if (it != chosen.end()) {
+      build_bins(rp, rows, cols, d_rp, d_ci, d_v, D, row_inst, it->second);
+      return it->second;
+    }
+  }
+  cudaEvent_t e0, e1;
+  PDCS_CUDA(cudaEventCreate(&e0));
+  PDCS_CUDA(cudaEventCreate(&e1));
+  int best = 4;
+  float best_ms = 1e30f;
+  CsrDev best_D{};
+  for (int lane : {4, 2, 8, 16}) {  // the default first: others must beat it by 3%
+    CsrDev C;
+    build_bins(rp, rows, cols, d_rp, d_ci, d_v, C, row_inst, lane);
+    spmv(C, xin, yout);
+    float t = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+      PDCS_CUDA(cudaEventRecord(e0, s_));
+      spmv(C, xin, yout);
+      PDCS_CUDA(cudaEventRecord(e1, s_));
+      PDCS_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      PDCS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      t = std::min(t, ms);
+    }
+    kernels_ -= 4;
+    if (lane != 4) t *= 1.03f;
+    if (t < best_ms) {
+      if (best_D.rows) A.drop(best_D.rows);
+      best_ms = t;
+      best = lane;
+      best_D = C;
+    } else {
+      A.drop(C.rows);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  D = best_D;
+  std::lock_guard<std::mutex> lock(mu);
+  chosen.emplace(key, best);
+  return best;
+}
+
 void Solver::size_table(ConeTable& T) {
   T.elem_total = 0;
   for (int s = 0; s < T.nseg; ++s) T.elem_total += T.seg_len[s];
   auto cap = [](int64_t v) { return (int32_t)std::min<int64_t>(v, 148 * 8); };
   T.ctaA = T.elem_total > 0 ? cap((T.elem_total + kThreads - 1) / kThreads) : 0;
-  T.ctaB = T.nwc > 0 ? cap((T.nwc + kWarps - 1) / kWarps) : 0;
+  const int64_t tasks = T.task0[kCls];
+  T.ctaB = tasks > 0 ? cap((tasks + kWarps - 1) / kWarps) : 0;
   int64_t ne = T.exp_count + T.dexp_count;
   T.ctaC = ne > 0 ? cap((ne + kThreads - 1) / kThreads) : 0;
   if (T.ctaA + T.ctaB + T.ctaC == 0) T.ctaA = 1;  // at least one CTA writes the partials
@@ -657,36 +777,55 @@ void Solver::size_table(ConeTable& T) {
 void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<int64_t>& rsoc_x,
                           const std::vector<int64_t>& socG, const std::vector<int64_t>& rsocG) {
   // warp-cone lists (shared by the iteration and KKT tables of each vector)
+  // warp-cone lists and their size-class schedule (lane groups of g = 2 << c lanes)
   auto upload_wc = [&](const std::vector<int64_t>& soc, const std::vector<int64_t>& rsoc, int64_t start0,
-                       int64_t*& d_start, int32_t*& d_len, int8_t*& d_kind) {
+                       ConeTable& T) {
     std::vector<int64_t> stv;
     std::vector<int32_t> lv;
     std::vector<int8_t> kv;
     int64_t s = start0;
     for (int64_t d : soc) { stv.push_back(s); lv.push_back((int32_t)d); kv.push_back(PK_SOC); s += d; }
     for (int64_t d : rsoc) { stv.push_back(s); lv.push_back((int32_t)d); kv.push_back(PK_RSOC); s += d; }
-    d_start = A.alloc<int64_t>(stv.size());
-    d_len = A.alloc<int32_t>(lv.size());
-    d_kind = A.alloc<int8_t>(kv.size());
+    std::vector<std::vector<int64_t>> cls(kCls);
+    for (size_t k = 0; k < lv.size(); ++k) {
+      int c = 0;
+      while (c < kCls - 1 && lv[k] > (2 << c)) ++c;
+      cls[c].push_back((int64_t)k);
+    }
+    std::vector<int64_t> sched;
+    int64_t task = 0;
+    for (int c = 0; c < kCls; ++c) {
+      T.cls_off[c] = (int64_t)sched.size();
+      T.task0[c] = task;
+      sched.insert(sched.end(), cls[c].begin(), cls[c].end());
+      const int64_t per = (c < kCls - 1) ? 32 / (2 << c) : 1;
+      task += ((int64_t)cls[c].size() + per - 1) / per;
+    }
+    T.cls_off[kCls] = (int64_t)sched.size();
+    T.task0[kCls] = task;
+    int64_t* d_start = A.alloc<int64_t>(stv.size());
+    int32_t* d_len = A.alloc<int32_t>(lv.size());
+    int8_t* d_kind = A.alloc<int8_t>(kv.size());
+    int64_t* d_sched = A.alloc<int64_t>(sched.size());
     if (!stv.empty()) {
       PDCS_CUDA(cudaMemcpyAsync(d_start, stv.data(), stv.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s_));
       PDCS_CUDA(cudaMemcpyAsync(d_len, lv.data(), lv.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s_));
       PDCS_CUDA(cudaMemcpyAsync(d_kind, kv.data(), kv.size() * sizeof(int8_t), cudaMemcpyHostToDevice, s_));
+      PDCS_CUDA(cudaMemcpyAsync(d_sched, sched.data(), sched.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s_));
       PDCS_CUDA(cudaStreamSynchronize(s_));
     }
+    T.nwc = (int64_t)stv.size();
+    T.wc_start = d_start;
+    T.wc_len = d_len;
+    T.wc_kind = d_kind;
+    T.sched = d_sched;
     return s;
   };
-  int64_t *xs = nullptr, *ys = nullptr;
-  int32_t *xlen = nullptr, *ylen = nullptr;
-  int8_t *xk = nullptr, *yk = nullptr;
-  int64_t xe = upload_wc(soc_x, rsoc_x, nb_, xs, xlen, xk);
-  int64_t ye = upload_wc(socG, rsocG, P.mGzero + P.mGnonnegative, ys, ylen, yk);
   ConeTable base_x{};
+  ConeTable base_y{};
+  int64_t xe = upload_wc(soc_x, rsoc_x, nb_, base_x);
+  int64_t ye = upload_wc(socG, rsocG, P.mGzero + P.mGnonnegative, base_y);
   base_x.len = n_;
-  base_x.nwc = (int64_t)(soc_x.size() + rsoc_x.size());
-  base_x.wc_start = xs;
-  base_x.wc_len = xlen;
-  base_x.wc_kind = xk;
   base_x.exp_base = xe;
   base_x.exp_count = P.exp_x;
   base_x.dexp_base = xe + 3 * P.exp_x;
@@ -709,12 +848,7 @@ void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<i
   SLK.exp_kind = PK_DEXP;  // code 28
   SLK.dexp_kind = PK_EXP;  // code 26
   SLK.S = nullptr;
-  ConeTable base_y{};
   base_y.len = m_;
-  base_y.nwc = (int64_t)(socG.size() + rsocG.size());
-  base_y.wc_start = ys;
-  base_y.wc_len = ylen;
-  base_y.wc_kind = yk;
   base_y.exp_base = ye;
   base_y.exp_count = P.expG;
   base_y.dexp_base = ye + 3 * P.expG;
@@ -750,6 +884,11 @@ void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<i
   YI.rho_ws = A.alloc<double>(nye);
   PDCS_CUDA(cudaMemsetAsync(XI.rho_ws, 0xff, sizeof(double) * std::max<int64_t>(nxe, 1), s_));
   PDCS_CUDA(cudaMemsetAsync(YI.rho_ws, 0xff, sizeof(double) * std::max<int64_t>(nye, 1), s_));
+  // per-block warm starts of the weighted-SOC root (the unscaled tables use the closed form)
+  XI.soc_ws = A.alloc<double>(std::max<int64_t>(XI.nwc, 1));
+  YI.soc_ws = A.alloc<double>(std::max<int64_t>(YI.nwc, 1));
+  PDCS_CUDA(cudaMemsetAsync(XI.soc_ws, 0xff, sizeof(double) * std::max<int64_t>(XI.nwc, 1), s_));
+  PDCS_CUDA(cudaMemsetAsync(YI.soc_ws, 0xff, sizeof(double) * std::max<int64_t>(YI.nwc, 1), s_));
   size_table(XI);
   size_table(SLK);
   size_table(YI);
@@ -767,6 +906,7 @@ void Solver::setup() {
     PDCS_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
     own_stream_ = true;
   }
+  A.bind(s_);
   PDCS_CUDA(cudaMallocHost(&host_state_, sizeof(PdhgState)));
   PDCS_CUDA(cudaMallocHost(&host_red_, 64 * sizeof(double)));
   part_r = A.alloc<double>((size_t)148 * 8 * 8);
@@ -891,8 +1031,6 @@ void Solver::setup() {
   PDCS_CUDA(cudaMemcpyAsync(rp_h.data(), g_rp, sizeof(int32_t) * (m_ + 1), cudaMemcpyDeviceToHost, s_));
   PDCS_CUDA(cudaMemcpyAsync(trp_h.data(), t_rp, sizeof(int32_t) * (n_ + 1), cudaMemcpyDeviceToHost, s_));
   PDCS_CUDA(cudaStreamSynchronize(s_));
-  build_bins(rp_h, m_, n_, g_rp, g_ci, g_v, G_, inst_of_y_);
-  build_bins(trp_h, n_, m_, t_rp, t_ci, t_v, Gt_, inst_of_x_);
   // ---- iterates and work vectors ----
   auto vecn = [&]() { return A.alloc<double>(n_); };
   auto vecm = [&]() { return A.alloc<double>(m_); };
@@ -913,6 +1051,9 @@ void Solver::setup() {
   }
   copy(xl, x, n_); copy(xm, x, n_); copy(xbest, x, n_);
   copy(yl, y, m_); copy(ym, y, m_); copy(ybest, y, m_);
+  // ---- SpMV schedules: autotuned per matrix unless fixed by the options ----
+  lane_G_ = tune_bins(rp_h, m_, n_, g_rp, g_ci, g_v, G_, inst_of_y_, x, tm[0]);
+  lane_Gt_ = tune_bins(trp_h, n_, m_, t_rp, t_ci, t_v, Gt_, inst_of_x_, y, tn[0]);
   // cone tables
   std::vector<int64_t> soc_x(P.soc_x, P.soc_x + P.n_soc_x), rsoc_x(P.rsoc_x, P.rsoc_x + P.n_rsoc_x);
   std::vector<int64_t> socG(P.socG, P.socG + P.n_socG), rsocG(P.rsocG, P.rsocG + P.n_rsocG);
@@ -999,22 +1140,22 @@ void Solver::capture_graph() {
     spmv_binned_kernel<1, false, float><<<Gt32_.cta0[kBins], kThreads, 0, s_>>>(Gt32_, dyl32_, nullptr, aty32_,
                                                                                nullptr, act, &st_dev->do_reflect);
     OpPrimalStep32 op1{xa_, dxl32_, qa_, aty32_, dx32_, x, st_dev, 0.0};
-    update_project_kernel<OpPrimalStep32><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, act);
+    launch_update_project(op1, XI, part_x, act, s_);
     spmv_binned_kernel<2, false, float><<<G32_.cta0[kBins], kThreads, 0, s_>>>(G32_, dx32_, dxl32_, gx32_, gxl32_,
                                                                              act);
     OpDualStep32 op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, st_dev, 0.0, part_x, XI.ctaA + XI.ctaB + XI.ctaC};
-    update_project_kernel<OpDualStep32><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, act);
+    launch_update_project(op2, YI, part_y, act, s_);
     reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, dx32_, dxl32_, dxm_, n_, dy32_, dyl32_, dym_, m_);
   }
   for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
     spmv_binned_kernel<1><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, yl, nullptr, aty, nullptr, act,
                                                                 &st_dev->do_reflect);
     OpPrimalStep op1{xl, aty, c_s, x, st_dev, 0.0};
-    update_project_kernel<OpPrimalStep><<<XI.ctaA + XI.ctaB + XI.ctaC, kThreads, 0, s_>>>(op1, XI, part_x, act);
+    launch_update_project(op1, XI, part_x, act, s_);
     spmv_binned_kernel<2><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, x, xl, gx, gxl, act);
     // the dual step's last CTA runs the attempt's control step
     OpDualStep op2{yl, gx, gxl, h_s, y, st_dev, 0.0, part_x, XI.ctaA + XI.ctaB + XI.ctaC};
-    update_project_kernel<OpDualStep><<<YI.ctaA + YI.ctaB + YI.ctaC, kThreads, 0, s_>>>(op2, YI, part_y, act);
+    launch_update_project(op2, YI, part_y, act, s_);
     reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, x, xl, xm, n_, y, yl, ym, m_);
   }
   PDCS_CUDA(cudaStreamEndCapture(s_, &graph_));
@@ -1688,6 +1829,8 @@ int Solver::run(pdcs_result* res) {
   res->time_exit_checks = t_exit_;
   res->time_restarts = t_restart_;
   res->restart_probes = probes_;
+  res->spmv_lane_nnz_G = lane_G_;
+  res->spmv_lane_nnz_Gt = lane_Gt_;
   return PDCS_OK;
 }
 

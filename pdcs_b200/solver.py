@@ -52,6 +52,7 @@ class Info:
     time_exit_checks: float = 0.0
     time_restarts: float = 0.0
     restart_probes: int = 0
+    spmv_lane_nnz: tuple = (0, 0)
 
 
 class Solution:
@@ -170,11 +171,12 @@ def _options_struct(L, hold: _Holder, *, n=0, m=0, rescaling_method: str = "ruiz
                     method: str = "average", logfile_name: Optional[str] = None, use_kkt_restart: bool = False,
                     kkt_restart_freq: int = 2000, use_duality_gap_restart: bool = True,
                     duality_gap_restart_freq: int = 2000, attempt_limit: int = 0, attempts_per_graph: int = 32,
-                    stream=None, force_resolving: bool = False, precision="fp64"):
+                    stream=None, force_resolving: bool = False, precision="fp64", spmv_lane_nnz: int = 0):
     """Fill a PdcsOptions from the reference's keyword arguments (rpdhg_alg_gpu_gen.jl:1219-1268).
 
     precision: "fp64" (the reference's arithmetic) or "fp32" (FP32 matrices and iterate deltas
-    between FP64 anchors; FP64 projections, averages and termination checks)."""
+    between FP64 anchors; FP64 projections, averages and termination checks).
+    spmv_lane_nnz: 0 autotunes the SpMV schedule per matrix; 1..16 fixes it (nonzeros per lane)."""
     if method not in ("average", "halpern"):
         raise ValueError("method only available for :average and :halpern")
     if method == "halpern":
@@ -215,6 +217,9 @@ def _options_struct(L, hold: _Holder, *, n=0, m=0, rescaling_method: str = "ruiz
     if prec is None:
         raise ValueError("precision must be 'fp64' or 'fp32'")
     O.precision = prec
+    if spmv_lane_nnz not in (0, 1, 2, 4, 8, 16):
+        raise ValueError("spmv_lane_nnz must be 0 (autotune) or a power of two up to 16")
+    O.spmv_lane_nnz = spmv_lane_nnz
     return O
 
 
@@ -230,7 +235,7 @@ def _info(R) -> Info:
                 returned_sequence=R.returned_sequence, kernel_launches=R.kernel_launches,
                 graph_launches=R.graph_launches, time_iterations=R.time_iterations,
                 time_exit_checks=R.time_exit_checks, time_restarts=R.time_restarts,
-                restart_probes=R.restart_probes)
+                restart_probes=R.restart_probes, spmv_lane_nnz=(R.spmv_lane_nnz_G, R.spmv_lane_nnz_Gt))
 
 
 def rpdhg_gpu_solve(*, device_output: bool = False, **kw) -> Solution:

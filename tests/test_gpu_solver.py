@@ -104,3 +104,19 @@ def test_resolving_fallback_matches_oracle(cuda, name):
     o = B.solve(p, threads=2, force_resolving=1, time_limit=120)
     assert g.info.exit_status == "optimal" and o["exit_code"] == 0
     assert abs(g.info.pObj - o["primal_objective"]) <= 2e-6 * (1 + abs(o["primal_objective"]))
+
+
+def test_spmv_schedules_agree(cuda):
+    """Every SpMV schedule (nonzeros per lane: 1 lane per row up to a CTA per row) gives the
+    same iterates to rounding; the autotuned default reports the schedule it picked."""
+    p = problems.logreg_exp_c1(samples=400, features=40, density=0.2)
+    ref = solver.solve_problem(p, attempt_limit=20, spmv_lane_nnz=4)
+    assert ref.info.spmv_lane_nnz == (4, 4)
+    for lane in (0, 1, 2, 8, 16):
+        g = solver.solve_problem(p, attempt_limit=20, spmv_lane_nnz=lane)
+        if lane:
+            assert g.info.spmv_lane_nnz == (lane, lane)
+        else:
+            assert all(v in (2, 4, 8, 16) for v in g.info.spmv_lane_nnz)
+        scale = max(1.0, np.abs(ref.primal).max())
+        assert np.abs(g.primal - ref.primal).max() <= 1e-9 * scale, lane
