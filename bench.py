@@ -1,19 +1,28 @@
 #!/usr/bin/env python
-"""Benchmark: time-to-1e-6 KKT and PDHG iterations/s on the exponential-cone
-logistic-regression program (20000 samples x 500 features, 5% density, FP64).
+"""Benchmark: time-to-1e-6 KKT throughput of the batched FP32-bulk solver vs
+plain FP64 GPU PDHG, on 4096 independent uneven SOCPs (n log-uniform in
+[50, 5000], m = 0.8 n, 2% density, SOC blocks of dims 3..20, each feasible and
+bounded by construction; seeded synthetic data).
 
-A step is one complete solve from a cold start to the reference's 1e-6
-relative criteria.  `value` is PDHG iterations per second over the timed
-steps with the problem already resident in HBM; `e2e` is the same metric
-through the public Python API from host numpy buffers (host->device copy of
-the problem and device->host copy of the solution inside the timed region).
+A step is one complete cold-start solve of the whole batch to the
+reference's 1e-6 relative criteria (every instance with its own step sizes,
+restarts and termination).  `value` is instances solved per second with the
+batch prepared (merged, uploaded, preconditioned) and resident in HBM when
+the timed region starts; `e2e` is the same metric through the public Python
+API from host numpy buffers (merge, host->device copies, preprocessing,
+solve and device->host copies of every solution inside the timed region).
+The plain FP64 GPU PDHG (one instance at a time, the reference's
+arithmetic) is timed on a seeded sample of the same instances, and the
+single-instance exponential-cone workload (20000 x 500 logistic regression)
+is reported beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-N > 1 runs N independent replicas (one process per GPU, weak scaling); the
-path has no collective.  `--impl reference` times the CPU restatement of the
-reference (the reference itself is Julia + CUDA.jl and cannot run here) on
-the host cores, on bounded samples of the same workload.
+N > 1 runs one process per GPU, each solving its own 4096-instance batch
+(weak scaling, no collective on the solve path).  `--impl reference` times
+the CPU restatement of the reference's algorithm (the reference itself is
+Julia + CUDA.jl and cannot run here) over all host cores, on bounded samples
+of the same instances.
 """
 import argparse
 import json
@@ -22,13 +31,13 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "time-to-1e-6 KKT & iter/s: batched mixed-prec vs plain FP64 PDHG, 1 B200"
+SEED = 20261206
 
 
 def parse():
@@ -37,30 +46,36 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--samples", type=int, default=20000)
-    ap.add_argument("--features", type=int, default=500)
-    ap.add_argument("--cpu-attempts", type=int, default=300,
-                    help="PDHG attempts per bounded CPU sample")
+    ap.add_argument("--count", type=int, default=4096, help="instances per batch")
+    ap.add_argument("--plain-sample", type=int, default=24, help="instances timed with the plain FP64 solver")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-single", action="store_true", help="skip the single-instance exp-cone section")
     return ap.parse_args()
 
 
-def workload(args):
+def workload(args, rank=0):
     from pdcs_b200 import problems
-    p = problems.logreg_exp_c1(samples=args.samples, features=args.features)
-    cfg = {"workload": f"l1-logistic regression in exp-cone form, {args.samples}x{args.features} "
-                       f"@5% (n={p.n}, m={p.m}, nnz={p.nnz}, {p.expG} exp cones)",
-           "n": p.n, "m": p.m, "nnz": p.nnz, "seed": p.seed, "tolerance": 1e-6,
-           "l2": "256 MiB buffer written between timed steps (problem fits in L2 within a solve)"}
-    return p, cfg
+    seed = SEED + 100003 * rank
+    batch = problems.batch_socp_c3(count=args.count, seed=seed)
+    n = sum(p.n for p in batch)
+    m = sum(p.m for p in batch)
+    nnz = sum(p.nnz for p in batch)
+    nb = sum(p.nb for p in batch)
+    cfg = {"workload": f"{args.count} uneven SOCPs: n log-uniform [50, 5000], m = 0.8 n, 2% density, "
+                       "SOC dims 3..20, feasible and bounded by construction",
+           "instances": args.count, "sum_n": n, "sum_m": m, "sum_nnz": nnz, "seed": seed, "tolerance": 1e-6,
+           "precision": "FP32 matrices and iterate deltas, FP64 anchors / projections / averages / checks",
+           "l2": f"inputs larger than L2 (G and G' {2 * nnz * 8 / 1e9:.1f} GB in FP32)"}
+    return batch, cfg, (n, m, nnz, nb)
 
 
-def bytes_per_iter(p, w=8):
-    """Algorithmic HBM bytes of one PDHG iteration: G and G' (values + int32
-    column indices) once each, both row pointers, the primal/dual vector
-    streams, the box bounds and the averaged iterates."""
-    n, m, nnz, n1 = p.n, p.m, p.nnz, p.nb
+def bytes_per_attempt(n, m, nnz, n1, w):
+    """Algorithmic HBM bytes of one PDHG attempt of the whole batch: G and G'
+    (values + int32 column indices) once each, both row pointers, the primal /
+    dual vector streams, the box bounds and the averaged iterates, with w-byte
+    values."""
     return 2 * nnz * (w + 4) + 4 * (m + 1) + 4 * (n + 1) + w * (4 * n + 2 * n1 + 4 * m) + w * 2 * (n + m)
 
 
@@ -113,195 +128,233 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(p, attempts):
-    """The oracle (CPU restatement) on all host cores, bounded sample."""
+# ---------------------------------------------------------------------------
+# CPU: the oracle (C++ restatement of the reference's algorithm), one instance
+# per worker process over all host cores (spawned: no GPU state is inherited)
+# ---------------------------------------------------------------------------
+def _oracle_solve_one(p):
     from oracle import binding as B
+    t = time.perf_counter()
+    r = B.solve(p, threads=1)
+    return r["iter"], r["exit_code"], time.perf_counter() - t
+
+
+def cpu_batch_rate(batch, seconds, rng_seed=7):
+    """Instances/s of the oracle over all host cores on a seeded sample of the batch,
+    sized so the run takes about `seconds`."""
+    import multiprocessing as mp
+    import numpy as np
     cores = os.cpu_count() or 1
-    r = B.solve(p, threads=cores, attempt_limit=attempts)
-    secs = r["solve_seconds"]
-    return {"value": r["iter"] / secs, "unit": "iter/s", "cores": cores, "kind": "port",
-            "sample": f"first {r['iter']} PDHG attempts of one solve of the same instance "
-                      f"({secs:.1f} s of CPU time, setup excluded)"}
+    order = np.random.default_rng(rng_seed).permutation(len(batch))
+    ctx = mp.get_context("spawn")
+    done, iters, t0 = 0, 0, time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        pos = 0
+        while time.perf_counter() - t0 < seconds and pos < len(order):
+            chunk = [batch[i] for i in order[pos:pos + cores]]
+            pos += len(chunk)
+            for it, code, _ in pool.map(_oracle_solve_one, chunk):
+                done += 1
+                iters += it
+    wall = time.perf_counter() - t0
+    return {"value": done / wall, "unit": "instances/s", "cores": cores, "kind": "port",
+            "iter_per_s": iters / wall,
+            "sample": f"{done} seeded instances of the same batch solved to 1e-6 by the oracle "
+                      f"(FP64, one instance per core) in {wall:.1f} s"}
 
 
 def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
+    from pdcs_b200 import replicas
+    rank, world, _ = replicas.env()
     if rank != 0:
         return 0
-    p, cfg = workload(args)
-    from oracle import binding as B
-    cores = os.cpu_count() or 1
-    for _ in range(max(0, min(args.warmup, 1))):
-        B.solve(p, threads=cores, attempt_limit=20)
-    iters, secs = 0, 0.0
+    batch, cfg, _ = workload(args)
+    for _ in range(min(args.warmup, 1)):
+        _oracle_solve_one(batch[0])
+    vals, its, secs = [], 0.0, 0.0
     for _ in range(args.steps):
-        r = B.solve(p, threads=cores, attempt_limit=args.cpu_attempts)
-        iters += r["iter"]
-        secs += r["solve_seconds"]
-    v = iters / secs
-    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "iter/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        r = cpu_batch_rate(batch, args.cpu_seconds / max(1, args.steps) * 2)
+        vals.append(r["value"])
+        its += r["iter_per_s"]
+        secs += 1.0 / r["value"]
+    v = statistics.mean(vals)
+    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "instances/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.count / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)", "config": cfg,
-            "cpu_baseline": {"value": v, "unit": "iter/s", "cores": cores, "kind": "port",
-                             "sample": f"each step: first {args.cpu_attempts} PDHG attempts of a solve "
-                                       "(the reference's Julia/CUDA.jl code cannot run here; this is the "
-                                       "C++ restatement of its algorithm)"},
-            "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic (seeded)", "config": cfg, "iter_per_s": its / args.steps,
+            "cpu_baseline": {"value": v, "unit": "instances/s", "cores": r["cores"], "kind": "port",
+                             "sample": "each step: " + r["sample"] + " (the reference's Julia/CUDA.jl code "
+                                       "cannot run here; this is the C++ restatement of its algorithm)"},
+            "e2e": {"value": v, "unit": "instances/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def device_problem(p, dev):
+# ---------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------
+def timed(stream, fn):
+    import torch
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    out = fn()
+    e.record(stream)
+    e.synchronize()
+    return out, s.elapsed_time(e) * 1e-3
+
+
+def single_instance_section(dev, stream):
+    """The exponential-cone program (20000 x 500 l1-logistic regression), plain FP64, one GPU."""
     import numpy as np
     import torch
+    from pdcs_b200 import problems, solver
+    p = problems.logreg_exp_c1()
     G = p.G.tocsr()
     t = lambda a, dt=torch.float64: torch.as_tensor(np.asarray(a), dtype=dt, device=dev)
     kw = p.kwargs()
     kw.update(c=t(p.c), h=t(p.h), bl=t(p.bl), bu=t(p.bu),
               G=(t(G.indptr, torch.int32), t(G.indices, torch.int32), t(G.data)))
-    return kw
-
-
-def timed_solve(kw, stream, **extra):
-    import torch
-    from pdcs_b200 import solver
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record(stream)
-    sol = solver.rpdhg_gpu_solve(**kw, stream=stream.cuda_stream, **extra)
-    e.record(stream)
-    e.synchronize()
-    return sol, s.elapsed_time(e) * 1e-3
+    for _ in range(2):
+        timed(stream, lambda: solver.rpdhg_gpu_solve(**kw, stream=stream.cuda_stream))
+    ts = []
+    for _ in range(3):
+        sol, dt = timed(stream, lambda: solver.rpdhg_gpu_solve(**kw, stream=stream.cuda_stream))
+        ts.append(dt)
+    i = sol.info
+    return {"workload": f"l1-logistic regression in exp-cone form, 20000x500 @5% (n={p.n}, m={p.m}, "
+                       f"nnz={p.nnz}, {p.expG} exp cones), plain FP64",
+            "time_to_1e-6_ms": 1e3 * statistics.median(ts), "iterations": i.iter,
+            "iter_per_s": i.iter / statistics.median(ts), "setup_ms": 1e3 * i.setup_time,
+            "exit_status": i.exit_status, "spmv_lane_nnz": list(i.spmv_lane_nnz)}
 
 
 def run_ours(args):
     import numpy as np
     import torch
-    import torch.distributed as dist
+    from pdcs_b200 import replicas, solver
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
+    rank, world, local = replicas.env()
+    replicas.init(world)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
-    p, cfg = workload(args)
-    kw_dev = device_problem(p, dev)
+    stream = torch.cuda.Stream(dev)
+    batch, cfg, (n, m, nnz, nb) = workload(args, rank)
+    units = len(batch)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-
+    # ---- batched FP32-bulk, prepared once, resident in HBM ----
+    t0 = time.perf_counter()
+    h = solver.BatchHandle(batch, precision="fp32", stream=stream.cuda_stream)
+    prepare_s = time.perf_counter() - t0
     for _ in range(args.warmup):
-        sol, _ = timed_solve(kw_dev, stream)
-    assert sol.info.exit_status == "optimal", sol
-
-    # ---- device-resident timed region ----
-    total_t, total_it, launches, sols = 0.0, 0, 0, []
-    barrier()
+        sols, _ = timed(stream, h.solve)
+    replicas.barrier(world)
+    torch.cuda.synchronize()
+    total_t, launches, iters, statuses = 0.0, 0, 0, {}
     with Clocks(local) as clk:
         for _ in range(args.steps):
-            flush.zero_()
-            sol, t = timed_solve(kw_dev, stream)
-            total_t += t
-            total_it += sol.info.iter
-            launches += sol.info.kernel_launches
-            sols.append(sol)
-    barrier()
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            (sols, info), dt = timed(stream, h.solve)
+            total_t += dt
+            launches += info.kernel_launches
+            iters += sum(s.info.iter for s in sols)
+            for s in sols:
+                statuses[s.info.exit_status] = statuses.get(s.info.exit_status, 0) + 1
+    torch.cuda.synchronize()
+    replicas.barrier(world)
     clocks = clk.summary()
-    t_max = total_t
-    it_sum = total_it
-    if world > 1:
-        tt = torch.tensor([total_t], dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt[0])
-        ii = torch.tensor([float(total_it)], dtype=torch.float64)
-        dist.all_reduce(ii, op=dist.ReduceOp.SUM)
-        it_sum = int(ii[0])
-    value = it_sum / t_max
-    last = sols[-1].info
+    t_max = replicas.max_over_ranks(total_t, world)
+    done = replicas.sum_over_ranks(units * args.steps, world)
+    value = done / t_max
+    it_rate = replicas.sum_over_ranks(iters, world) / t_max
+    iters_per_inst = [s.info.iter for s in sols]
 
-    # ---- per-attempt time from two bounded runs (no checkpoints below 2000 attempts) ----
-    a1, a2 = 200, 1800
-    _, t1 = timed_solve(kw_dev, stream, attempt_limit=a1)
-    _, t2 = timed_solve(kw_dev, stream, attempt_limit=a2)
-    t_att = (t2 - t1) / (a2 - a1)
-    B_it = bytes_per_iter(p)
+    # ---- per-attempt time with every instance iterating (no checkpoint below 2000 attempts) ----
+    (_, _), t1 = timed(stream, lambda: h.solve(attempt_limit=64))
+    (_, _), t2 = timed(stream, lambda: h.solve(attempt_limit=320))
+    t_att = (t2 - t1) / 256
+    h.close()
+    B_att = bytes_per_attempt(n, m, nnz, nb, 4)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = B_it / t_att / 1e9
+    achieved = B_att / t_att / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic_logreg_c1.json")
+    tpath = os.path.join(ROOT, "profiles", "traffic_batch_c3.json")
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get("dram_bytes_per_attempt")
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic,
-                "kernel": "one PDHG attempt (G'y SpMV, primal update+projection, Gx/Gx_lag SpMV, "
-                          "dual update+exp-cone projection, control, reflection)",
-                "algorithmic_bytes_per_attempt": B_it, "attempt_ms": t_att * 1e3,
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic,
+                "kernel": "one batched FP32-bulk PDHG attempt of all 4096 instances (G'y and Gx/Gx_lag SpMVs, "
+                          "primal/dual update + projections, per-instance control, reflection)",
+                "algorithmic_bytes_per_attempt": B_att, "attempt_ms": t_att * 1e3,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"}
+
+    # ---- the same batch, batched FP64 (one timed solve) ----
+    h64 = solver.BatchHandle(batch, precision="fp64", stream=stream.cuda_stream)
+    timed(stream, lambda: h64.solve(attempt_limit=64))
+    (s64, _), t64 = timed(stream, h64.solve)
+    h64.close()
+
+    # ---- plain FP64 GPU PDHG, one instance at a time, on a seeded sample ----
+    idx = np.random.default_rng(5).choice(units, size=min(args.plain_sample, units), replace=False)
+    timed(stream, lambda: solver.solve_problem(batch[int(idx[0])], stream=stream.cuda_stream))
+    plain_t, plain_main, plain_it = 0.0, 0.0, 0
+    for i in idx:
+        s, dt = timed(stream, lambda: solver.solve_problem(batch[int(i)], stream=stream.cuda_stream))
+        plain_t += dt
+        plain_main += s.info.time
+        plain_it += s.info.iter
+    plain = {"instances_per_s": len(idx) / plain_t, "iter_per_s": plain_it / plain_t,
+             "main_loop_instances_per_s": len(idx) / plain_main,
+             "sample": f"{len(idx)} seeded instances of the batch, each a full pdcs_solve (FP64, "
+                       "upload + preprocessing + solve)"}
 
     # ---- end to end through the public API from host buffers ----
     e2e = None
     if not args.no_e2e:
-        from pdcs_b200 import solver
-        kw_host = p.kwargs()
-        G = p.G.tocsr()
-        h2d = G.indptr.size * 4 + G.indices.size * 4 + G.data.nbytes + p.c.nbytes + p.h.nbytes + \
-            p.bl.nbytes + p.bu.nbytes
-        d2h = 8 * (p.n + p.m)
-        et, eit = 0.0, 0
-        barrier()
+        h2d = sum(p.G.indptr.size * 4 + p.G.indices.size * 4 + p.G.data.nbytes + p.c.nbytes + p.h.nbytes +
+                  p.bl.nbytes + p.bu.nbytes for p in batch)
+        d2h = 8 * (n + m)
+        et = 0.0
+        replicas.barrier(world)
         for _ in range(args.steps):
-            flush.zero_()
             torch.cuda.synchronize()
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            sol_h = solver.rpdhg_gpu_solve(**kw_host, stream=stream.cuda_stream)
-            e.record(stream)
-            e.synchronize()
-            et += s.elapsed_time(e) * 1e-3
-            eit += sol_h.info.iter
-        barrier()
-        if world > 1:
-            tt = torch.tensor([et], dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            et = float(tt[0])
-            ii = torch.tensor([float(eit)], dtype=torch.float64)
-            dist.all_reduce(ii, op=dist.ReduceOp.SUM)
-            eit = int(ii[0])
-        e2e = {"value": eit / et, "unit": "iter/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "ms_per_step": 1e3 * et / args.steps, "iterations_per_solve": sol_h.info.iter}
+            t = time.perf_counter()
+            sols_h, _ = solver.rpdhg_gpu_solve_batch(batch, precision="fp32", stream=stream.cuda_stream)
+            torch.cuda.synchronize()
+            et += time.perf_counter() - t
+        replicas.barrier(world)
+        et = replicas.max_over_ranks(et, world)
+        e2e = {"value": replicas.sum_over_ranks(units * args.steps, world) / et, "unit": "instances/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": 1e3 * et / args.steps,
+               "optimal": sum(1 for s in sols_h if s.info.exit_status == "optimal")}
 
+    single = None if args.no_single or rank != 0 else single_instance_section(dev, stream)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(p, args.cpu_attempts)
+        cpu = cpu_batch_rate(batch, args.cpu_seconds)
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+        line = {"metric": METRIC, "value": value, "unit": "instances/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-                "config": {**cfg, "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
-                "time_to_1e-6_ms": 1e3 * t_max / args.steps,
-                "iterations_per_solve": last.iter, "restarts": last.restart_used,
-                "kkt": {"l_inf_rel_primal_res": last.l_inf_rel_primal_res,
-                        "l_inf_rel_dual_res": last.l_inf_rel_dual_res, "rel_gap": last.rel_gap},
-                "setup_ms": last.setup_time * 1e3,
-                "breakdown_ms": {"iterations": last.time_iterations * 1e3, "exit_checks": last.time_exit_checks * 1e3,
-                                 "restarts": last.time_restarts * 1e3, "restart_probes": last.restart_probes},
-                "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
-                "roofline": roofline, "cpu_baseline": cpu}
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+                "config": {**cfg, "parallelism": f"{world} GPUs, one batch each" if world > 1 else "single GPU"},
+                "time_to_1e-6_ms": 1e3 * t_max / args.steps, "iter_per_s": it_rate,
+                "statuses": statuses, "iterations_max": max(iters_per_inst),
+                "iterations_mean": float(np.mean(iters_per_inst)), "prepare_s": prepare_s,
+                "batched_fp64": {"time_to_1e-6_ms": 1e3 * t64, "instances_per_s": units / t64,
+                                 "optimal": sum(1 for s in s64 if s.info.exit_status == "optimal")},
+                "plain_fp64": plain, "speedup_vs_plain_fp64": value / plain["instances_per_s"] / world,
+                "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
+                "cpu_baseline": cpu, "single_instance": single}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finalize(world)
     return 0
 
 
