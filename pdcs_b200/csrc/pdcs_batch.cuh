@@ -261,6 +261,11 @@ class BatchSolver : public Solver {
   std::vector<int64_t> xrun_start_, xrun_len_, yrun_start_, yrun_len_;  // K * kMaxRuns
   std::vector<int64_t> xloc_, yloc_;                                    // K * kMaxRuns local starts
   std::vector<int32_t> h_ix_, h_iy_;
+  // per instance and side (0 = x, 1 = y): its warp cones [soc_first, soc_end) and
+  // [rsoc_first, rsoc_end) in the side's cone list, its exp cone ordinals
+  // [exp_first, exp_end) and dual-exp ordinals [dexp_first, dexp_end)
+  std::vector<std::array<int64_t, 8>> cones_[2];
+  std::vector<int8_t> cone_cls_[2];  // size class of every warp cone
   // device
   int32_t *ix_ = nullptr, *iy_ = nullptr;
   RunTable rx_{}, ry_{};
@@ -299,6 +304,22 @@ class BatchSolver : public Solver {
   int validate_batch();
   void merge();
   void setup_batch();
+  // active work lists of the iteration graph (rebuilt when the iterating set changes)
+  struct ActDev {
+    int2* chunk = nullptr;
+    int64_t* meta = nullptr;
+    int64_t* sched = nullptr;
+    int32_t* exp = nullptr;
+  } act_[2];
+  int4* rchunk_ = nullptr;
+  int64_t* n_rchunk_ = nullptr;
+  int32_t* act_inst_ = nullptr;
+  int64_t* n_act_ = nullptr;
+  ConeTable XIg_{}, YIg_{};  // XI / YI reading the active lists
+  std::vector<uint8_t> act_set_;  // iterating set the lists describe
+  size_t act_bytes_ = 0;          // largest upload of the lists
+  void setup_act_lists();
+  void build_act_lists(const std::vector<Inst*>& its);
   void capture_batch_graph();
   template <class T>
   T* stage(size_t count);
@@ -491,15 +512,53 @@ void BatchSolver::merge() {
       }
     }
   });
+  for (int w = 0; w < 2; ++w) cones_[w].assign(K, {});
   for (int64_t k = 0; k < K; ++k) {
     const pdcs_problem& q = probs_[k];
+    cones_[0][k][0] = (int64_t)h_socx_.size();
+    cones_[1][k][0] = (int64_t)h_socG_.size();
     h_socx_.insert(h_socx_.end(), q.soc_x, q.soc_x + q.n_soc_x);
     h_socG_.insert(h_socG_.end(), q.socG, q.socG + q.n_socG);
+    cones_[0][k][1] = (int64_t)h_socx_.size();
+    cones_[1][k][1] = (int64_t)h_socG_.size();
   }
   for (int64_t k = 0; k < K; ++k) {
     const pdcs_problem& q = probs_[k];
+    cones_[0][k][2] = (int64_t)(h_socx_.size() + h_rsocx_.size());
+    cones_[1][k][2] = (int64_t)(h_socG_.size() + h_rsocG_.size());
     h_rsocx_.insert(h_rsocx_.end(), q.rsoc_x, q.rsoc_x + q.n_rsoc_x);
     h_rsocG_.insert(h_rsocG_.end(), q.rsocG, q.rsocG + q.n_rsocG);
+    cones_[0][k][3] = (int64_t)(h_socx_.size() + h_rsocx_.size());
+    cones_[1][k][3] = (int64_t)(h_socG_.size() + h_rsocG_.size());
+  }
+  {
+    int64_t ex = 0, ey = 0, dx = 0, dy = 0, EX = 0, EY = 0;
+    for (int64_t k = 0; k < K; ++k) {
+      EX += probs_[k].exp_x;
+      EY += probs_[k].expG;
+    }
+    for (int64_t k = 0; k < K; ++k) {
+      const pdcs_problem& q = probs_[k];
+      cones_[0][k][4] = ex;
+      cones_[0][k][5] = ex += q.exp_x;
+      cones_[0][k][6] = EX + dx;
+      cones_[0][k][7] = EX + (dx += q.dual_exp_x);
+      cones_[1][k][4] = ey;
+      cones_[1][k][5] = ey += q.expG;
+      cones_[1][k][6] = EY + dy;
+      cones_[1][k][7] = EY + (dy += q.dual_expG);
+    }
+  }
+  for (int w = 0; w < 2; ++w) {
+    const std::vector<int64_t>& soc = w ? h_socG_ : h_socx_;
+    const std::vector<int64_t>& rsoc = w ? h_rsocG_ : h_rsocx_;
+    cone_cls_[w].clear();
+    for (const std::vector<int64_t>* L : {&soc, &rsoc})
+      for (int64_t d : *L) {
+        int c = 0;
+        while (c < kCls - 1 && d > (2 << c)) ++c;  // the classes of the cone tables' schedule
+        cone_cls_[w].push_back((int8_t)c);
+      }
   }
   pdcs_problem mp;
   std::memset(&mp, 0, sizeof(mp));
@@ -657,6 +716,133 @@ void BatchSolver::setup_compaction() {
   }
 }
 
+// Device buffers of the active work lists, sized for every instance iterating.
+void BatchSolver::setup_act_lists() {
+  auto nchunks = [](int64_t len) { return (len + kThreads - 1) / kThreads; };
+  const ConeTable* T[2] = {&XI, &YI};
+  size_t bytes = 0;
+  int64_t nr = 0;
+  for (int w = 0; w < 2; ++w) {
+    const std::vector<int64_t>& rl = w ? yrun_len_ : xrun_len_;
+    int64_t nc = 0;
+    for (int64_t k = 0; k < K_; ++k) {
+      for (int q = 0; q < (w ? 2 : 1); ++q) nc += nchunks(rl[k * kMaxRuns + q]);
+      for (int q = 0; q < kMaxRuns; ++q) nr += nchunks(rl[k * kMaxRuns + q]);
+    }
+    const int64_t ne = T[w]->exp_count + T[w]->dexp_count;
+    act_[w].chunk = A.alloc<int2>(std::max<int64_t>(nc, 1));
+    act_[w].meta = A.alloc<int64_t>(2 * kCls + 4);
+    act_[w].sched = A.alloc<int64_t>(std::max<int64_t>(T[w]->nwc, 1));
+    act_[w].exp = A.alloc<int32_t>(std::max<int64_t>(ne, 1));
+    bytes += nc * sizeof(int2) + (2 * kCls + 4) * sizeof(int64_t) + T[w]->nwc * sizeof(int64_t) + ne * sizeof(int32_t);
+  }
+  rchunk_ = A.alloc<int4>(std::max<int64_t>(nr, 1));
+  n_rchunk_ = A.alloc<int64_t>(1);
+  act_inst_ = A.alloc<int32_t>(K_);
+  n_act_ = A.alloc<int64_t>(1);
+  bytes += nr * sizeof(int4) + K_ * sizeof(int32_t) + 2 * sizeof(int64_t) + 16 * 256;
+  act_bytes_ = bytes;
+  const size_t need = pin_cap_ + bytes;
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  PDCS_CUDA(cudaFreeHost(pin_));
+  pin_ = nullptr;
+  PDCS_CUDA(cudaMallocHost(&pin_, need));
+  pin_cap_ = need;
+  pin_off_ = 0;
+  XIg_ = XI;
+  XIg_.act_chunk = act_[0].chunk;
+  XIg_.act_meta = act_[0].meta;
+  XIg_.act_sched = act_[0].sched;
+  XIg_.act_exp = act_[0].exp;
+  YIg_ = YI;
+  YIg_.act_chunk = act_[1].chunk;
+  YIg_.act_meta = act_[1].meta;
+  YIg_.act_sched = act_[1].sched;
+  YIg_.act_exp = act_[1].exp;
+}
+
+// Lists of the work of the iterating instances: elementwise chunks, warp cones
+// by size class, exp cones, reflection chunks and the instances themselves.
+void BatchSolver::build_act_lists(const std::vector<Inst*>& its) {
+  std::vector<uint8_t> set(K_, 0);
+  for (Inst* I : its) set[I->k] = 1;
+  if (set == act_set_) return;
+  act_set_ = set;
+  auto chunks = [](int64_t start, int64_t len, auto&& emit) {
+    for (int64_t o = 0; o < len; o += kThreads) emit(start + o, std::min<int64_t>(kThreads, len - o));
+  };
+  for (int w = 0; w < 2; ++w) {
+    const std::vector<int64_t>& rs = w ? yrun_start_ : xrun_start_;
+    const std::vector<int64_t>& rl = w ? yrun_len_ : xrun_len_;
+    std::vector<int2> ch;
+    std::vector<int64_t> bycls[kCls];
+    std::vector<int32_t> ex;
+    for (Inst* I : its) {
+      const int64_t k = I->k;
+      for (int q = 0; q < (w ? 2 : 1); ++q)  // elementwise runs: x box; y zero, nonneg
+        chunks(rs[k * kMaxRuns + q], rl[k * kMaxRuns + q],
+               [&](int64_t a, int64_t l) { ch.push_back(make_int2((int32_t)a, (int32_t)l)); });
+      const std::array<int64_t, 8>& c = cones_[w][k];
+      for (int64_t i = c[0]; i < c[1]; ++i) bycls[cone_cls_[w][i]].push_back(i);
+      for (int64_t i = c[2]; i < c[3]; ++i) bycls[cone_cls_[w][i]].push_back(i);
+      for (int64_t i = c[4]; i < c[5]; ++i) ex.push_back((int32_t)i);
+      for (int64_t i = c[6]; i < c[7]; ++i) ex.push_back((int32_t)i);
+    }
+    int64_t* meta = stage<int64_t>(2 * kCls + 4);
+    meta[0] = (int64_t)ch.size();
+    int64_t task = 0, off = 0;
+    size_t total = 0;
+    for (int c = 0; c < kCls; ++c) total += bycls[c].size();
+    int64_t* sched = stage<int64_t>(std::max<size_t>(total, 1));
+    for (int c = 0; c < kCls; ++c) {
+      meta[1 + c] = task;
+      meta[kCls + 2 + c] = off;
+      std::memcpy(sched + off, bycls[c].data(), bycls[c].size() * sizeof(int64_t));
+      const int64_t per = (c < kCls - 1) ? 32 / (2 << c) : 1;
+      task += ((int64_t)bycls[c].size() + per - 1) / per;
+      off += (int64_t)bycls[c].size();
+    }
+    meta[1 + kCls] = task;
+    meta[2 * kCls + 2] = off;
+    meta[2 * kCls + 3] = (int64_t)ex.size();
+    PDCS_CUDA(cudaMemcpyAsync(act_[w].meta, meta, sizeof(int64_t) * (2 * kCls + 4), cudaMemcpyHostToDevice, s_));
+    if (total)
+      PDCS_CUDA(cudaMemcpyAsync(act_[w].sched, sched, sizeof(int64_t) * total, cudaMemcpyHostToDevice, s_));
+    if (!ch.empty()) {
+      int2* hc = stage<int2>(ch.size());
+      std::memcpy(hc, ch.data(), ch.size() * sizeof(int2));
+      PDCS_CUDA(cudaMemcpyAsync(act_[w].chunk, hc, sizeof(int2) * ch.size(), cudaMemcpyHostToDevice, s_));
+    }
+    if (!ex.empty()) {
+      int32_t* he = stage<int32_t>(ex.size());
+      std::memcpy(he, ex.data(), ex.size() * sizeof(int32_t));
+      PDCS_CUDA(cudaMemcpyAsync(act_[w].exp, he, sizeof(int32_t) * ex.size(), cudaMemcpyHostToDevice, s_));
+    }
+  }
+  std::vector<int4> rc;
+  for (Inst* I : its)
+    for (int w = 0; w < 2; ++w) {
+      const std::vector<int64_t>& rs = w ? yrun_start_ : xrun_start_;
+      const std::vector<int64_t>& rl = w ? yrun_len_ : xrun_len_;
+      for (int q = 0; q < kMaxRuns; ++q)
+        chunks(rs[I->k * kMaxRuns + q], rl[I->k * kMaxRuns + q],
+               [&](int64_t a, int64_t l) { rc.push_back(make_int4((int32_t)a, (int32_t)l, w, 0)); });
+    }
+  int64_t* hn = stage<int64_t>(2);
+  hn[0] = (int64_t)rc.size();
+  hn[1] = (int64_t)its.size();
+  PDCS_CUDA(cudaMemcpyAsync(n_rchunk_, hn, sizeof(int64_t), cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(n_act_, hn + 1, sizeof(int64_t), cudaMemcpyHostToDevice, s_));
+  if (!rc.empty()) {
+    int4* hr = stage<int4>(rc.size());
+    std::memcpy(hr, rc.data(), rc.size() * sizeof(int4));
+    PDCS_CUDA(cudaMemcpyAsync(rchunk_, hr, sizeof(int4) * rc.size(), cudaMemcpyHostToDevice, s_));
+  }
+  int32_t* hi = stage<int32_t>(std::max<size_t>(its.size(), 1));
+  for (size_t i = 0; i < its.size(); ++i) hi[i] = (int32_t)its[i]->k;
+  PDCS_CUDA(cudaMemcpyAsync(act_inst_, hi, sizeof(int32_t) * its.size(), cudaMemcpyHostToDevice, s_));
+}
+
 // Rebuild the iteration graph's row lists from the rows of the masked instances.
 void BatchSolver::compact(const uint8_t* mask) {
   const CsrDev* full[2] = {&G_, &Gt_};
@@ -680,28 +866,31 @@ void BatchSolver::capture_batch_graph() {
     spmv_binned_kernel<1, false, float><<<Gt32c_.cta0[kBins], kThreads, 0, s_>>>(Gt32c_, dyl32_, nullptr, aty32_,
                                                                                nullptr, cur);
     OpPrimalStep32B op1{xa_, dxl32_, qa_, aty32_, dx32_, x, ix_, live_, ps_, dxsq_};
-    launch_update_project(op1, XI, part_x, cur, s_);
+    launch_update_project(op1, XIg_, part_x, cur, s_);
     spmv_binned_kernel<2, false, float><<<G32c_.cta0[kBins], kThreads, 0, s_>>>(G32c_, dx32_, dxl32_, gx32_,
                                                                               gxl32_, cur);
     OpDualStep32B op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_};
-    launch_update_project(op2, YI, part_y, cur, s_);
-    BatchCtl ctl{sts_, ps_, ds_, live_, rx_, ry_, dxsq_, dysq_, dgdy_, cur, nxt, done_ctas_, live_cnt_ + 2};
+    launch_update_project(op2, YIg_, part_y, cur, s_);
+    BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,
+                 dgdy_, cur,  nxt,     done_ctas_, live_cnt_ + 2, act_inst_, n_act_};
     batch_control_kernel<<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
-    batch_reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dx32_, dxl32_, dxm_, n_, dy32_,
-                                                               dyl32_, dym_, m_);
+    batch_reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dx32_, dxl32_, dxm_, dy32_,
+                                                               dyl32_, dym_, rchunk_, n_rchunk_);
   }
   for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
     int32_t* cur = live_cnt_ + (a & 1);
     int32_t* nxt = live_cnt_ + ((a + 1) & 1);
     spmv_binned_kernel<1><<<Gtc_.cta0[kBins], kThreads, 0, s_>>>(Gtc_, yl, nullptr, aty, nullptr, cur);
     OpPrimalStepB op1{xl, aty, c_s, x, ix_, live_, ps_, dxsq_};
-    launch_update_project(op1, XI, part_x, cur, s_);
+    launch_update_project(op1, XIg_, part_x, cur, s_);
     spmv_binned_kernel<2><<<Gc_.cta0[kBins], kThreads, 0, s_>>>(Gc_, x, xl, gx, gxl, cur);
     OpDualStepB op2{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_};
-    launch_update_project(op2, YI, part_y, cur, s_);
-    BatchCtl ctl{sts_, ps_, ds_, live_, rx_, ry_, dxsq_, dysq_, dgdy_, cur, nxt, done_ctas_, live_cnt_ + 2};
+    launch_update_project(op2, YIg_, part_y, cur, s_);
+    BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,
+                 dgdy_, cur,  nxt,     done_ctas_, live_cnt_ + 2, act_inst_, n_act_};
     batch_control_kernel<<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
-    batch_reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, x, xl, xm, n_, y, yl, ym, m_);
+    batch_reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, x, xl, xm, y, yl, ym, rchunk_,
+                                                             n_rchunk_);
   }
   PDCS_CUDA(cudaStreamEndCapture(s_, &bgraph_));
   PDCS_CUDA(cudaGraphInstantiate(&bgraph_exec_, bgraph_, 0));
@@ -878,6 +1067,7 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   // instances that halt during these graphs are still computed; their products
   // are not read before the next attempt or anchor recomputes them)
   compact(live_);
+  build_act_lists(its);
   if (fp32_) {
     // FP64 anchors at the current iterates: for instances that (re)start
     // iterating, and every round for the others (refinement keeps the FP32
@@ -1375,6 +1565,7 @@ int BatchSolver::prepare() {
   setup();
   setup_batch();
   setup_compaction();
+  setup_act_lists();
   // the merged matrix lives on the device now
   std::vector<int32_t>().swap(h_ci_);
   std::vector<double>().swap(h_v_);
@@ -1399,6 +1590,7 @@ void BatchSolver::reset_state() {
   if (YI.nwc) PDCS_CUDA(cudaMemsetAsync(YI.soc_ws, 0xff, sizeof(double) * YI.nwc, s_));
   PDCS_CUDA(cudaMemsetAsync(live_cnt_, 0, 4 * sizeof(int32_t), s_));
   PDCS_CUDA(cudaMemsetAsync(done_ctas_, 0, sizeof(uint32_t), s_));
+  act_set_.clear();
   inst_.clear();
   inst_.resize(K_);
   for (int64_t k = 0; k < K_; ++k) {

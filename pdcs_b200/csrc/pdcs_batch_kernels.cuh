@@ -205,6 +205,8 @@ struct BatchCtl {
   int32_t* live_next;
   uint32_t* done_ctas;
   int32_t* live_accum;
+  const int32_t* act_inst;  // instances iterating this round (NULL: all K)
+  const int64_t* n_act;
 };
 
 __global__ void __launch_bounds__(kThreads) batch_control_kernel(int64_t K, BatchCtl c) {
@@ -214,8 +216,10 @@ __global__ void __launch_bounds__(kThreads) batch_control_kernel(int64_t K, Batc
   }
   const int lane = threadIdx.x & 31;
   const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t nk = c.act_inst ? *c.n_act : K;
   int nlive = 0;
-  for (int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < K; k += wstride) {
+  for (int64_t kk = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; kk < nk; kk += wstride) {
+    const int64_t k = c.act_inst ? (int64_t)c.act_inst[kk] : kk;
     if (!c.live[k]) {
       // no step ran for this instance: nothing to reflect
       if (lane == 0) c.sts[k].do_reflect = 0;
@@ -266,19 +270,24 @@ __global__ void __launch_bounds__(kThreads) batch_control_kernel(int64_t K, Batc
 
 // Reflection + eta-weighted averaging with per-instance coefficients
 // (reflect_kernel per instance); runs when the attempt's control step ran.
+// Work: the chunks {first element, length <= kThreads, 0 = x / 1 = y} of the
+// iterating instances, a CTA per chunk.
 __global__ void __launch_bounds__(kThreads) batch_reflect_kernel(const int32_t* __restrict__ live_cur,
                                                                 const PdhgState* __restrict__ sts,
                                                                 const int32_t* __restrict__ ix,
                                                                 const int32_t* __restrict__ iy,
                                                                 double* __restrict__ x, double* __restrict__ xl,
-                                                                double* __restrict__ xm, int64_t n,
-                                                                double* __restrict__ y, double* __restrict__ yl,
-                                                                double* __restrict__ ym, int64_t m) {
-  if (live_cur && *live_cur == 0) return;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += stride) {
-    const bool isx = i < n;
-    const int64_t j = isx ? i : i - n;
+                                                                double* __restrict__ xm, double* __restrict__ y,
+                                                                double* __restrict__ yl, double* __restrict__ ym,
+                                                                const int4* __restrict__ rchunk,
+                                                                const int64_t* __restrict__ n_rchunk) {
+  if (*live_cur == 0) return;
+  const int64_t nch = *n_rchunk;
+  for (int64_t q = blockIdx.x; q < nch; q += gridDim.x) {
+    const int4 ch = rchunk[q];
+    if ((int)threadIdx.x >= ch.y) continue;
+    const bool isx = ch.z == 0;
+    const int64_t j = (int64_t)ch.x + threadIdx.x;
     const PdhgState& s = sts[isx ? ix[j] : iy[j]];
     if (!s.do_reflect) continue;
     double* v = isx ? x : y;

@@ -157,19 +157,23 @@ __global__ void __launch_bounds__(kThreads) reflect32_kernel(const PdhgState* __
   }
 }
 
+// batch_reflect_kernel on the deltas: the chunks of the iterating instances, a CTA per chunk
 __global__ void __launch_bounds__(kThreads) batch_reflect32_kernel(const int32_t* __restrict__ live_cur,
                                                                   const PdhgState* __restrict__ sts,
                                                                   const int32_t* __restrict__ ix,
                                                                   const int32_t* __restrict__ iy,
                                                                   float* __restrict__ dx, float* __restrict__ dxl,
-                                                                  double* __restrict__ dxm, int64_t n,
-                                                                  float* __restrict__ dy, float* __restrict__ dyl,
-                                                                  double* __restrict__ dym, int64_t m) {
+                                                                  double* __restrict__ dxm, float* __restrict__ dy,
+                                                                  float* __restrict__ dyl, double* __restrict__ dym,
+                                                                  const int4* __restrict__ rchunk,
+                                                                  const int64_t* __restrict__ n_rchunk) {
   if (*live_cur == 0) return;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += stride) {
-    const bool isx = i < n;
-    const int64_t j = isx ? i : i - n;
+  const int64_t nch = *n_rchunk;
+  for (int64_t q = blockIdx.x; q < nch; q += gridDim.x) {
+    const int4 ch = rchunk[q];
+    if ((int)threadIdx.x >= ch.y) continue;
+    const bool isx = ch.z == 0;
+    const int64_t j = (int64_t)ch.x + threadIdx.x;
     const PdhgState& s = sts[isx ? ix[j] : iy[j]];
     if (!s.do_reflect) continue;
     if (isx) reflect32_elem(s, dx, dxl, dxm, j);

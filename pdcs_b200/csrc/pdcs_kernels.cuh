@@ -262,6 +262,14 @@ struct ConeTable {
   int64_t cls_off[kCls + 1];  // ranges of sched per class
   int64_t task0[kCls + 1];    // first warp task of each class; task0[kCls] = tasks
   double* soc_ws;             // per warp cone warm start of the weighted-SOC root (NULL: none)
+  // Active work lists (batched solver's iteration graph; NULL: the whole table).
+  // act_meta: [0] elementwise chunks, [1 .. kCls + 1] warp tasks per class
+  // (as task0), [kCls + 2 .. 2 kCls + 2] ranges of act_sched (as cls_off),
+  // [2 kCls + 3] exp / dual-exp cones in act_exp.
+  const int2* act_chunk;      // elementwise chunks {first element, length <= kThreads}
+  const int64_t* act_meta;
+  const int64_t* act_sched;   // warp-cone indices, class by class
+  const int32_t* act_exp;     // exp / dual-exp cone ordinals (0 .. exp_count + dexp_count)
   int64_t elem_total;        // sum of seg_len
   int32_t ctaA, ctaB, ctaC;  // CTAs for elementwise / warp cones / exp cones
 };
@@ -403,7 +411,24 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
   for (int k = 0; k < Op::NACC; ++k) acc[k] = 0.0;
   const int b = blockIdx.x;
   const int nblocks = gridDim.x;
-  if (b < T.ctaA) {
+  if (b < T.ctaA && T.act_chunk) {
+    // chunks of the elementwise segments, a CTA per chunk
+    const int64_t nch = T.act_meta[0];
+    for (int64_t q = b; q < nch; q += T.ctaA) {
+      const int2 ch = T.act_chunk[q];
+      if ((int)threadIdx.x >= ch.y) continue;
+      const int64_t j = (int64_t)ch.x + threadIdx.x;
+      if constexpr (MaskedOp<Op>) {
+        if (!op.live(j)) continue;
+      }
+      int32_t kind = T.seg_kind[0];
+      for (int s = 1; s < T.nseg; ++s)
+        if (j >= T.seg_start[s]) kind = T.seg_kind[s];
+      double z = op.z(j);
+      double p = elem_proj(kind, z, j, T);
+      op.fin(j, z, p, acc);
+    }
+  } else if (b < T.ctaA) {
     const int64_t stride = (int64_t)T.ctaA * kThreads;
     for (int s = 0; s < T.nseg; ++s) {
       const int64_t j0 = T.seg_start[s], j1 = j0 + T.seg_len[s];
@@ -421,19 +446,26 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
     const int lane = threadIdx.x & 31;
     const int64_t wstride = (int64_t)T.ctaB * kWarps;
     const double r2 = 0.7071067811865476;
-    for (int64_t task = (int64_t)(b - T.ctaA) * kWarps + (threadIdx.x >> 5); task < T.task0[kCls];
+    int64_t task0[kCls + 1], cls_off[kCls + 1];
+    const int64_t* sched = T.act_sched ? T.act_sched : T.sched;
+#pragma unroll
+    for (int q = 0; q <= kCls; ++q) {
+      task0[q] = T.act_sched ? T.act_meta[1 + q] : T.task0[q];
+      cls_off[q] = T.act_sched ? T.act_meta[kCls + 2 + q] : T.cls_off[q];
+    }
+    for (int64_t task = (int64_t)(b - T.ctaA) * kWarps + (threadIdx.x >> 5); task < task0[kCls];
          task += wstride) {
       int c = 0;
 #pragma unroll
       for (int q = 1; q < kCls; ++q)
-        if (task >= T.task0[q]) c = q;
+        if (task >= task0[q]) c = q;
       if (c < kCls - 1) {
         // 32 / g blocks of at most g elements, one per lane group
         const int g = 2 << c;
         const int gl = lane & (g - 1);
-        const int64_t idx = T.cls_off[c] + (task - T.task0[c]) * (32 / g) + lane / g;
-        bool have = idx < T.cls_off[c + 1];
-        const int64_t k = have ? T.sched[idx] : 0;
+        const int64_t idx = cls_off[c] + (task - task0[c]) * (32 / g) + lane / g;
+        bool have = idx < cls_off[c + 1];
+        const int64_t k = have ? sched[idx] : 0;
         const int64_t st = have ? T.wc_start[k] : 0;
         if constexpr (MaskedOp<Op>) {
           if (have && !op.live(st)) have = false;  // group-uniform: a block belongs to one instance
@@ -463,7 +495,7 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
         if (gl < d) op.fin(st + gl, z, v, acc);
       } else {
         // blocks of more than 32 elements: a warp each, values staged in op.out
-        const int64_t k = T.sched[T.cls_off[c] + (task - T.task0[c])];
+        const int64_t k = sched[cls_off[c] + (task - task0[c])];
         const int64_t st = T.wc_start[k];
         if constexpr (MaskedOp<Op>) {
           if (!op.live(st)) continue;  // warp-uniform
@@ -509,8 +541,9 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
     }
   } else if constexpr (EXP) {
     const int64_t tstride = (int64_t)T.ctaC * kThreads;
-    const int64_t total = T.exp_count + T.dexp_count;
-    for (int64_t k = (int64_t)(b - T.ctaA - T.ctaB) * kThreads + threadIdx.x; k < total; k += tstride) {
+    const int64_t total = T.act_exp ? T.act_meta[2 * kCls + 3] : T.exp_count + T.dexp_count;
+    for (int64_t kk = (int64_t)(b - T.ctaA - T.ctaB) * kThreads + threadIdx.x; kk < total; kk += tstride) {
+      const int64_t k = T.act_exp ? (int64_t)T.act_exp[kk] : kk;
       const bool first = k < T.exp_count;
       const int64_t j = first ? T.exp_base + 3 * k : T.dexp_base + 3 * (k - T.exp_count);
       if constexpr (MaskedOp<Op>) {
