@@ -270,6 +270,8 @@ def run_ours(args):
     it_rate = replicas.sum_over_ranks(iters, world) / t_max
     iters_per_inst = [s.info.iter for s in sols]
 
+    lanes = list(sols[0].info.spmv_lane_nnz)
+
     # ---- per-attempt time with every instance iterating (no checkpoint below 2000 attempts) ----
     (_, _), t1 = timed(stream, lambda: h.solve(attempt_limit=64))
     (_, _), t2 = timed(stream, lambda: h.solve(attempt_limit=320))
@@ -293,6 +295,18 @@ def run_ours(args):
                           "primal/dual update + projections, per-instance control, reflection)",
                 "algorithmic_bytes_per_attempt": B_att, "attempt_ms": t_att * 1e3,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"}
+
+    # ---- the autotuned SpMV schedule against one fixed schedule (4 nonzeros per lane) ----
+    hf = solver.BatchHandle(batch, precision="fp32", stream=stream.cuda_stream, spmv_lane_nnz=4)
+    timed(stream, lambda: hf.solve(attempt_limit=64))
+    (_, _), tf1 = timed(stream, lambda: hf.solve(attempt_limit=64))
+    (_, _), tf2 = timed(stream, lambda: hf.solve(attempt_limit=320))
+    (sf, _), tf = timed(stream, hf.solve)
+    hf.close()
+    schedule = {"autotuned_lane_nnz_G_Gt": lanes, "autotuned_attempt_ms": t_att * 1e3,
+                "fixed_lane_nnz": 4, "fixed_attempt_ms": (tf2 - tf1) / 256 * 1e3,
+                "fixed_time_to_1e-6_ms": 1e3 * tf,
+                "fixed_optimal": sum(1 for s in sf if s.info.exit_status == "optimal")}
 
     # ---- the same batch, batched FP64 (one timed solve) ----
     h64 = solver.BatchHandle(batch, precision="fp64", stream=stream.cuda_stream)
@@ -351,6 +365,7 @@ def run_ours(args):
                 "batched_fp64": {"time_to_1e-6_ms": 1e3 * t64, "instances_per_s": units / t64,
                                  "optimal": sum(1 for s in s64 if s.info.exit_status == "optimal")},
                 "plain_fp64": plain, "speedup_vs_plain_fp64": value / plain["instances_per_s"] / world,
+                "spmv_schedule": schedule,
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
                 "cpu_baseline": cpu, "single_instance": single}
         print(json.dumps(line), flush=True)

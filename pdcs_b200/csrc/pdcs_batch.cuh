@@ -863,12 +863,10 @@ void BatchSolver::capture_batch_graph() {
   for (int a = 0; a < attempts_per_graph_ && fp32_; ++a) {
     int32_t* cur = live_cnt_ + (a & 1);
     int32_t* nxt = live_cnt_ + ((a + 1) & 1);
-    spmv_binned_kernel<1, false, float><<<Gt32c_.cta0[kBins], kThreads, 0, s_>>>(Gt32c_, dyl32_, nullptr, aty32_,
-                                                                               nullptr, cur);
+    launch_spmv<1, false, float>(Gt32c_, dyl32_, nullptr, aty32_, nullptr, cur, s_);
     OpPrimalStep32B op1{xa_, dxl32_, qa_, aty32_, dx32_, x, ix_, live_, ps_, dxsq_};
     launch_update_project(op1, XIg_, part_x, cur, s_);
-    spmv_binned_kernel<2, false, float><<<G32c_.cta0[kBins], kThreads, 0, s_>>>(G32c_, dx32_, dxl32_, gx32_,
-                                                                              gxl32_, cur);
+    launch_spmv<2, false, float>(G32c_, dx32_, dxl32_, gx32_, gxl32_, cur, s_);
     OpDualStep32B op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_};
     launch_update_project(op2, YIg_, part_y, cur, s_);
     BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,
@@ -880,10 +878,10 @@ void BatchSolver::capture_batch_graph() {
   for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
     int32_t* cur = live_cnt_ + (a & 1);
     int32_t* nxt = live_cnt_ + ((a + 1) & 1);
-    spmv_binned_kernel<1><<<Gtc_.cta0[kBins], kThreads, 0, s_>>>(Gtc_, yl, nullptr, aty, nullptr, cur);
+    launch_spmv<1>(Gtc_, yl, nullptr, aty, nullptr, cur, s_);
     OpPrimalStepB op1{xl, aty, c_s, x, ix_, live_, ps_, dxsq_};
     launch_update_project(op1, XIg_, part_x, cur, s_);
-    spmv_binned_kernel<2><<<Gc_.cta0[kBins], kThreads, 0, s_>>>(Gc_, x, xl, gx, gxl, cur);
+    launch_spmv<2>(Gc_, x, xl, gx, gxl, cur, s_);
     OpDualStepB op2{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_};
     launch_update_project(op2, YIg_, part_y, cur, s_);
     BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,

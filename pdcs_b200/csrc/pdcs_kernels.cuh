@@ -103,6 +103,7 @@ struct CsrT {
   const T* v;
   const int4* rows;          // row descriptors ordered by bin (one 16-byte load per row)
   const int64_t* dbin;       // device bin offsets (a compacted row list) or NULL: bin_off
+  int32_t lane_nnz;          // schedule: at most lane_nnz nonzeros per lane in bins 0..5
   int64_t bin_off[kBins + 1];
   int32_t cta0[kBins + 1];   // first CTA of each bin, cta0[kBins] = grid size
 };
@@ -126,7 +127,9 @@ struct RowAcc {
 };
 
 // MASK: rows whose instance (rows[q].w) has imask == 0 are skipped (batched solver).
-template <int NV, bool MASK = false, class T = double>
+// LN = A.lane_nnz: a lane holds at most LN nonzeros of its row in bins 0..5, so
+// all of a lane's value / index loads are issued together, then all its gathers.
+template <int NV, bool MASK = false, class T = double, int LN = 4>
 __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
                                                               const std::type_identity_t<T>* __restrict__ x0,
                                                               const std::type_identity_t<T>* __restrict__ x1,
@@ -160,30 +163,25 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
       const int32_t row = ri.x;
       if (MASK && valid) valid = imask[ri.w] != 0;
       const int32_t kb = valid ? ri.y : 0, ke = valid ? ri.z : 0;
-      T s0 = T(0), s1 = T(0), t0 = T(0), t1 = T(0), u0 = T(0), u1 = T(0), w0 = T(0), w1 = T(0);
-      int32_t k = kb + lane_g;
-      for (; k + 3 * g < ke; k += 4 * g) {  // four independent gathers in flight
-        const T a = A.v[k], b = A.v[k + g], c = A.v[k + 2 * g], d = A.v[k + 3 * g];
-        const int32_t ca = A.ci[k], cb = A.ci[k + g], cc = A.ci[k + 2 * g], cd = A.ci[k + 3 * g];
-        s0 = fma(a, x0[ca], s0);
-        t0 = fma(b, x0[cb], t0);
-        u0 = fma(c, x0[cc], u0);
-        w0 = fma(d, x0[cd], w0);
-        if (NV == 2) {
-          s1 = fma(a, x1[ca], s1);
-          t1 = fma(b, x1[cb], t1);
-          u1 = fma(c, x1[cc], u1);
-          w1 = fma(d, x1[cd], w1);
+      T av[LN];
+      int32_t cv[LN];
+#pragma unroll
+      for (int u = 0; u < LN; ++u) {
+        const int32_t k = kb + lane_g + u * g;
+        const bool ok = k < ke;
+        av[u] = ok ? A.v[k] : T(0);
+        cv[u] = ok ? A.ci[k] : -1;
+      }
+      T p0[4] = {T(0), T(0), T(0), T(0)}, p1[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+      for (int u = 0; u < LN; ++u) {
+        if (cv[u] >= 0) {
+          p0[u & 3] = fma(av[u], x0[cv[u]], p0[u & 3]);
+          if (NV == 2) p1[u & 3] = fma(av[u], x1[cv[u]], p1[u & 3]);
         }
       }
-      for (; k < ke; k += g) {
-        const T a = A.v[k];
-        const int32_t ca = A.ci[k];
-        s0 = fma(a, x0[ca], s0);
-        if (NV == 2) s1 = fma(a, x1[ca], s1);
-      }
-      s0 = (s0 + t0) + (u0 + w0);
-      s1 = (s1 + t1) + (u1 + w1);
+      T s0 = (p0[0] + p0[1]) + (p0[2] + p0[3]);
+      T s1 = (p1[0] + p1[1]) + (p1[2] + p1[3]);
       for (int o = g >> 1; o > 0; o >>= 1) {
         s0 += __shfl_down_sync(kFull, s0, o, g);
         if (NV == 2) s1 += __shfl_down_sync(kFull, s1, o, g);
@@ -230,6 +228,21 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
       }
       __syncthreads();
     }
+  }
+}
+
+// Launch spmv_binned_kernel with the matrix's schedule (A.lane_nnz).
+template <int NV, bool MASK = false, class T>
+inline void launch_spmv(const CsrT<T>& A, const std::type_identity_t<T>* x0, const std::type_identity_t<T>* x1,
+                        std::type_identity_t<T>* y0, std::type_identity_t<T>* y1, const int32_t* active,
+                        cudaStream_t s, int32_t* clear_flag = nullptr, const uint8_t* imask = nullptr) {
+  const int grid = A.cta0[kBins];
+  switch (A.lane_nnz) {
+    case 1: spmv_binned_kernel<NV, MASK, T, 1><<<grid, kThreads, 0, s>>>(A, x0, x1, y0, y1, active, clear_flag, imask); break;
+    case 2: spmv_binned_kernel<NV, MASK, T, 2><<<grid, kThreads, 0, s>>>(A, x0, x1, y0, y1, active, clear_flag, imask); break;
+    case 8: spmv_binned_kernel<NV, MASK, T, 8><<<grid, kThreads, 0, s>>>(A, x0, x1, y0, y1, active, clear_flag, imask); break;
+    case 16: spmv_binned_kernel<NV, MASK, T, 16><<<grid, kThreads, 0, s>>>(A, x0, x1, y0, y1, active, clear_flag, imask); break;
+    default: spmv_binned_kernel<NV, MASK, T, 4><<<grid, kThreads, 0, s>>>(A, x0, x1, y0, y1, active, clear_flag, imask); break;
   }
 }
 

@@ -488,13 +488,12 @@ class Solver {
   void capture_graph();
   // ---- device helpers ----
   void spmv(const CsrDev& M, const double* xin, double* yout) {
-    spmv_binned_kernel<1><<<M.cta0[kBins], kThreads, 0, s_>>>(M, xin, nullptr, yout, nullptr, nullptr);
+    launch_spmv<1>(M, xin, nullptr, yout, nullptr, nullptr, s_);
     kernels_++;
   }
   // rows of the instances with mask[k] != 0 only (batched solver)
   void spmv_masked(const CsrDev& M, const double* xin, double* yout, const uint8_t* mask) {
-    spmv_binned_kernel<1, true><<<M.cta0[kBins], kThreads, 0, s_>>>(M, xin, nullptr, yout, nullptr, nullptr, nullptr,
-                                                                    mask);
+    launch_spmv<1, true>(M, xin, nullptr, yout, nullptr, nullptr, s_, nullptr, mask);
     kernels_++;
   }
   void axpby(double* out, double a, const double* u, double b, const double* v, int64_t len) {
@@ -654,6 +653,7 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
   D.ci = d_ci;
   D.v = d_v;
   D.dbin = nullptr;
+  D.lane_nnz = lane_nnz;
   auto bin_of = [&](int64_t i) {
     const int64_t L = rp[i + 1] - rp[i];
     if (L > 32LL * lane_nnz) return kBins - 1;
@@ -1089,6 +1089,7 @@ void Solver::setup_fp32() {
     F.v = v;
     F.rows = D.rows;
     F.dbin = D.dbin;
+    F.lane_nnz = D.lane_nnz;
     for (int b = 0; b <= kBins; ++b) {
       F.bin_off[b] = D.bin_off[b];
       F.cta0[b] = D.cta0[b];
@@ -1137,22 +1138,19 @@ void Solver::capture_graph() {
   PDCS_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
   const int32_t* act = &st_dev->active;
   for (int a = 0; a < attempts_per_graph_ && fp32_; ++a) {
-    spmv_binned_kernel<1, false, float><<<Gt32_.cta0[kBins], kThreads, 0, s_>>>(Gt32_, dyl32_, nullptr, aty32_,
-                                                                               nullptr, act, &st_dev->do_reflect);
+    launch_spmv<1, false, float>(Gt32_, dyl32_, nullptr, aty32_, nullptr, act, s_, &st_dev->do_reflect);
     OpPrimalStep32 op1{xa_, dxl32_, qa_, aty32_, dx32_, x, st_dev, 0.0};
     launch_update_project(op1, XI, part_x, act, s_);
-    spmv_binned_kernel<2, false, float><<<G32_.cta0[kBins], kThreads, 0, s_>>>(G32_, dx32_, dxl32_, gx32_, gxl32_,
-                                                                             act);
+    launch_spmv<2, false, float>(G32_, dx32_, dxl32_, gx32_, gxl32_, act, s_);
     OpDualStep32 op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, st_dev, 0.0, part_x, XI.ctaA + XI.ctaB + XI.ctaC};
     launch_update_project(op2, YI, part_y, act, s_);
     reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, dx32_, dxl32_, dxm_, n_, dy32_, dyl32_, dym_, m_);
   }
   for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
-    spmv_binned_kernel<1><<<Gt_.cta0[kBins], kThreads, 0, s_>>>(Gt_, yl, nullptr, aty, nullptr, act,
-                                                                &st_dev->do_reflect);
+    launch_spmv<1>(Gt_, yl, nullptr, aty, nullptr, act, s_, &st_dev->do_reflect);
     OpPrimalStep op1{xl, aty, c_s, x, st_dev, 0.0};
     launch_update_project(op1, XI, part_x, act, s_);
-    spmv_binned_kernel<2><<<G_.cta0[kBins], kThreads, 0, s_>>>(G_, x, xl, gx, gxl, act);
+    launch_spmv<2>(G_, x, xl, gx, gxl, act, s_);
     // the dual step's last CTA runs the attempt's control step
     OpDualStep op2{yl, gx, gxl, h_s, y, st_dev, 0.0, part_x, XI.ctaA + XI.ctaB + XI.ctaC};
     launch_update_project(op2, YI, part_y, act, s_);
