@@ -110,7 +110,7 @@ typedef struct {
   int32_t force_resolving;       /* test hook: enter the resolving fallback at the first outer iteration */
   int32_t spmv_lane_nnz;         /* SpMV schedule, nonzeros per lane of a row's lane group (power of two,
                                     1..16); 0 (default) = autotuned per matrix at setup */
-  int32_t reserved_opt;
+  int32_t differentiable;        /* keep the unscaled data the solution-map adjoint (pdcs_batch_grad) needs */
 } pdcs_options;
 
 typedef struct {
@@ -180,6 +180,43 @@ int pdcs_batch_create(int64_t count, const pdcs_problem* problems, const pdcs_op
 /* attempt_limit > 0 overrides the option for this solve. */
 int pdcs_batch_solve(pdcs_batch* batch, int64_t attempt_limit, pdcs_result* results, pdcs_batch_info* info);
 void pdcs_batch_destroy(pdcs_batch* batch);
+
+/* Solution-map adjoint.  No counterpart in the reference.  The solution
+ * (x*, y*) of the unscaled problem is a fixed point of the PDHG map T; with
+ * M = dT/dz there, the loss gradient g = (dL/dx*, dL/dy*) pulls back through
+ * u = (I - M)^{-T} g (M with Pock-Chambolle diagonal steps, constant on each
+ * cone block), solved by restarted GMRES whose operator products use
+ * the solver's SpMV kernels and the projection Jacobians (box, nonneg, SOC,
+ * RSOC, exponential and dual-exponential cones).  Outputs dL/dc, dL/dh,
+ * dL/dG (nonzero values in the problem's own CSR order), dL/dl, dL/du. */
+typedef struct {
+  double rel_tol;     /* relative residual of the adjoint solve (default 1e-10) */
+  int32_t restart;    /* GMRES restart length (default 100, at most 200) */
+  int32_t reserved;
+  int64_t max_iter;   /* total GMRES iterations (default 5000) */
+} pdcs_grad_options;
+
+typedef struct {
+  int64_t iterations; /* GMRES iterations of this instance */
+  double residual;    /* |g - (I - M)' u| / |g| */
+  double time;        /* seconds of the whole adjoint call */
+  int32_t converged;
+  int32_t reserved;
+} pdcs_grad_info;
+
+/* Gradients at the last pdcs_batch_solve of a batch created with
+ * options.differentiable = 1.  Every argument array has `count` entries, one
+ * per instance (host pointers, each sized like the instance's vector; any
+ * array, or entry, may be NULL).  opts may be NULL (defaults). */
+int pdcs_batch_grad(pdcs_batch* batch, const double* const* dldx, const double* const* dldy, double* const* dc,
+                    double* const* dh, double* const* dG, double* const* dl, double* const* du,
+                    const pdcs_grad_options* opts, pdcs_grad_info* info);
+
+/* Gradients of one problem at a given solution (x, y) (host arrays, e.g. from
+ * pdcs_solve); the problem's variables must all lie in the box or a cone block. */
+int pdcs_grad(const pdcs_problem* prob, const pdcs_options* opts, const double* x, const double* y,
+              const double* dldx, const double* dldy, double* dc, double* dh, double* dG, double* dl, double* du,
+              const pdcs_grad_options* gopts, pdcs_grad_info* info);
 
 /* Block projections on device memory.  Replaces the projection entry points
  * few_block_proj (cuda/few_block_proj.cu:414-432, bound by gpu_kernel.jl:377-406)

@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = [os.path.join(HERE, "csrc", "pdcs_solver.cu")]
 DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("pdcs_kernels.cuh", "pdcs_device.cuh", "pdcs_preprocess.cuh",
-                                                     "pdcs_batch.cuh", "pdcs_batch_kernels.cuh", "pdcs_fp32.cuh")] + [
+                                                     "pdcs_batch.cuh", "pdcs_batch_kernels.cuh", "pdcs_fp32.cuh", "pdcs_adjoint.cuh")] + [
     os.path.join(ROOT, "include", "pdcs.h")]
 LIB = os.path.join(HERE, "libpdcs_b200.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++20",

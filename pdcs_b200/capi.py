@@ -65,7 +65,7 @@ class PdcsOptions(C.Structure):
                 ("use_duality_gap_restart", C.c_int32), ("precision", C.c_int32),
                 ("duality_gap_restart_freq", C.c_int64), ("attempt_limit", C.c_int64),
                 ("stream", _vp), ("attempts_per_graph", C.c_int32), ("force_resolving", C.c_int32),
-                ("spmv_lane_nnz", C.c_int32), ("reserved_opt", C.c_int32)]
+                ("spmv_lane_nnz", C.c_int32), ("differentiable", C.c_int32)]
 
 
 class PdcsResult(C.Structure):
@@ -90,9 +90,20 @@ class PdcsBatchInfo(C.Structure):
                 ("service_rounds", C.c_int64), ("single_fallbacks", C.c_int64)]
 
 
+class PdcsGradOptions(C.Structure):
+    _fields_ = [("rel_tol", C.c_double), ("restart", C.c_int32), ("reserved", C.c_int32),
+                ("max_iter", C.c_int64)]
+
+
+class PdcsGradInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("residual", C.c_double), ("time", C.c_double),
+                ("converged", C.c_int32), ("reserved", C.c_int32)]
+
+
 # every symbol declared in include/pdcs.h
 EXPORTS = ["pdcs_default_options", "pdcs_solve", "pdcs_solve_batch", "pdcs_batch_create", "pdcs_batch_solve",
-           "pdcs_batch_destroy", "pdcs_block_proj", "pdcs_spmv_csr", "pdcs_spmv_csr_noalloc", "pdcs_version"]
+           "pdcs_batch_destroy", "pdcs_batch_grad", "pdcs_grad", "pdcs_block_proj", "pdcs_spmv_csr",
+           "pdcs_spmv_csr_noalloc", "pdcs_version"]
 
 _lib = None
 
@@ -118,6 +129,12 @@ def load():
     L.pdcs_batch_solve.restype = C.c_int
     L.pdcs_batch_destroy.argtypes = [_vp]
     L.pdcs_batch_destroy.restype = None
+    _pp = _P(_vp)
+    L.pdcs_batch_grad.argtypes = [_vp, _pp, _pp, _pp, _pp, _pp, _pp, _pp, _P(PdcsGradOptions), _P(PdcsGradInfo)]
+    L.pdcs_batch_grad.restype = C.c_int
+    L.pdcs_grad.argtypes = [_P(PdcsProblem), _P(PdcsOptions), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                            _P(PdcsGradOptions), _P(PdcsGradInfo)]
+    L.pdcs_grad.restype = C.c_int
     L.pdcs_block_proj.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]
     L.pdcs_block_proj.restype = C.c_int
     L.pdcs_spmv_csr.argtypes = [C.c_int64, C.c_int64, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp]

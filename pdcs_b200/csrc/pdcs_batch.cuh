@@ -27,6 +27,7 @@
 #include <unordered_map>
 #include <utility>
 
+#include "pdcs_adjoint.cuh"
 #include "pdcs_batch_kernels.cuh"
 
 namespace pdcs {
@@ -242,6 +243,14 @@ class BatchSolver : public Solver {
     int rc = prepare();
     return rc != PDCS_OK ? rc : solve(res, info, 0);
   }
+  // Solution-map adjoint at the last solve's solution (differentiable mode):
+  // per-instance loss gradients dL/dx*, dL/dy* in, parameter gradients out
+  // (any array may be NULL).  Arrays are indexed by instance.
+  int grad(const double* const* dldx, const double* const* dldy, double* const* dc, double* const* dh,
+           double* const* dG, double* const* dl, double* const* du, const pdcs_grad_options& go,
+           pdcs_grad_info* info);
+  // set the solution the adjoint differentiates at (instance-local host arrays)
+  void set_solution(const double* const* xs, const double* const* ys);
 
  private:
   struct InstConst {
@@ -266,6 +275,27 @@ class BatchSolver : public Solver {
   // [exp_first, exp_end) and dual-exp ordinals [dexp_first, dexp_end)
   std::vector<std::array<int64_t, 8>> cones_[2];
   std::vector<int8_t> cone_cls_[2];  // size class of every warp cone
+  // differentiable mode
+  bool solved_ = false;
+  double *xs_raw_ = nullptr, *ys_raw_ = nullptr;  // the solution in the original scale (merged)
+  ConeTable XA_{}, YA_{};                         // unscaled cone tables of X and K_d*
+  struct Adj {
+    int mr = 0;
+    double *V = nullptr, *g = nullptr, *u = nullptr, *Au = nullptr, *coef = nullptr;
+    double *a = nullptr, *b = nullptr, *xp = nullptr, *tw = nullptr, *tsw = nullptr, *tt = nullptr, *tq = nullptr,
+           *tr = nullptr, *ttr = nullptr, *ts = nullptr, *dG = nullptr, *Tx = nullptr, *Sy = nullptr;
+    double *dots1 = nullptr, *dots2 = nullptr, *dotsn = nullptr;
+    uint8_t* mask = nullptr;
+  } adj_;
+  void setup_adjoint(int mr);
+  void apply_AT(const double* u, double* out, const uint8_t* mask);
+  void scatter_x(const double* merged, double* const* out) const;
+  void scatter_y(const double* merged, double* const* out) const;
+  int64_t merged_row(int64_t k, int64_t i) const {
+    int t = kMaxRuns - 1;
+    while (t > 0 && i < yloc_[k * kMaxRuns + t]) --t;
+    return yrun_start_[k * kMaxRuns + t] + (i - yloc_[k * kMaxRuns + t]);
+  }
   // device
   int32_t *ix_ = nullptr, *iy_ = nullptr;
   RunTable rx_{}, ry_{};
@@ -1564,10 +1594,24 @@ int BatchSolver::prepare() {
   setup_batch();
   setup_compaction();
   setup_act_lists();
-  // the merged matrix lives on the device now
+  // the merged matrix lives on the device now (its row pointers stay for the adjoint's scatter)
   std::vector<int32_t>().swap(h_ci_);
   std::vector<double>().swap(h_v_);
-  std::vector<int32_t>().swap(h_rp_);
+  if (!O.differentiable) std::vector<int32_t>().swap(h_rp_);
+  if (O.differentiable) {
+    xs_raw_ = A.alloc<double>(n_);
+    ys_raw_ = A.alloc<double>(m_);
+    XA_ = XI;
+    XA_.S = nullptr;
+    XA_.lo = bl_raw_;
+    XA_.hi = bu_raw_;
+    XA_.rho_ws = nullptr;
+    XA_.soc_ws = nullptr;
+    YA_ = YI;
+    YA_.S = nullptr;
+    YA_.rho_ws = nullptr;
+    YA_.soc_ws = nullptr;
+  }
   P.G_rowptr = nullptr;
   P.G_colind = nullptr;
   P.G_val = nullptr;
@@ -1629,6 +1673,10 @@ int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_
   std::vector<double> hx(n_), hy(m_);
   PDCS_CUDA(cudaMemcpyAsync(hx.data(), xo, sizeof(double) * n_, cudaMemcpyDeviceToHost, s_));
   PDCS_CUDA(cudaMemcpyAsync(hy.data(), yo, sizeof(double) * m_, cudaMemcpyDeviceToHost, s_));
+  if (O.differentiable) {
+    PDCS_CUDA(cudaMemcpyAsync(xs_raw_, xo, sizeof(double) * n_, cudaMemcpyDeviceToDevice, s_));
+    PDCS_CUDA(cudaMemcpyAsync(ys_raw_, yo, sizeof(double) * m_, cudaMemcpyDeviceToDevice, s_));
+  }
   PDCS_CUDA(cudaStreamSynchronize(s_));
   const double solve_time = now_s() - t_start_;
   int64_t fallbacks = 0;
@@ -1644,6 +1692,16 @@ int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_
       Solver one(&probs_[k], &o1);
       int r1 = one.run(&R);
       if (r1 != PDCS_OK) return r1;
+      if (O.differentiable && R.x && R.y) {  // its solution, for the adjoint
+        for (int t = 0; t < kMaxRuns; ++t) {
+          std::memcpy(hx.data() + xrun_start_[k * kMaxRuns + t], R.x + xloc_[k * kMaxRuns + t],
+                      sizeof(double) * xrun_len_[k * kMaxRuns + t]);
+          std::memcpy(hy.data() + yrun_start_[k * kMaxRuns + t], R.y + yloc_[k * kMaxRuns + t],
+                      sizeof(double) * yrun_len_[k * kMaxRuns + t]);
+        }
+        PDCS_CUDA(cudaMemcpy(xs_raw_, hx.data(), sizeof(double) * n_, cudaMemcpyHostToDevice));
+        PDCS_CUDA(cudaMemcpy(ys_raw_, hy.data(), sizeof(double) * m_, cudaMemcpyHostToDevice));
+      }
       continue;
     }
     for (int t = 0; t < kMaxRuns; ++t) {
@@ -1679,6 +1737,7 @@ int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_
     R.spmv_lane_nnz_G = lane_G_;
     R.spmv_lane_nnz_Gt = lane_Gt_;
   }
+  solved_ = true;
   if (info) {
     info->setup_time = setup_time_;
     info->solve_time = solve_time;
@@ -1688,6 +1747,320 @@ int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_
     info->single_fallbacks = fallbacks;
     info->time_iterations = t_iter_;
   }
+  return PDCS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Solution-map adjoint (differentiable mode); kernels in pdcs_adjoint.cuh.
+// ---------------------------------------------------------------------------
+void BatchSolver::scatter_x(const double* merged, double* const* out) const {
+  for (int64_t k = 0; k < K_; ++k)
+    if (out && out[k])
+      for (int t = 0; t < kMaxRuns; ++t)
+        std::memcpy(out[k] + xloc_[k * kMaxRuns + t], merged + xrun_start_[k * kMaxRuns + t],
+                    sizeof(double) * xrun_len_[k * kMaxRuns + t]);
+}
+
+void BatchSolver::scatter_y(const double* merged, double* const* out) const {
+  for (int64_t k = 0; k < K_; ++k)
+    if (out && out[k])
+      for (int t = 0; t < kMaxRuns; ++t)
+        std::memcpy(out[k] + yloc_[k * kMaxRuns + t], merged + yrun_start_[k * kMaxRuns + t],
+                    sizeof(double) * yrun_len_[k * kMaxRuns + t]);
+}
+
+void BatchSolver::set_solution(const double* const* xs, const double* const* ys) {
+  std::vector<double> hx(n_, 0.0), hy(m_, 0.0);
+  for (int64_t k = 0; k < K_; ++k)
+    for (int t = 0; t < kMaxRuns; ++t) {
+      if (xs[k])
+        std::memcpy(hx.data() + xrun_start_[k * kMaxRuns + t], xs[k] + xloc_[k * kMaxRuns + t],
+                    sizeof(double) * xrun_len_[k * kMaxRuns + t]);
+      if (ys[k])
+        std::memcpy(hy.data() + yrun_start_[k * kMaxRuns + t], ys[k] + yloc_[k * kMaxRuns + t],
+                    sizeof(double) * yrun_len_[k * kMaxRuns + t]);
+    }
+  PDCS_CUDA(cudaMemcpyAsync(xs_raw_, hx.data(), sizeof(double) * n_, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(ys_raw_, hy.data(), sizeof(double) * m_, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  solved_ = true;
+}
+
+void BatchSolver::setup_adjoint(int mr) {
+  if (adj_.mr >= mr) return;
+  const int64_t N = n_ + m_;
+  adj_.mr = mr;
+  adj_.V = A.alloc<double>((size_t)(mr + 1) * N);
+  if (!adj_.g) {
+    adj_.g = A.alloc<double>(N);
+    adj_.u = A.alloc<double>(N);
+    adj_.Au = A.alloc<double>(N);
+    for (double** v : {&adj_.a, &adj_.xp, &adj_.tt, &adj_.tq, &adj_.tr, &adj_.ttr, &adj_.Tx}) *v = A.alloc<double>(n_);
+    for (double** v : {&adj_.b, &adj_.tw, &adj_.tsw, &adj_.ts, &adj_.Sy}) *v = A.alloc<double>(m_);
+    adj_.dG = A.alloc<double>(nnz_);
+    adj_.mask = A.alloc<uint8_t>(K_);
+  }
+  for (double** v : {&adj_.coef, &adj_.dots1, &adj_.dots2, &adj_.dotsn}) *v = A.alloc<double>((size_t)K_ * (mr + 1));
+}
+
+// out = (I - M') u on the masked instances
+void BatchSolver::apply_AT(const double* u, double* out, const uint8_t* mask) {
+  auto cta = [](int64_t v) { return (int)std::max<int64_t>(1, std::min<int64_t>(v, 148 * 8)); };
+  const int wy = YA_.nwc ? cta((YA_.nwc + kWarps - 1) / kWarps) : 0;
+  const int wx = XA_.nwc ? cta((XA_.nwc + kWarps - 1) / kWarps) : 0;
+  jac_kernel<<<std::max(1, YA_.ctaA + wy + YA_.ctaC), kThreads, 0, s_>>>(YA_, wy, adj_.b, u + n_, adj_.tw, iy_, mask);
+  adj_mul_kernel<<<grid_for(m_), kThreads, 0, s_>>>(m_, adj_.Sy, adj_.tw, adj_.tsw);
+  spmv_masked(Gtraw_, adj_.tsw, adj_.tt, mask);
+  adj_q_kernel<<<grid_for(n_), kThreads, 0, s_>>>(n_, ix_, mask, u, adj_.tt, adj_.tq);
+  jac_kernel<<<std::max(1, XA_.ctaA + wx + XA_.ctaC), kThreads, 0, s_>>>(XA_, wx, adj_.a, adj_.tq, adj_.tr, ix_, mask);
+  adj_mul_kernel<<<grid_for(n_), kThreads, 0, s_>>>(n_, adj_.Tx, adj_.tr, adj_.ttr);
+  spmv_masked(Graw_, adj_.ttr, adj_.ts, mask);
+  adj_finish_kernel<<<grid_for(n_ + m_), kThreads, 0, s_>>>(n_, m_, ix_, iy_, mask, u, adj_.tr, adj_.tt, adj_.tw,
+                                                           adj_.ts, out);
+  kernels_ += 6;
+}
+
+int BatchSolver::grad(const double* const* dldx, const double* const* dldy, double* const* dc, double* const* dh,
+                      double* const* dG, double* const* dl, double* const* du, const pdcs_grad_options& go,
+                      pdcs_grad_info* info) {
+  if (!O.differentiable || !solved_) return PDCS_ERR_INVALID;
+  const double t0 = now_s();
+  const int mr = std::max(2, std::min(go.restart > 0 ? go.restart : 100, 200));
+  const double tol = go.rel_tol > 0 ? go.rel_tol : 1e-10;
+  const int64_t maxit = go.max_iter > 0 ? go.max_iter : 5000;
+  setup_adjoint(mr);
+  const int64_t N = n_ + m_, K = K_;
+  const int ld = adj_.mr + 1;
+  // block-constant Pock-Chambolle steps: T = 0.9 / column sums, S = 0.9 / row sums of |G|
+  row_absstat_kernel<true><<<warp_grid(m_), kThreads, 0, s_>>>(m_, Graw_.rp, Graw_.v, nullptr, adj_.Sy);
+  row_absstat_kernel<true><<<warp_grid(n_), kThreads, 0, s_>>>(n_, Gtraw_.rp, Gtraw_.v, nullptr, adj_.Tx);
+  adj_steps_kernel<<<grid_for(m_), kThreads, 0, s_>>>(m_, adj_.Sy);
+  adj_steps_kernel<<<grid_for(n_), kThreads, 0, s_>>>(n_, adj_.Tx);
+  adj_block_min_kernel<<<grid_for(std::max(n_, m_)), kThreads, 0, s_>>>(XA_, adj_.Tx);
+  adj_block_min_kernel<<<grid_for(std::max(n_, m_)), kThreads, 0, s_>>>(YA_, adj_.Sy);
+  // projection points a = x + T (G'y - c), b = y - S (G (2 P_X(a) - x) - h)
+  spmv(Gtraw_, ys_raw_, adj_.tt);
+  adj_point_kernel<<<grid_for(n_), kThreads, 0, s_>>>(n_, adj_.Tx, xs_raw_, adj_.tt, c_raw, 1.0, adj_.a);
+  OpAxpyProj px{adj_.a, adj_.a, 0.0, adj_.xp, nullptr, nullptr};
+  update_project(px, XA_, part_a);
+  axpby_kernel<<<grid_for(n_), kThreads, 0, s_>>>(adj_.tq, 2.0, adj_.xp, -1.0, xs_raw_, n_);
+  spmv(Graw_, adj_.tq, adj_.ts);
+  adj_point_kernel<<<grid_for(m_), kThreads, 0, s_>>>(m_, adj_.Sy, ys_raw_, adj_.ts, h_raw, -1.0, adj_.b);
+  kernels_ += 9;
+  // right-hand side g = (dL/dx*, dL/dy*) in the merged layout
+  {
+    std::vector<double> hg(N, 0.0);
+    for (int64_t k = 0; k < K; ++k)
+      for (int t = 0; t < kMaxRuns; ++t) {
+        if (dldx && dldx[k])
+          std::memcpy(hg.data() + xrun_start_[k * kMaxRuns + t], dldx[k] + xloc_[k * kMaxRuns + t],
+                      sizeof(double) * xrun_len_[k * kMaxRuns + t]);
+        if (dldy && dldy[k])
+          std::memcpy(hg.data() + n_ + yrun_start_[k * kMaxRuns + t], dldy[k] + yloc_[k * kMaxRuns + t],
+                      sizeof(double) * yrun_len_[k * kMaxRuns + t]);
+      }
+    PDCS_CUDA(cudaMemcpyAsync(adj_.g, hg.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s_));
+    PDCS_CUDA(cudaMemsetAsync(adj_.u, 0, sizeof(double) * N, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+  }
+  const int dgrid = (int)std::max<int64_t>(1, std::min<int64_t>(K, 148 * 8));  // a CTA per instance
+  // per-instance dot products <V_p, w>, p < np, into out (device; no synchronisation)
+  auto dots = [&](const uint8_t* mask, const double* V, int np, const double* w, double* out) {
+    for (int q = 0; q < np; q += 8) {
+      adj_dots_kernel<<<dgrid, kThreads, 0, s_>>>(K, mask, rx_, ry_, n_, V, N, q, std::min(8, np - q), w, out, ld);
+      kernels_++;
+    }
+  };
+  auto fetch = [&](const double* dev) {
+    double* h = stage<double>((size_t)K * ld);
+    PDCS_CUDA(cudaMemcpyAsync(h, dev, sizeof(double) * K * ld, cudaMemcpyDeviceToHost, s_));
+    return h;
+  };
+  auto upload_mask8 = [&](const std::vector<uint8_t>& act) {
+    uint8_t* h = stage<uint8_t>(K);
+    std::memcpy(h, act.data(), K);
+    PDCS_CUDA(cudaMemcpyAsync(adj_.mask, h, K, cudaMemcpyHostToDevice, s_));
+  };
+  auto any = [](const std::vector<uint8_t>& v) { return std::any_of(v.begin(), v.end(), [](uint8_t b) { return b; }); };
+  std::vector<double> beta0(K), res(K, 0.0);
+  std::vector<int64_t> iters(K, 0);
+  std::vector<uint8_t> conv(K, 0);
+  {
+    dots(nullptr, adj_.g, 1, adj_.g, adj_.dotsn);
+    const double* h = fetch(adj_.dotsn);
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    for (int64_t k = 0; k < K; ++k) {
+      beta0[k] = std::sqrt(h[k * ld]);
+      conv[k] = beta0[k] > 0 ? 0 : 1;
+    }
+  }
+  // restarted GMRES: one Arnoldi process per instance, all instances per launch;
+  // classical Gram-Schmidt twice with the coefficients kept on the device
+  std::vector<double> Hh((size_t)K * (mr + 1) * mr), cs((size_t)K * mr), sn((size_t)K * mr), gam((size_t)K * (mr + 1));
+  std::vector<int> jk(K);
+  std::vector<double> coef((size_t)K * ld);
+  auto Hc = [&](int64_t k, int i, int j) -> double& { return Hh[((size_t)k * (mr + 1) + i) * mr + j]; };
+  double* V = adj_.V;
+  int64_t total_it = 0;
+  bool first = true;
+  while (total_it < maxit) {
+    std::vector<uint8_t> run(K);
+    for (int64_t k = 0; k < K; ++k) run[k] = !conv[k];
+    if (!any(run)) break;
+    upload_mask8(run);
+    if (first) {
+      copy(V, adj_.g, N);
+    } else {  // V_0 = g - A u
+      apply_AT(adj_.u, adj_.Au, adj_.mask);
+      axpby_kernel<<<grid_for(N), kThreads, 0, s_>>>(V, 1.0, adj_.g, -1.0, adj_.Au, N);
+      kernels_++;
+    }
+    first = false;
+    dots(adj_.mask, V, 1, V, adj_.dotsn);
+    const double* hb = fetch(adj_.dotsn);
+    adj_normalize_kernel<<<grid_for(N), kThreads, 0, s_>>>(N, n_, ix_, iy_, adj_.mask, adj_.dotsn, ld, V);
+    kernels_++;
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    for (int64_t k = 0; k < K; ++k) {
+      if (!run[k]) continue;
+      const double beta = std::sqrt(hb[k * ld]);
+      res[k] = beta / beta0[k];
+      jk[k] = 0;
+      if (beta <= tol * beta0[k]) {
+        conv[k] = 1;
+        run[k] = 0;
+        continue;
+      }
+      gam[(size_t)k * (mr + 1)] = beta;
+      for (int i = 1; i <= mr; ++i) gam[(size_t)k * (mr + 1) + i] = 0.0;
+    }
+    if (!any(run)) break;
+    std::vector<uint8_t> arn = run;  // instances still extending their Krylov basis this cycle
+    for (int j = 0; j < mr && total_it < maxit; ++j) {
+      if (!any(arn)) break;
+      upload_mask8(arn);
+      double* W = V + (size_t)(j + 1) * N;
+      apply_AT(V + (size_t)j * N, W, adj_.mask);
+      dots(adj_.mask, V, j + 1, W, adj_.dots1);
+      adj_combine_kernel<<<grid_for(N), kThreads, 0, s_>>>(N, n_, ix_, iy_, adj_.mask, V, N, j + 1, adj_.dots1, ld,
+                                                          -1.0, W);
+      dots(adj_.mask, V, j + 1, W, adj_.dots2);
+      adj_combine_kernel<<<grid_for(N), kThreads, 0, s_>>>(N, n_, ix_, iy_, adj_.mask, V, N, j + 1, adj_.dots2, ld,
+                                                          -1.0, W);
+      dots(adj_.mask, W, 1, W, adj_.dotsn);
+      adj_normalize_kernel<<<grid_for(N), kThreads, 0, s_>>>(N, n_, ix_, iy_, adj_.mask, adj_.dotsn, ld, W);
+      kernels_ += 3;
+      const double* h1 = fetch(adj_.dots1);
+      const double* h2 = fetch(adj_.dots2);
+      const double* hn = fetch(adj_.dotsn);
+      PDCS_CUDA(cudaStreamSynchronize(s_));
+      total_it++;
+      for (int64_t k = 0; k < K; ++k) {
+        if (!arn[k]) continue;
+        const double hnk = std::sqrt(hn[k * ld]);
+        for (int i = 0; i <= j; ++i) Hc(k, i, j) = h1[k * ld + i] + h2[k * ld + i];
+        Hc(k, j + 1, j) = hnk;
+        // previous rotations, then a new one that zeroes H(j+1, j)
+        for (int i = 0; i < j; ++i) {
+          const double a0 = Hc(k, i, j), a1 = Hc(k, i + 1, j);
+          Hc(k, i, j) = cs[k * mr + i] * a0 + sn[k * mr + i] * a1;
+          Hc(k, i + 1, j) = -sn[k * mr + i] * a0 + cs[k * mr + i] * a1;
+        }
+        const double a0 = Hc(k, j, j), a1 = Hc(k, j + 1, j);
+        const double rr = std::hypot(a0, a1);
+        const double c = rr > 0 ? a0 / rr : 1.0, sv = rr > 0 ? a1 / rr : 0.0;
+        cs[k * mr + j] = c;
+        sn[k * mr + j] = sv;
+        Hc(k, j, j) = rr;
+        Hc(k, j + 1, j) = 0.0;
+        double& gj = gam[(size_t)k * (mr + 1) + j];
+        gam[(size_t)k * (mr + 1) + j + 1] = -sv * gj;
+        gj = c * gj;
+        jk[k] = j + 1;
+        iters[k]++;
+        res[k] = std::fabs(gam[(size_t)k * (mr + 1) + j + 1]) / beta0[k];
+        if (res[k] <= tol || hnk <= 1e-300) arn[k] = 0;  // converged (or breakdown: exact solution)
+      }
+    }
+    // u += V y, y = H^{-1} gamma (back substitution per instance)
+    std::fill(coef.begin(), coef.end(), 0.0);
+    int jmax = 0;
+    for (int64_t k = 0; k < K; ++k) {
+      if (!run[k] || jk[k] == 0) continue;
+      const int J = jk[k];
+      jmax = std::max(jmax, J);
+      for (int i = J - 1; i >= 0; --i) {
+        double v = gam[(size_t)k * (mr + 1) + i];
+        for (int q = i + 1; q < J; ++q) v -= Hc(k, i, q) * coef[k * ld + q];
+        coef[k * ld + i] = v / Hc(k, i, i);
+      }
+    }
+    if (jmax > 0) {
+      upload_mask8(run);
+      double* h = stage<double>((size_t)K * ld);
+      std::memcpy(h, coef.data(), sizeof(double) * K * ld);
+      PDCS_CUDA(cudaMemcpyAsync(adj_.coef, h, sizeof(double) * K * ld, cudaMemcpyHostToDevice, s_));
+      adj_combine_kernel<<<grid_for(N), kThreads, 0, s_>>>(N, n_, ix_, iy_, adj_.mask, V, N, jmax, adj_.coef, ld, 1.0,
+                                                          adj_.u);
+      kernels_++;
+    }
+  }
+  // true relative residuals |g - A u| / |g|
+  {
+    std::vector<uint8_t> all(K, 1);
+    upload_mask8(all);
+    apply_AT(adj_.u, adj_.Au, adj_.mask);
+    axpby_kernel<<<grid_for(N), kThreads, 0, s_>>>(adj_.Au, 1.0, adj_.g, -1.0, adj_.Au, N);
+    kernels_++;
+    dots(nullptr, adj_.Au, 1, adj_.Au, adj_.dotsn);
+    const double* h = fetch(adj_.dotsn);
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    for (int64_t k = 0; k < K; ++k) res[k] = beta0[k] > 0 ? std::sqrt(h[k * ld]) / beta0[k] : 0.0;
+  }
+  // parameter gradients: w = D_K u_y, t = G' (S w), q = u_x - 2 t, r = D_X q
+  {
+    std::vector<uint8_t> all(K, 1);
+    upload_mask8(all);
+    apply_AT(adj_.u, adj_.Au, adj_.mask);  // leaves w (tw), q (tq), r (tr) of u in the work vectors
+    // outputs in the Krylov basis storage (no longer needed; (mr + 1) N >= 3 N entries):
+    // dh over y at V, dc over x then dl, du over the box part at V + N
+    double* dhv = adj_.V;
+    double* dcv = adj_.V + N;
+    double* dlv = dcv + n_;
+    double* duv = dcv + n_ + nb_;
+    adj_dc_kernel<<<grid_for(n_), kThreads, 0, s_>>>(n_, nb_, adj_.Tx, adj_.tr, adj_.tq, adj_.a, bl_raw_, bu_raw_,
+                                                     dcv, dlv, duv);
+    adj_mul_kernel<<<grid_for(m_), kThreads, 0, s_>>>(m_, adj_.Sy, adj_.tw, dhv);
+    adj_dG_kernel<<<warp_grid(m_), kThreads, 0, s_>>>(m_, Graw_.rp, Graw_.ci, adj_.Tx, adj_.Sy, ys_raw_, adj_.tw,
+                                                      xs_raw_, adj_.tr, adj_.dG);
+    kernels_ += 3;
+    std::vector<double> hdc(n_ + 2 * nb_), hdh(m_), hdG(dG ? nnz_ : 0);
+    PDCS_CUDA(cudaMemcpyAsync(hdc.data(), dcv, sizeof(double) * (n_ + 2 * nb_), cudaMemcpyDeviceToHost, s_));
+    PDCS_CUDA(cudaMemcpyAsync(hdh.data(), dhv, sizeof(double) * m_, cudaMemcpyDeviceToHost, s_));
+    if (dG) PDCS_CUDA(cudaMemcpyAsync(hdG.data(), adj_.dG, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    scatter_x(hdc.data(), dc);
+    scatter_y(hdh.data(), dh);
+    for (int64_t k = 0; k < K; ++k) {
+      const int64_t b0 = xrun_start_[k * kMaxRuns], nb = xrun_len_[k * kMaxRuns];
+      if (dl && dl[k]) std::memcpy(dl[k], hdc.data() + n_ + b0, sizeof(double) * nb);
+      if (du && du[k]) std::memcpy(du[k], hdc.data() + n_ + nb_ + b0, sizeof(double) * nb);
+      if (dG && dG[k]) {  // merged entries keep each row's order: copy row by row
+        const pdcs_problem& q = probs_[k];
+        for (int64_t i = 0; i < q.m; ++i)
+          std::memcpy(dG[k] + q.G_rowptr[i], hdG.data() + h_rp_[merged_row(k, i)],
+                      sizeof(double) * (q.G_rowptr[i + 1] - q.G_rowptr[i]));
+      }
+    }
+  }
+  const double t1 = now_s();
+  if (info)
+    for (int64_t k = 0; k < K; ++k) {
+      info[k].iterations = iters[k];
+      info[k].residual = res[k];
+      info[k].time = t1 - t0;
+      info[k].converged = res[k] <= std::max(10 * tol, 1e-8) ? 1 : 0;
+    }
   return PDCS_OK;
 }
 

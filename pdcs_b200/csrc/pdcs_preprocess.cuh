@@ -144,6 +144,13 @@ __global__ void fill_kernel(double* a, double v, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) a[i] = v;
 }
 
+// dst[q] = src[idx[q]]
+__global__ void gather_kernel(double* __restrict__ dst, const double* __restrict__ src,
+                              const int32_t* __restrict__ idx, int64_t n) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) dst[q] = src[idx[q]];
+}
+
 __global__ void mul_kernel(double* a, const double* b, int64_t n) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) a[i] *= b[i];

@@ -434,6 +434,9 @@ class Solver {
   float *dx32_ = nullptr, *dxl32_ = nullptr, *dy32_ = nullptr, *dyl32_ = nullptr;
   float *aty32_ = nullptr, *gx32_ = nullptr, *gxl32_ = nullptr;
   double *xa_ = nullptr, *ya_ = nullptr, *qa_ = nullptr, *ra_ = nullptr, *dxm_ = nullptr, *dym_ = nullptr;
+  // differentiable mode: the unscaled data the solution-map adjoint works on
+  CsrDev Graw_{}, Gtraw_{};
+  double *bl_raw_ = nullptr, *bu_raw_ = nullptr;
   double *part_x = nullptr, *part_y = nullptr, *part_r = nullptr, *red_out = nullptr;
   double *part_a = nullptr, *part_b = nullptr;  // partials of host-driven (non-graph) reductions
   PdhgState* st_dev = nullptr;
@@ -919,6 +922,8 @@ void Solver::setup() {
   h_raw = A.alloc<double>(m_);
   double* bl_raw = A.alloc<double>(nb_);
   double* bu_raw = A.alloc<double>(nb_);
+  bl_raw_ = bl_raw;
+  bu_raw_ = bu_raw;
   const cudaMemcpyKind kind = P.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   auto put = [&](void* dst, const void* src, size_t bytes) {
     if (bytes) PDCS_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, s_));
@@ -991,6 +996,11 @@ void Solver::setup() {
   copy(h_s, h_raw, m_);
   copy(bl_s, bl_raw, nb_);
   copy(bu_s, bu_raw, nb_);
+  double* g_v_raw = nullptr;
+  if (O.differentiable) {  // the adjoint differentiates the unscaled problem
+    g_v_raw = A.alloc<double>(nnz_);
+    copy(g_v_raw, g_v, nnz_);
+  }
   fill_kernel<<<grid_for(n_), kThreads, 0, s_>>>(Dr, 1.0, n_);
   fill_kernel<<<grid_for(m_), kThreads, 0, s_>>>(Dl, 1.0, m_);
   double* var = A.alloc<double>(n_);
@@ -1054,6 +1064,14 @@ void Solver::setup() {
   // ---- SpMV schedules: autotuned per matrix unless fixed by the options ----
   lane_G_ = tune_bins(rp_h, m_, n_, g_rp, g_ci, g_v, G_, inst_of_y_, x, tm[0]);
   lane_Gt_ = tune_bins(trp_h, n_, m_, t_rp, t_ci, t_v, Gt_, inst_of_x_, y, tn[0]);
+  if (O.differentiable) {
+    double* t_v_raw = A.alloc<double>(nnz_);
+    gather_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(t_v_raw, g_v_raw, perm_t, nnz_);
+    Graw_ = G_;
+    Graw_.v = g_v_raw;
+    Gtraw_ = Gt_;
+    Gtraw_.v = t_v_raw;
+  }
   // cone tables
   std::vector<int64_t> soc_x(P.soc_x, P.soc_x + P.n_soc_x), rsoc_x(P.rsoc_x, P.rsoc_x + P.n_rsoc_x);
   std::vector<int64_t> socG(P.socG, P.socG + P.n_socG), rsocG(P.rsocG, P.rsocG + P.n_rsocG);
@@ -1963,6 +1981,57 @@ int pdcs_batch_solve(pdcs_batch* batch, int64_t attempt_limit, pdcs_result* resu
     return PDCS_ERR_CUDA;
   } catch (const std::exception& e) {
     std::fprintf(stderr, "pdcs_batch_solve: %s\n", e.what());
+    return PDCS_ERR_INVALID;
+  }
+}
+
+static pdcs_grad_options grad_defaults(const pdcs_grad_options* g) {
+  pdcs_grad_options o{};
+  if (g) o = *g;
+  if (o.rel_tol <= 0) o.rel_tol = 1e-10;
+  if (o.restart <= 0) o.restart = 100;
+  if (o.max_iter <= 0) o.max_iter = 5000;
+  return o;
+}
+
+int pdcs_batch_grad(pdcs_batch* batch, const double* const* dldx, const double* const* dldy, double* const* dc,
+                    double* const* dh, double* const* dG, double* const* dl, double* const* du,
+                    const pdcs_grad_options* opts, pdcs_grad_info* info) {
+  if (!batch || !batch->solver) return PDCS_ERR_INVALID;
+  try {
+    return batch->solver->grad(dldx, dldy, dc, dh, dG, dl, du, grad_defaults(opts), info);
+  } catch (const pdcs::CudaError& e) {
+    std::fprintf(stderr, "pdcs_batch_grad: %s\n", e.what());
+    return PDCS_ERR_CUDA;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "pdcs_batch_grad: %s\n", e.what());
+    return PDCS_ERR_INVALID;
+  }
+}
+
+int pdcs_grad(const pdcs_problem* prob, const pdcs_options* opts, const double* x, const double* y,
+              const double* dldx, const double* dldy, double* dc, double* dh, double* dG, double* dl, double* du,
+              const pdcs_grad_options* gopts, pdcs_grad_info* info) {
+  if (!prob || !x || !y) return PDCS_ERR_INVALID;
+  pdcs_options o;
+  if (opts) o = *opts;
+  else pdcs_default_options(&o);
+  o.differentiable = 1;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PDCS_ERR_NO_DEVICE;
+  try {
+    pdcs::BatchSolver b(1, prob, &o);
+    int rc = b.prepare();
+    if (rc != PDCS_OK) return rc;
+    b.set_solution(&x, &y);
+    return b.grad(&dldx, &dldy, &dc, &dh, &dG, &dl, &du, grad_defaults(gopts), info);
+  } catch (const pdcs::CudaError& e) {
+    std::fprintf(stderr, "pdcs_grad: %s\n", e.what());
+    return PDCS_ERR_CUDA;
+  } catch (const std::domain_error&) {
+    return PDCS_ERR_BOUNDS;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "pdcs_grad: %s\n", e.what());
     return PDCS_ERR_INVALID;
   }
 }

@@ -245,6 +245,23 @@ def batch_socp_c3(count=4096, seed=20261206, nmin=50, nmax=5000, density=0.02):
     return out
 
 
+def batch_mixed_c4(count=256, seed=20261207, n=2000, m=1500, density=0.01):
+    """Mixed SOC + exponential-cone instances of equal size (the differentiable
+    layer's workload): x = [box 800 | SOC blocks | 200 exp cones], y = [nonneg 300 |
+    SOC blocks | 200 exp cones], each built feasible and bounded like socp_c0."""
+    out = []
+    for k in range(count):
+        r2 = np.random.default_rng(seed + 7919 * k)
+        n_exp, m_exp = n // 10, (2 * m) // 15
+        n_box = (2 * n) // 5
+        soc_x = _random_dims(r2, n - n_box - 3 * n_exp, 3, 10)
+        mn = m // 5
+        socG = _random_dims(r2, m - mn - 3 * m_exp, 3, 10)
+        out.append(random_feasible(n_box=n_box, soc_x=soc_x, exp_x=n_exp, mGnonnegative=mn, socG=socG, expG=m_exp,
+                                   density=density, seed=seed + 7919 * k, name=f"mixed_c4_{k}"))
+    return out
+
+
 def primal_infeasible_lp():
     """x1 + x2 >= 1 and -x1 - x2 >= 0 with x free: no feasible point."""
     G = sp.csr_matrix(np.array([[1.0, 1.0], [-1.0, -1.0], [1.0, 0.0]]))

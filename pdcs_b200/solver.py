@@ -171,7 +171,8 @@ def _options_struct(L, hold: _Holder, *, n=0, m=0, rescaling_method: str = "ruiz
                     method: str = "average", logfile_name: Optional[str] = None, use_kkt_restart: bool = False,
                     kkt_restart_freq: int = 2000, use_duality_gap_restart: bool = True,
                     duality_gap_restart_freq: int = 2000, attempt_limit: int = 0, attempts_per_graph: int = 32,
-                    stream=None, force_resolving: bool = False, precision="fp64", spmv_lane_nnz: int = 0):
+                    stream=None, force_resolving: bool = False, precision="fp64", spmv_lane_nnz: int = 0,
+                    differentiable: bool = False):
     """Fill a PdcsOptions from the reference's keyword arguments (rpdhg_alg_gpu_gen.jl:1219-1268).
 
     precision: "fp64" (the reference's arithmetic) or "fp32" (FP32 matrices and iterate deltas
@@ -220,6 +221,7 @@ def _options_struct(L, hold: _Holder, *, n=0, m=0, rescaling_method: str = "ruiz
     if spmv_lane_nnz not in (0, 1, 2, 4, 8, 16):
         raise ValueError("spmv_lane_nnz must be 0 (autotune) or a power of two up to 16")
     O.spmv_lane_nnz = spmv_lane_nnz
+    O.differentiable = int(differentiable)
     return O
 
 
@@ -312,6 +314,45 @@ class BatchHandle:
         capi.check(rc, "pdcs_batch_solve")
         return [Solution(outs[i][0], outs[i][1], _info(Rs[i])) for i in range(self.count)], _batch_info(B)
 
+    def grad(self, dldx, dldy=None, rel_tol=1e-10, restart=100, max_iter=5000):
+        """Solution-map adjoint at the last solve (the handle must be created with
+        differentiable=True).  dldx / dldy: per-instance loss gradients w.r.t. x*, y*
+        (dldy may be None).  Returns (list of dicts c, h, G, bl, bu -- G in the
+        instance's CSR order with sorted indices --, list of GradInfo)."""
+        if not self._h:
+            raise RuntimeError("batch handle is closed")
+        K = self.count
+        keep = []
+
+        def ptrs(arrays, sizes):
+            out = (C.c_void_p * K)()
+            for i in range(K):
+                a = None if arrays is None else arrays[i]
+                if a is None:
+                    out[i] = None
+                    continue
+                a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+                if a.shape != (sizes[i],):
+                    raise ValueError(f"instance {i}: expected {sizes[i]} values")
+                keep.append(a)
+                out[i] = a.ctypes.data if a.size else None
+            return out
+        ns = [n for n, _ in self.sizes]
+        ms = [m for _, m in self.sizes]
+        nnzs = [P.nnz for P in self._Ps]
+        nbs = [P.nb for P in self._Ps]
+        res = [dict(c=np.zeros(ns[i]), h=np.zeros(ms[i]), G=np.zeros(nnzs[i]), bl=np.zeros(nbs[i]),
+                    bu=np.zeros(nbs[i])) for i in range(K)]
+        outs = {}
+        for key in ("c", "h", "G", "bl", "bu"):
+            outs[key] = (C.c_void_p * K)(*[res[i][key].ctypes.data if res[i][key].size else None for i in range(K)])
+        go = capi.PdcsGradOptions(rel_tol=rel_tol, restart=restart, max_iter=max_iter)
+        infos = (capi.PdcsGradInfo * K)()
+        rc = self._L.pdcs_batch_grad(self._h, ptrs(dldx, ns), ptrs(dldy, ms), outs["c"], outs["h"], outs["G"],
+                                     outs["bl"], outs["bu"], C.byref(go), infos)
+        capi.check(rc, "pdcs_batch_grad")
+        return res, [GradInfo(i.iterations, i.residual, i.time, bool(i.converged)) for i in infos]
+
     def close(self):
         if self._h:
             self._L.pdcs_batch_destroy(self._h)
@@ -328,6 +369,34 @@ class BatchHandle:
             self.close()
         except Exception:
             pass
+
+
+@dataclasses.dataclass
+class GradInfo:
+    iterations: int
+    residual: float
+    time: float
+    converged: bool
+
+
+def rpdhg_gpu_grad(problem, x, y, dldx, dldy=None, rel_tol=1e-10, restart=100, max_iter=5000, **options):
+    """Solution-map adjoint of one problem at the solution (x, y) (pdcs_grad): returns
+    (dict of dL/dc, dL/dh, dL/dG (nonzero values, CSR order with sorted indices), dL/dbl,
+    dL/dbu; GradInfo)."""
+    L = capi.load()
+    hold = _Holder()
+    kw = problem.kwargs() if hasattr(problem, "kwargs") else dict(problem)
+    P = _problem_struct(hold, **{k: v for k, v in kw.items() if k in _PROBLEM_KEYS})
+    O = _options_struct(L, hold, **options)
+    out = dict(c=np.zeros(P.n), h=np.zeros(P.m), G=np.zeros(P.nnz), bl=np.zeros(P.nb), bu=np.zeros(P.nb))
+    ptr = lambda a: a.ctypes.data if a.size else None
+    go = capi.PdcsGradOptions(rel_tol=rel_tol, restart=restart, max_iter=max_iter)
+    info = capi.PdcsGradInfo()
+    rc = L.pdcs_grad(C.byref(P), C.byref(O), hold.f64(x), hold.f64(y), hold.f64(dldx),
+                     None if dldy is None else hold.f64(dldy), ptr(out["c"]), ptr(out["h"]), ptr(out["G"]),
+                     ptr(out["bl"]), ptr(out["bu"]), C.byref(go), C.byref(info))
+    capi.check(rc, "pdcs_grad")
+    return out, GradInfo(info.iterations, info.residual, info.time, bool(info.converged))
 
 
 def _batch_info(B) -> "BatchInfo":
