@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-single", action="store_true", help="skip the single-instance exp-cone section")
+    ap.add_argument("--no-single", action="store_true",
+                    help="skip the single-instance exp-cone and differentiable-layer sections")
     return ap.parse_args()
 
 
@@ -228,6 +229,40 @@ def single_instance_section(dev, stream):
             "exit_status": i.exit_status, "spmv_lane_nnz": list(i.spmv_lane_nnz)}
 
 
+def differentiable_section(dev, stream):
+    """256 mixed SOC + exponential-cone instances (n = 2000, m = 1500, 1% density): the torch
+    conic layer's forward (batched solve) against forward + backward (solution-map adjoint),
+    loss 1/2 |x* - x_target|^2."""
+    import torch
+    from pdcs_b200 import problems
+    from pdcs_b200.autograd import ConicBatchLayer
+    batch = problems.batch_mixed_c4(count=256)
+    layer = ConicBatchLayer(batch, stream=stream.cuda_stream)
+    params = [t.requires_grad_() for t in layer.flat_params(batch)]
+    xt = torch.randn(sum(p.n for p in batch), dtype=torch.float64, generator=torch.Generator().manual_seed(11))
+
+    def step(backward):
+        for t in params:
+            t.grad = None
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x = layer(*params)
+        t1 = time.perf_counter()
+        if backward:
+            (0.5 * ((x - xt) ** 2).sum()).backward()
+        torch.cuda.synchronize()
+        return t1 - t0, time.perf_counter() - t0
+    step(True)
+    fwd = [step(False)[0] for _ in range(2)]
+    both = [step(True)[1] for _ in range(2)]
+    g = params[0].grad
+    return {"workload": "256 mixed SOC + exponential-cone instances, n=2000, m=1500, 1% density, "
+                        "loss 1/2 |x* - x_target|^2 (torch.autograd conic layer, FP64)",
+            "forward_ms": 1e3 * statistics.median(fwd), "forward_backward_ms": 1e3 * statistics.median(both),
+            "backward_over_forward": (statistics.median(both) - statistics.median(fwd)) / statistics.median(fwd),
+            "grad_c_norm": float(g.norm()) if g is not None else None}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -316,17 +351,18 @@ def run_ours(args):
 
     # ---- plain FP64 GPU PDHG, one instance at a time, on a seeded sample ----
     idx = np.random.default_rng(5).choice(units, size=min(args.plain_sample, units), replace=False)
-    timed(stream, lambda: solver.solve_problem(batch[int(idx[0])], stream=stream.cuda_stream))
+    plain_kw = dict(stream=stream.cuda_stream, spmv_lane_nnz=4)  # one fixed SpMV schedule, no tuning
+    timed(stream, lambda: solver.solve_problem(batch[int(idx[0])], **plain_kw))
     plain_t, plain_main, plain_it = 0.0, 0.0, 0
     for i in idx:
-        s, dt = timed(stream, lambda: solver.solve_problem(batch[int(i)], stream=stream.cuda_stream))
+        s, dt = timed(stream, lambda: solver.solve_problem(batch[int(i)], **plain_kw))
         plain_t += dt
         plain_main += s.info.time
         plain_it += s.info.iter
     plain = {"instances_per_s": len(idx) / plain_t, "iter_per_s": plain_it / plain_t,
              "main_loop_instances_per_s": len(idx) / plain_main,
              "sample": f"{len(idx)} seeded instances of the batch, each a full pdcs_solve (FP64, "
-                       "upload + preprocessing + solve)"}
+                       "upload + preprocessing + solve, fixed SpMV schedule)"}
 
     # ---- end to end through the public API from host buffers ----
     e2e = None
@@ -350,6 +386,7 @@ def run_ours(args):
                "optimal": sum(1 for s in sols_h if s.info.exit_status == "optimal")}
 
     single = None if args.no_single or rank != 0 else single_instance_section(dev, stream)
+    layer = None if args.no_single or rank != 0 else differentiable_section(dev, stream)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_batch_rate(batch, args.cpu_seconds)
@@ -367,7 +404,7 @@ def run_ours(args):
                 "plain_fp64": plain, "speedup_vs_plain_fp64": value / plain["instances_per_s"] / world,
                 "spmv_schedule": schedule,
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-                "cpu_baseline": cpu, "single_instance": single}
+                "cpu_baseline": cpu, "single_instance": single, "differentiable_layer": layer}
         print(json.dumps(line), flush=True)
     replicas.finalize(world)
     return 0

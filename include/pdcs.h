@@ -109,7 +109,8 @@ typedef struct {
   int32_t attempts_per_graph;    /* PDHG attempts captured per CUDA graph (default 32) */
   int32_t force_resolving;       /* test hook: enter the resolving fallback at the first outer iteration */
   int32_t spmv_lane_nnz;         /* SpMV schedule, nonzeros per lane of a row's lane group (power of two,
-                                    1..16); 0 (default) = autotuned per matrix at setup */
+                                    1..16); 0 (default) = autotuned per matrix at setup for matrices of
+                                    2^20 or more nonzeros, 4 below */
   int32_t differentiable;        /* keep the unscaled data the solution-map adjoint (pdcs_batch_grad) needs */
 } pdcs_options;
 

@@ -695,6 +695,10 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
   D.rows = d_desc;
 }
 
+// matrices with fewer nonzeros keep the default schedule: timing four candidates
+// costs more than a small solve can gain from the choice
+constexpr int64_t kTuneMinNnz = 1 << 20;
+
 // SpMV schedule autotuner: time each nonzeros-per-lane target on this matrix
 // (CUDA events, best of 3 after a warm-up) and keep the fastest, leaving the
 // default (4) only for a gain of 3% or more; a fixed target (spmv_lane_nnz > 0)
@@ -704,9 +708,10 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
 int Solver::tune_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
                       const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst, const double* xin,
                       double* yout) {
-  if (O.spmv_lane_nnz > 0) {
-    build_bins(rp, rows, cols, d_rp, d_ci, d_v, D, row_inst, O.spmv_lane_nnz);
-    return O.spmv_lane_nnz;
+  if (O.spmv_lane_nnz > 0 || rp[rows] < kTuneMinNnz) {  // fixed, or too small for the search to pay off
+    const int lane = O.spmv_lane_nnz > 0 ? O.spmv_lane_nnz : 4;
+    build_bins(rp, rows, cols, d_rp, d_ci, d_v, D, row_inst, lane);
+    return lane;
   }
   static std::mutex mu;
   static std::map<std::array<uint64_t, 4>, int> chosen;

@@ -116,7 +116,7 @@ def test_spmv_schedules_agree(cuda):
         g = solver.solve_problem(p, attempt_limit=20, spmv_lane_nnz=lane)
         if lane:
             assert g.info.spmv_lane_nnz == (lane, lane)
-        else:
-            assert all(v in (2, 4, 8, 16) for v in g.info.spmv_lane_nnz)
+        else:  # below 2^20 nonzeros the autotuner keeps the default
+            assert g.info.spmv_lane_nnz == (4, 4)
         scale = max(1.0, np.abs(ref.primal).max())
         assert np.abs(g.primal - ref.primal).max() <= 1e-9 * scale, lane
