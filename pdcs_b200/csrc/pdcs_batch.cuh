@@ -894,16 +894,16 @@ void BatchSolver::capture_batch_graph() {
     int32_t* cur = live_cnt_ + (a & 1);
     int32_t* nxt = live_cnt_ + ((a + 1) & 1);
     launch_spmv<1, false, float>(Gt32c_, dyl32_, nullptr, aty32_, nullptr, cur, s_);
-    OpPrimalStep32B op1{xa_, dxl32_, qa_, aty32_, dx32_, x, ix_, live_, ps_, dxsq_};
+    OpPrimalStep32B op1{xa_, dxp32_, qa_, aty32_, x, ix_, live_, ps_, dxsq_};
     launch_update_project(op1, XIg_, part_x, cur, s_);
-    launch_spmv<2, false, float>(G32c_, dx32_, dxl32_, gx32_, gxl32_, cur, s_);
+    launch_spmv<kPair, false, float>(G32c_, &dxp32_->x, nullptr, gx32_, gxl32_, cur, s_);
     OpDualStep32B op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_};
     launch_update_project(op2, YIg_, part_y, cur, s_);
     BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,
                  dgdy_, cur,  nxt,     done_ctas_, live_cnt_ + 2, act_inst_, n_act_};
     batch_control_kernel<<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
-    batch_reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dx32_, dxl32_, dxm_, dy32_,
-                                                               dyl32_, dym_, rchunk_, n_rchunk_);
+    batch_reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dxp32_, dxm_, dy32_, dyl32_,
+                                                               dym_, rchunk_, n_rchunk_);
   }
   for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
     int32_t* cur = live_cnt_ + (a & 1);

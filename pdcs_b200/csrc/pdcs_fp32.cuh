@@ -3,6 +3,8 @@
 // Between two refinements the iterates are stored as FP32 deltas from FP64
 // anchors:
 //   x = xa + dx,  x_lag = xa + dxl,  x_avg = xa + dxm (dxm in FP64)
+// with dx and dxl interleaved in one array of float2 pairs {dx, dxl}, so the
+// SpMV of the pair (G dx, G dxl) gathers 8 bytes per nonzero in one load
 //   y = ya + dy,  y_lag = ya + dyl,  y_avg = ya + dym
 // and the per-anchor products are precomputed in FP64:
 //   qa = G' ya - c,   ra = G xa - h.
@@ -27,19 +29,18 @@ struct OpPrimalStep32 {
   static constexpr bool kFusedControl = false;
   __device__ static const int32_t* kinds() { return kSum1; }
   const double* xa;
-  const float* dxl;
+  float2* dxp;  // {dx, dxl}
   const double* qa;
   const float* aty;
-  float* dx;
   double* out;  // FP64 scratch of the large-SOC path
   const PdhgState* st;
   double ps;
   __device__ void load() { ps = st->ps; }
-  __device__ double z(int64_t j) const { return xa[j] + (double)dxl[j] + ps * (qa[j] + (double)aty[j]); }
+  __device__ double z(int64_t j) const { return xa[j] + (double)dxp[j].y + ps * (qa[j] + (double)aty[j]); }
   __device__ void fin(int64_t j, double, double p, double* acc) const {
     const float d = (float)(p - xa[j]);
-    dx[j] = d;
-    const double s = (double)d - (double)dxl[j];
+    dxp[j].x = d;
+    const double s = (double)d - (double)dxp[j].y;
     acc[0] = fma(s, s, acc[0]);
   }
 };
@@ -81,10 +82,9 @@ struct OpPrimalStep32B {
   static constexpr bool kFusedControl = false;
   __device__ static const int32_t* kinds() { return kSum1; }
   const double* xa;
-  const float* dxl;
+  float2* dxp;  // {dx, dxl}
   const double* qa;
   const float* aty;
-  float* dx;
   double* out;
   const int32_t* inst;
   const uint8_t* mask;
@@ -93,12 +93,12 @@ struct OpPrimalStep32B {
   __device__ void load() {}
   __device__ bool live(int64_t j) const { return mask[inst[j]] != 0; }
   __device__ double z(int64_t j) const {
-    return xa[j] + (double)dxl[j] + ps[inst[j]] * (qa[j] + (double)aty[j]);
+    return xa[j] + (double)dxp[j].y + ps[inst[j]] * (qa[j] + (double)aty[j]);
   }
   __device__ void fin(int64_t j, double, double p, double*) const {
     const float d = (float)(p - xa[j]);
-    dx[j] = d;
-    const double s = (double)d - (double)dxl[j];
+    dxp[j].x = d;
+    const double s = (double)d - (double)dxp[j].y;
     dxsq[j] = s * s;
   }
 };
@@ -133,27 +133,37 @@ struct OpDualStep32B {
   }
 };
 
-// Reflection + averaging on the deltas (the anchor cancels: tmp + inv = 1).
-__device__ __forceinline__ void reflect32_elem(const PdhgState& s, float* d, float* dl, double* dm, int64_t j) {
+// Reflection + averaging on the deltas (the anchor cancels: tmp + inv = 1):
+// returns the new delta of both the iterate and its lag.
+__device__ __forceinline__ float reflect32_value(const PdhgState& s, float d, float dl, double& dm) {
   const double tmp = s.refl_tmp, inv = s.refl_inv, e = s.refl_extra, eta = s.refl_eta, cum = s.refl_cum;
-  const double cur = (double)d[j];
-  const float nv = (float)(tmp * ((1.0 + e) * cur - e * (double)dl[j]) + inv * cur);
-  dm[j] = (dm[j] * cum + (double)nv * eta) / (cum + eta);
-  d[j] = nv;
-  dl[j] = nv;
+  const double cur = (double)d;
+  const float nv = (float)(tmp * ((1.0 + e) * cur - e * (double)dl) + inv * cur);
+  dm = (dm * cum + (double)nv * eta) / (cum + eta);
+  return nv;
+}
+__device__ __forceinline__ void reflect32_x(const PdhgState& s, float2* dxp, double* dxm, int64_t j) {
+  const float2 p = dxp[j];
+  const float nv = reflect32_value(s, p.x, p.y, dxm[j]);
+  dxp[j] = make_float2(nv, nv);
+}
+__device__ __forceinline__ void reflect32_y(const PdhgState& s, float* dy, float* dyl, double* dym, int64_t i) {
+  const float nv = reflect32_value(s, dy[i], dyl[i], dym[i]);
+  dy[i] = nv;
+  dyl[i] = nv;
 }
 
 __global__ void __launch_bounds__(kThreads) reflect32_kernel(const PdhgState* __restrict__ st,
-                                                            float* __restrict__ dx, float* __restrict__ dxl,
-                                                            double* __restrict__ dxm, int64_t n,
+                                                            float2* __restrict__ dxp, double* __restrict__ dxm,
+                                                            int64_t n,
                                                             float* __restrict__ dy, float* __restrict__ dyl,
                                                             double* __restrict__ dym, int64_t m) {
   if (!st->do_reflect) return;
   const PdhgState s = *st;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n + m; i += stride) {
-    if (i < n) reflect32_elem(s, dx, dxl, dxm, i);
-    else reflect32_elem(s, dy, dyl, dym, i - n);
+    if (i < n) reflect32_x(s, dxp, dxm, i);
+    else reflect32_y(s, dy, dyl, dym, i - n);
   }
 }
 
@@ -162,7 +172,7 @@ __global__ void __launch_bounds__(kThreads) batch_reflect32_kernel(const int32_t
                                                                   const PdhgState* __restrict__ sts,
                                                                   const int32_t* __restrict__ ix,
                                                                   const int32_t* __restrict__ iy,
-                                                                  float* __restrict__ dx, float* __restrict__ dxl,
+                                                                  float2* __restrict__ dxp,
                                                                   double* __restrict__ dxm, float* __restrict__ dy,
                                                                   float* __restrict__ dyl, double* __restrict__ dym,
                                                                   const int4* __restrict__ rchunk,
@@ -176,23 +186,24 @@ __global__ void __launch_bounds__(kThreads) batch_reflect32_kernel(const int32_t
     const int64_t j = (int64_t)ch.x + threadIdx.x;
     const PdhgState& s = sts[isx ? ix[j] : iy[j]];
     if (!s.do_reflect) continue;
-    if (isx) reflect32_elem(s, dx, dxl, dxm, j);
-    else reflect32_elem(s, dy, dyl, dym, j);
+    if (isx) reflect32_x(s, dxp, dxm, j);
+    else reflect32_y(s, dy, dyl, dym, j);
   }
 }
 
-// anchor: va = v, d = 0, dl = vl - v, dm = vm - v (elements of masked instances; mask NULL = all)
+// anchor: va = v, d = 0, dl = vl - v, dm = vm - v (elements of masked instances; mask NULL = all).
+// d and dl are read at stride ds (2: the interleaved {dx, dxl} pairs).
 __global__ void anchor_kernel(const double* __restrict__ v, const double* __restrict__ vl,
                               const double* __restrict__ vm, double* __restrict__ va, float* __restrict__ d,
-                              float* __restrict__ dl, double* __restrict__ dm, const int32_t* __restrict__ inst,
-                              const uint8_t* __restrict__ mask, int64_t len) {
+                              float* __restrict__ dl, int ds, double* __restrict__ dm,
+                              const int32_t* __restrict__ inst, const uint8_t* __restrict__ mask, int64_t len) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride) {
     if (mask && !mask[inst[i]]) continue;
     const double a = v[i];
     va[i] = a;
-    d[i] = 0.0f;
-    dl[i] = (float)(vl[i] - a);
+    d[i * ds] = 0.0f;
+    dl[i * ds] = (float)(vl[i] - a);
     dm[i] = vm[i] - a;
   }
 }
@@ -200,15 +211,15 @@ __global__ void anchor_kernel(const double* __restrict__ v, const double* __rest
 // materialize: v = va + d, vl = va + dl, vm = va + dm
 __global__ void materialize_kernel(double* __restrict__ v, double* __restrict__ vl, double* __restrict__ vm,
                                    const double* __restrict__ va, const float* __restrict__ d,
-                                   const float* __restrict__ dl, const double* __restrict__ dm,
+                                   const float* __restrict__ dl, int ds, const double* __restrict__ dm,
                                    const int32_t* __restrict__ inst, const uint8_t* __restrict__ mask,
                                    int64_t len) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += stride) {
     if (mask && !mask[inst[i]]) continue;
     const double a = va[i];
-    v[i] = a + (double)d[i];
-    vl[i] = a + (double)dl[i];
+    v[i] = a + (double)d[i * ds];
+    vl[i] = a + (double)dl[i * ds];
     vm[i] = a + dm[i];
   }
 }

@@ -126,6 +126,27 @@ struct RowAcc {
   }
 };
 
+// Vectors of one SpMV pass (NV): 1 (x0), 2 (x0 and x1, two arrays) or kPair
+// (x0 holds the two vectors interleaved, x0[2 c] and x0[2 c + 1]: one gather
+// of 2 T per nonzero instead of two gathers of T).
+constexpr int kPair = 3;
+template <class T> struct Vec2T;
+template <> struct Vec2T<float> { using type = float2; };
+template <> struct Vec2T<double> { using type = double2; };
+
+template <int NV, class T>
+__device__ __forceinline__ void spmv_gather(const T* __restrict__ x0, const T* __restrict__ x1, int32_t c, T& a,
+                                            T& b) {
+  if constexpr (NV == kPair) {
+    const auto v = reinterpret_cast<const typename Vec2T<T>::type*>(x0)[c];
+    a = v.x;
+    b = v.y;
+  } else {
+    a = x0[c];
+    b = NV == 2 ? x1[c] : T(0);
+  }
+}
+
 // MASK: rows whose instance (rows[q].w) has imask == 0 are skipped (batched solver).
 // LN = A.lane_nnz: a lane holds at most LN nonzeros of its row in bins 0..5, so
 // all of a lane's value / index loads are issued together, then all its gathers.
@@ -176,19 +197,21 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
 #pragma unroll
       for (int u = 0; u < LN; ++u) {
         if (cv[u] >= 0) {
-          p0[u & 3] = fma(av[u], x0[cv[u]], p0[u & 3]);
-          if (NV == 2) p1[u & 3] = fma(av[u], x1[cv[u]], p1[u & 3]);
+          T a, b;
+          spmv_gather<NV>(x0, x1, cv[u], a, b);
+          p0[u & 3] = fma(av[u], a, p0[u & 3]);
+          if (NV >= 2) p1[u & 3] = fma(av[u], b, p1[u & 3]);
         }
       }
       T s0 = (p0[0] + p0[1]) + (p0[2] + p0[3]);
       T s1 = (p1[0] + p1[1]) + (p1[2] + p1[3]);
       for (int o = g >> 1; o > 0; o >>= 1) {
         s0 += __shfl_down_sync(kFull, s0, o, g);
-        if (NV == 2) s1 += __shfl_down_sync(kFull, s1, o, g);
+        if (NV >= 2) s1 += __shfl_down_sync(kFull, s1, o, g);
       }
       if (valid && lane_g == 0) {
         y0[row] = s0;
-        if (NV == 2) y1[row] = s1;
+        if (NV >= 2) y1[row] = s1;
       }
     }
   } else {
@@ -201,15 +224,16 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
       RowAcc<T> a0, a1;
       for (int32_t k = kb + threadIdx.x; k < ke; k += kThreads) {
         const T a = A.v[k];
-        const int32_t col = A.ci[k];
-        a0.add(a * x0[col]);
-        if (NV == 2) a1.add(a * x1[col]);
+        T u0, u1;
+        spmv_gather<NV>(x0, x1, A.ci[k], u0, u1);
+        a0.add(a * u0);
+        if (NV >= 2) a1.add(a * u1);
       }
       T s0 = a0.s, s1 = a1.s;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         s0 += __shfl_down_sync(kFull, s0, o);
-        if (NV == 2) s1 += __shfl_down_sync(kFull, s1, o);
+        if (NV >= 2) s1 += __shfl_down_sync(kFull, s1, o);
       }
       const int w = threadIdx.x >> 5;
       if ((threadIdx.x & 31) == 0) {
@@ -224,7 +248,7 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
           t1.add(red1[i]);
         }
         y0[row] = t0.s;
-        if (NV == 2) y1[row] = t1.s;
+        if (NV >= 2) y1[row] = t1.s;
       }
       __syncthreads();
     }

@@ -431,7 +431,8 @@ class Solver {
   // FP32-bulk mode (precision 1): FP32 matrices and deltas, FP64 anchors and averages
   bool fp32_ = false;
   CsrT<float> G32_{}, Gt32_{};
-  float *dx32_ = nullptr, *dxl32_ = nullptr, *dy32_ = nullptr, *dyl32_ = nullptr;
+  float2* dxp32_ = nullptr;  // {dx, dxl} pairs
+  float *dy32_ = nullptr, *dyl32_ = nullptr;
   float *aty32_ = nullptr, *gx32_ = nullptr, *gxl32_ = nullptr;
   double *xa_ = nullptr, *ya_ = nullptr, *qa_ = nullptr, *ra_ = nullptr, *dxm_ = nullptr, *dym_ = nullptr;
   // differentiable mode: the unscaled data the solution-map adjoint works on
@@ -1121,8 +1122,7 @@ void Solver::setup_fp32() {
   };
   G32_ = narrow(G_, gv);
   Gt32_ = narrow(Gt_, tv);
-  dx32_ = A.alloc<float>(n_);
-  dxl32_ = A.alloc<float>(n_);
+  dxp32_ = A.alloc<float2>(n_);
   aty32_ = A.alloc<float>(n_);
   dy32_ = A.alloc<float>(m_);
   dyl32_ = A.alloc<float>(m_);
@@ -1137,8 +1137,8 @@ void Solver::setup_fp32() {
 }
 
 void Solver::anchor(const int32_t* ix, const int32_t* iy, const uint8_t* mask) {
-  anchor_kernel<<<grid_for(n_), kThreads, 0, s_>>>(x, xl, xm, xa_, dx32_, dxl32_, dxm_, ix, mask, n_);
-  anchor_kernel<<<grid_for(m_), kThreads, 0, s_>>>(y, yl, ym, ya_, dy32_, dyl32_, dym_, iy, mask, m_);
+  anchor_kernel<<<grid_for(n_), kThreads, 0, s_>>>(x, xl, xm, xa_, &dxp32_->x, &dxp32_->y, 2, dxm_, ix, mask, n_);
+  anchor_kernel<<<grid_for(m_), kThreads, 0, s_>>>(y, yl, ym, ya_, dy32_, dyl32_, 1, dym_, iy, mask, m_);
   if (mask) {
     spmv_masked(Gt_, ya_, qa_, mask);
     spmv_masked(G_, xa_, ra_, mask);
@@ -1152,8 +1152,9 @@ void Solver::anchor(const int32_t* ix, const int32_t* iy, const uint8_t* mask) {
 }
 
 void Solver::materialize(const int32_t* ix, const int32_t* iy, const uint8_t* mask) {
-  materialize_kernel<<<grid_for(n_), kThreads, 0, s_>>>(x, xl, xm, xa_, dx32_, dxl32_, dxm_, ix, mask, n_);
-  materialize_kernel<<<grid_for(m_), kThreads, 0, s_>>>(y, yl, ym, ya_, dy32_, dyl32_, dym_, iy, mask, m_);
+  materialize_kernel<<<grid_for(n_), kThreads, 0, s_>>>(x, xl, xm, xa_, &dxp32_->x, &dxp32_->y, 2, dxm_, ix, mask,
+                                                         n_);
+  materialize_kernel<<<grid_for(m_), kThreads, 0, s_>>>(y, yl, ym, ya_, dy32_, dyl32_, 1, dym_, iy, mask, m_);
   kernels_ += 2;
 }
 
@@ -1162,12 +1163,12 @@ void Solver::capture_graph() {
   const int32_t* act = &st_dev->active;
   for (int a = 0; a < attempts_per_graph_ && fp32_; ++a) {
     launch_spmv<1, false, float>(Gt32_, dyl32_, nullptr, aty32_, nullptr, act, s_, &st_dev->do_reflect);
-    OpPrimalStep32 op1{xa_, dxl32_, qa_, aty32_, dx32_, x, st_dev, 0.0};
+    OpPrimalStep32 op1{xa_, dxp32_, qa_, aty32_, x, st_dev, 0.0};
     launch_update_project(op1, XI, part_x, act, s_);
-    launch_spmv<2, false, float>(G32_, dx32_, dxl32_, gx32_, gxl32_, act, s_);
+    launch_spmv<kPair, false, float>(G32_, &dxp32_->x, nullptr, gx32_, gxl32_, act, s_);
     OpDualStep32 op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, st_dev, 0.0, part_x, XI.ctaA + XI.ctaB + XI.ctaC};
     launch_update_project(op2, YI, part_y, act, s_);
-    reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, dx32_, dxl32_, dxm_, n_, dy32_, dyl32_, dym_, m_);
+    reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, dxp32_, dxm_, n_, dy32_, dyl32_, dym_, m_);
   }
   for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
     launch_spmv<1>(Gt_, yl, nullptr, aty, nullptr, act, s_, &st_dev->do_reflect);
