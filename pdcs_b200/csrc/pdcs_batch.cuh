@@ -29,6 +29,7 @@
 
 #include "pdcs_adjoint.cuh"
 #include "pdcs_batch_kernels.cuh"
+#include "pdcs_bsearch.cuh"
 
 namespace pdcs {
 
@@ -114,6 +115,7 @@ enum ReqType : int32_t {
   RQ_LIN,       // dst = a u + b v (up to 6, in order)
   RQ_SPMV,      // side 0: G p0 -> p1; side 1: G' p0 -> p1
   RQ_REFLECT,   // reflection + averaging with the instance's current coefficients
+  RQ_BSEARCH,   // restart binary search(es) on the device: p0, p1 (then p2, p3); count searches
 };
 
 struct LinOp {
@@ -134,7 +136,7 @@ struct ReqPayload {
 struct Req {
   ReqPayload key;
   uint64_t hash = 0;
-  double s0 = 0.0, s1 = 0.0;  // per-instance scalars (probe steps)
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // per-instance scalars (probe steps, search parameters)
   double out[20] = {};
 };
 
@@ -230,8 +232,10 @@ class BatchSolver : public Solver {
   BatchSolver(int64_t K, const pdcs_problem* probs, const pdcs_options* o)
       : Solver(probs, o), K_(K), probs_(probs) {}
   ~BatchSolver() override {
-    if (bgraph_exec_) cudaGraphExecDestroy(bgraph_exec_);
-    if (bgraph_) cudaGraphDestroy(bgraph_);
+    for (int t = 0; t < 2; ++t) {
+      if (bgraph_exec_[t]) cudaGraphExecDestroy(bgraph_exec_[t]);
+      if (bgraph_[t]) cudaGraphDestroy(bgraph_[t]);
+    }
     if (pin_) cudaFreeHost(pin_);
   }
   // merge, upload and precondition once (the problems must stay valid until destruction:
@@ -309,8 +313,19 @@ class BatchSolver : public Solver {
   double *cx_ = nullptr, *cy_ = nullptr;  // contributions: 8 x n, 8 x m
   double *dxsq_ = nullptr, *dysq_ = nullptr, *dgdy_ = nullptr;
   double* seg_out_ = nullptr;  // K * 20
-  cudaGraph_t bgraph_ = nullptr;
-  cudaGraphExec_t bgraph_exec_ = nullptr;
+  int64_t* cones_dev_[2] = {};  // cones_ on the device
+  double* bs_prm_ = nullptr;    // K * 4
+  double* bs_out_ = nullptr;    // K * 5
+  int32_t* bs_list_ = nullptr;  // K
+  // iteration graphs: [0] grids for the whole batch, [1] the tail graph, grids
+  // capped for rounds in which few nonzeros iterate (most CTAs of the full
+  // grids would find no work and return, at the cost of their launch)
+  cudaGraph_t bgraph_[2] = {};
+  cudaGraphExec_t bgraph_exec_[2] = {};
+  static constexpr int kTailBinCtas = 64;     // SpMV CTAs per row bin
+  static constexpr int kTailCtas = 148;       // CTAs per part of the other kernels
+  // the tail graph runs while fewer than kTailNnz nonzeros, and 1/16 of the batch's, iterate
+  static constexpr int64_t kTailNnz = 1 << 20;
   // active-row lists of G (0) and G' (1) for the iteration graph
   struct Compact {
     int4* rows = nullptr;
@@ -330,6 +345,10 @@ class BatchSolver : public Solver {
   size_t pin_cap_ = 0, pin_off_ = 0;
   std::vector<Inst> inst_;
   int64_t rounds_ = 0;
+  // host wall time per service request type (verbose report)
+  double svc_s_[16] = {};
+  int64_t svc_groups_[16] = {}, svc_insts_[16] = {};
+  double iter_s_ = 0.0;
 
   int validate_batch();
   void merge();
@@ -350,7 +369,7 @@ class BatchSolver : public Solver {
   size_t act_bytes_ = 0;          // largest upload of the lists
   void setup_act_lists();
   void build_act_lists(const std::vector<Inst*>& its);
-  void capture_batch_graph();
+  void capture_batch_graph(int tail);
   template <class T>
   T* stage(size_t count);
   void sync_reset() {
@@ -371,11 +390,13 @@ class BatchSolver : public Solver {
   void schedule();
 
   // ---- requests (set the payload, suspend) ----
-  DevAwait post(Inst& I, const ReqPayload& p, double s0 = 0.0, double s1 = 0.0) {
+  DevAwait post(Inst& I, const ReqPayload& p, double s0 = 0.0, double s1 = 0.0, double s2 = 0.0, double s3 = 0.0) {
     I.req.key = p;
     I.req.hash = fnv1a(&I.req.key, sizeof(ReqPayload));
     I.req.s0 = s0;
     I.req.s1 = s1;
+    I.req.s2 = s2;
+    I.req.s3 = s3;
     return DevAwait{&I};
   }
   static ReqPayload payload(int32_t type) {
@@ -397,6 +418,8 @@ class BatchSolver : public Solver {
   Co<> exit_check(Inst& I);
   Co<double> mnorm(Inst& I, const double* dx, const double* dy, double ta, double si);
   Co<double> binary_search(Inst& I, double r, const double* px, const double* py, double ta, double si);
+  Co<bool> binary_search_dev(Inst& I, double r, const double* px0, const double* py0, const double* px1,
+                             const double* py1, double* vals);
   Co<double> approx(Inst& I, const ReqPayload& pr, double ta, double si, double& h1dx, double& h2dy, double t);
   Co<> restart_threshold(Inst& I, bool dgap);
   Co<bool> restart_check(Inst& I, bool dgap);
@@ -657,6 +680,13 @@ void BatchSolver::setup_batch() {
   dysq_ = A.alloc<double>(m_);
   dgdy_ = A.alloc<double>(m_);
   seg_out_ = A.alloc<double>(K * 20);
+  bs_prm_ = A.alloc<double>(4 * K);
+  bs_out_ = A.alloc<double>(5 * K);
+  bs_list_ = A.alloc<int32_t>(K);
+  for (int w = 0; w < 2; ++w) {
+    cones_dev_[w] = A.alloc<int64_t>(8 * K);
+    PDCS_CUDA(cudaMemcpyAsync(cones_dev_[w], cones_[w].data(), sizeof(int64_t) * 8 * K, cudaMemcpyHostToDevice, s_));
+  }
   PDCS_CUDA(cudaMemsetAsync(live_cnt_, 0, 4 * sizeof(int32_t), s_));
   PDCS_CUDA(cudaMemsetAsync(done_ctas_, 0, sizeof(uint32_t), s_));
   PDCS_CUDA(cudaMemsetAsync(live_, 0, K, s_));
@@ -887,41 +917,68 @@ void BatchSolver::compact(const uint8_t* mask) {
   }
 }
 
-void BatchSolver::capture_batch_graph() {
+namespace {
+// a copy of A's schedule with at most cap CTAs per row bin (the kernel loops over its bin's rows)
+template <class T>
+CsrT<T> capped_bins(const CsrT<T>& A, int cap) {
+  CsrT<T> B = A;
+  B.cta0[0] = 0;
+  for (int b = 0; b < kBins; ++b) B.cta0[b + 1] = B.cta0[b] + std::min(A.cta0[b + 1] - A.cta0[b], cap);
+  return B;
+}
+// a copy of T with at most cap CTAs per part (every part loops over its work)
+ConeTable capped_parts(const ConeTable& T, int cap) {
+  ConeTable C = T;
+  C.ctaA = std::min(T.ctaA, cap);
+  C.ctaB = std::min(T.ctaB, cap);
+  C.ctaC = std::min(T.ctaC, cap);
+  return C;
+}
+}  // namespace
+
+void BatchSolver::capture_batch_graph(int tail) {
+  const int bin_cap = tail ? kTailBinCtas : INT32_MAX, cap = tail ? kTailCtas : INT32_MAX;
+  const CsrT<float> G32 = capped_bins(G32c_, bin_cap), Gt32 = capped_bins(Gt32c_, bin_cap);
+  const CsrDev G = capped_bins(Gc_, bin_cap), Gt = capped_bins(Gtc_, bin_cap);
+  const ConeTable XI = capped_parts(XIg_, cap), YI = capped_parts(YIg_, cap);
+  const int ctl_grid = tail ? (int)std::max<int64_t>(1, std::min<int64_t>(K_, cap))
+                            : (int)std::max<int64_t>(1, std::min<int64_t>((K_ * 32 + kThreads - 1) / kThreads, 148 * 16));
+  const int refl_grid = std::min(grid_reflect_, cap);
   PDCS_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-  const int ctl_grid = (int)std::max<int64_t>(1, std::min<int64_t>((K_ * 32 + kThreads - 1) / kThreads, 148 * 16));
   for (int a = 0; a < attempts_per_graph_ && fp32_; ++a) {
     int32_t* cur = live_cnt_ + (a & 1);
     int32_t* nxt = live_cnt_ + ((a + 1) & 1);
-    launch_spmv<1, false, float>(Gt32c_, dyl32_, nullptr, aty32_, nullptr, cur, s_);
+    launch_spmv<1, false, float>(Gt32, dyl32_, nullptr, aty32_, nullptr, cur, s_);
     OpPrimalStep32B op1{xa_, dxp32_, qa_, aty32_, x, ix_, live_, ps_, dxsq_};
-    launch_update_project(op1, XIg_, part_x, cur, s_);
-    launch_spmv<kPair, false, float>(G32c_, &dxp32_->x, nullptr, gx32_, gxl32_, cur, s_);
+    launch_update_project(op1, XI, part_x, cur, s_);
+    launch_spmv<kPair, false, float>(G32, &dxp32_->x, nullptr, gx32_, gxl32_, cur, s_);
     OpDualStep32B op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_};
-    launch_update_project(op2, YIg_, part_y, cur, s_);
+    launch_update_project(op2, YI, part_y, cur, s_);
     BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,
                  dgdy_, cur,  nxt,     done_ctas_, live_cnt_ + 2, act_inst_, n_act_};
-    batch_control_kernel<<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
-    batch_reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dxp32_, dxm_, dy32_, dyl32_,
-                                                               dym_, rchunk_, n_rchunk_);
+    if (tail) batch_control_kernel<true><<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
+    else batch_control_kernel<false><<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
+    batch_reflect32_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dxp32_, dxm_, dy32_, dyl32_, dym_,
+                                                           rchunk_, n_rchunk_);
   }
   for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
     int32_t* cur = live_cnt_ + (a & 1);
     int32_t* nxt = live_cnt_ + ((a + 1) & 1);
-    launch_spmv<1>(Gtc_, yl, nullptr, aty, nullptr, cur, s_);
+    launch_spmv<1>(Gt, yl, nullptr, aty, nullptr, cur, s_);
     OpPrimalStepB op1{xl, aty, c_s, x, ix_, live_, ps_, dxsq_};
-    launch_update_project(op1, XIg_, part_x, cur, s_);
-    launch_spmv<2>(Gc_, x, xl, gx, gxl, cur, s_);
+    launch_update_project(op1, XI, part_x, cur, s_);
+    launch_spmv<2>(G, x, xl, gx, gxl, cur, s_);
     OpDualStepB op2{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_};
-    launch_update_project(op2, YIg_, part_y, cur, s_);
+    launch_update_project(op2, YI, part_y, cur, s_);
     BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,
                  dgdy_, cur,  nxt,     done_ctas_, live_cnt_ + 2, act_inst_, n_act_};
-    batch_control_kernel<<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
-    batch_reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, x, xl, xm, y, yl, ym, rchunk_,
-                                                             n_rchunk_);
+    if (tail) batch_control_kernel<true><<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
+    else batch_control_kernel<false><<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
+    batch_reflect_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, x, xl, xm, y, yl, ym, rchunk_,
+                                                         n_rchunk_);
   }
-  PDCS_CUDA(cudaStreamEndCapture(s_, &bgraph_));
-  PDCS_CUDA(cudaGraphInstantiate(&bgraph_exec_, bgraph_, 0));
+  PDCS_CUDA(cudaStreamEndCapture(s_, &bgraph_[tail]));
+  PDCS_CUDA(cudaGraphInstantiate(&bgraph_exec_[tail], bgraph_[tail], 0));
 }
 
 // Run one batched operation for a group of instances with identical requests.
@@ -1028,6 +1085,53 @@ void BatchSolver::exec_group(std::vector<Inst*>& g) {
       }
       break;
     }
+    case RQ_BSEARCH: {
+      double* prm = stage<double>(4 * K_);
+      int32_t* list = stage<int32_t>(g.size());
+      for (size_t i = 0; i < g.size(); ++i) {
+        const Inst* I = g[i];
+        list[i] = (int32_t)I->k;
+        prm[4 * I->k] = I->req.s0;
+        prm[4 * I->k + 1] = I->req.s1;
+        prm[4 * I->k + 2] = I->req.s2;
+        prm[4 * I->k + 3] = I->req.s3;
+      }
+      PDCS_CUDA(cudaMemcpyAsync(bs_prm_, prm, sizeof(double) * 4 * K_, cudaMemcpyHostToDevice, s_));
+      PDCS_CUDA(cudaMemcpyAsync(bs_list_, list, sizeof(int32_t) * g.size(), cudaMemcpyHostToDevice, s_));
+      BsArgs B{};
+      B.list = bs_list_;
+      B.rx = rx_;
+      B.ry = ry_;
+      B.cones_x = cones_dev_[0];
+      B.cones_y = cones_dev_[1];
+      B.X = XI;
+      B.Y = YI;
+      B.G = G_;
+      B.Gt = Gt_;
+      B.c = c_s;
+      B.h = h_s;
+      B.h1 = tn[2];
+      B.h2 = tm[2];
+      B.xs = tn[3];
+      B.ys = tm[3];
+      B.gpx = tm[1];
+      B.gxs = tm[4];
+      B.nsearch = q.count;
+      for (int i = 0; i < q.count; ++i) {
+        B.px[i] = q.p[2 * i];
+        B.py[i] = q.p[2 * i + 1];
+      }
+      B.prm = bs_prm_;
+      B.out = bs_out_;
+      bsearch_kernel<<<(int)g.size(), kThreads, 0, s_>>>(B);
+      kernels_++;
+      double* o = stage<double>(5 * K_);
+      PDCS_CUDA(cudaMemcpyAsync(o, bs_out_, sizeof(double) * 5 * K_, cudaMemcpyDeviceToHost, s_));
+      sync_reset();
+      for (Inst* I : g)
+        for (int i = 0; i < 5; ++i) I->req.out[i] = o[5 * I->k + i];
+      break;
+    }
     case RQ_MNORM: {
       double* gdx = const_cast<double*>(q.p[2]);
       spmv_masked(G_, q.p[0], gdx, mask);
@@ -1063,7 +1167,10 @@ void BatchSolver::exec_group(std::vector<Inst*>& g) {
 // Run shared graphs of PDHG attempts until some iterating instance halts.
 void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   Timer tm_(t_iter_);
-  if (!bgraph_exec_) capture_batch_graph();
+  if (!bgraph_exec_[0]) {
+    capture_batch_graph(0);
+    capture_batch_graph(1);
+  }
   std::vector<uint8_t> iterating(K_, 0);
   for (Inst* I : its) iterating[I->k] = 1;
   PdhgState* hs = stage<PdhgState>(K_);
@@ -1110,8 +1217,11 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   int64_t graphs = (to_check + attempts_per_graph_ - 1) / attempts_per_graph_;
   graphs = std::max<int64_t>(1, std::min<int64_t>(graphs, 4));
   const double t_round = now_s();
+  int64_t live_nnz = 0;
+  for (Inst* I : its) live_nnz += probs_[I->k].nnz;
+  const int tail = (live_nnz < kTailNnz && 16 * live_nnz < nnz_) ? 1 : 0;
   for (int64_t gi = 0; gi < graphs; ++gi) {
-    PDCS_CUDA(cudaGraphLaunch(bgraph_exec_, s_));
+    PDCS_CUDA(cudaGraphLaunch(bgraph_exec_[tail], s_));
     graphs_++;
     kernels_ += 6LL * attempts_per_graph_;
   }
@@ -1119,9 +1229,9 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   PDCS_CUDA(cudaMemcpyAsync(back, sts_, sizeof(PdhgState) * K_, cudaMemcpyDeviceToHost, s_));
   sync_reset();  // `back` stays readable: nothing is staged before the loop below ends
   if (O.verbose)
-    std::printf("[pdcs_b200 batch] %.3f s: %zu of %lld instances iterating, %lld attempts in %.3f ms\n",
+    std::printf("[pdcs_b200 batch] %.3f s: %zu of %lld instances iterating, %lld attempts in %.3f ms%s\n",
                 now_s() - t_start_, its.size(), (long long)K_, (long long)(graphs * attempts_per_graph_),
-                1e3 * (now_s() - t_round));
+                1e3 * (now_s() - t_round), tail ? " (tail graph)" : "");
   const bool timeout = O.time_limit > 0 && now_s() - t_start_ > O.time_limit;
   std::vector<Inst*> halted;
   for (Inst* I : its) {
@@ -1172,12 +1282,19 @@ void BatchSolver::schedule() {
         for (auto& l : kv.second) order.push_back(&l);
       std::sort(order.begin(), order.end(), [](auto* a, auto* b) { return (*a)[0]->k < (*b)[0]->k; });
       for (auto* l : order) {
+        const double t0 = now_s();
+        const int32_t type = (*l)[0]->req.key.type & 15;
         exec_group(*l);
         for (Inst* I : *l) resume(*I);
+        svc_s_[type] += now_s() - t0;
+        svc_groups_[type]++;
+        svc_insts_[type] += (int64_t)l->size();
       }
       continue;
     }
+    const double t0 = now_s();
     exec_iterate(its);
+    iter_s_ += now_s() - t0;
   }
 }
 
@@ -1368,6 +1485,30 @@ Co<double> BatchSolver::binary_search(Inst& I, double r, const double* px, const
   co_return (last_h1dx + last_h2dy) / r;
 }
 
+// The binary search(es) of one restart test on the device (bsearch_kernel):
+// (px0, py0), then (px1, py1) when px1 is given, the second from the radius the
+// first ends at.  Returns false, leaving bs_t0 as it was, when an instance's
+// search needs more evaluations than the device path runs (the caller then
+// runs binary_search).
+Co<bool> BatchSolver::binary_search_dev(Inst& I, double r, const double* px0, const double* py0,
+                                        const double* px1, const double* py1, double* vals) {
+  ReqPayload p = payload(RQ_BSEARCH);
+  p.count = px1 ? 2 : 1;
+  p.p[0] = px0;
+  p.p[1] = py0;
+  p.p[2] = px1;
+  p.p[3] = py1;
+  co_await post(I, p, r, I.S.tau, I.S.sigma, I.bs_t0);
+  const double* q = I.req.out;
+  I.probes += (int64_t)q[0];
+  probes_ += (int64_t)q[0];
+  if (q[4] == 0.0) co_return false;
+  I.bs_t0 = q[1];
+  vals[0] = q[2];
+  vals[1] = q[3];
+  co_return true;
+}
+
 // one evaluation of the binary search at t (approx of Solver::binary_search)
 Co<double> BatchSolver::approx(Inst& I, const ReqPayload& pr, double ta, double si, double& h1dx, double& h2dy,
                                double t) {
@@ -1386,7 +1527,9 @@ Co<> BatchSolver::restart_threshold(Inst& I, bool dgap) {
     co_await lin(I, {{dx, 1.0, x0, -1.0, x0l, 0}, {dy, 1.0, y0, -1.0, y0l, 1}});
     double r = co_await mnorm(I, dx, dy, I.S.tau, I.S.sigma);
     I.ndg_r = r;
-    I.ndg_thr = co_await binary_search(I, r, x0, y0, I.S.tau, I.S.sigma);
+    double v[2];
+    if (co_await binary_search_dev(I, r, x0, y0, nullptr, nullptr, v)) I.ndg_thr = v[0];
+    else I.ndg_thr = co_await binary_search(I, r, x0, y0, I.S.tau, I.S.sigma);
     if (I.ndg_thr < 0) I.dgap_flag = false;
   } else {
     co_await converge_info(I, x, y, I.ci[0], tm[0], tn[0]);
@@ -1399,8 +1542,14 @@ Co<bool> BatchSolver::restart_check(Inst& I, bool dgap) {
     double *dx = tn[4], *dy = tm[5];
     co_await lin(I, {{dx, 1.0, x, -1.0, x0, 0}, {dy, 1.0, y, -1.0, y0, 1}});
     double rl = co_await mnorm(I, dx, dy, I.S.tau, I.S.sigma);
-    double rho = co_await binary_search(I, rl, x, y, I.S.tau, I.S.sigma);
-    double rho_m = co_await binary_search(I, rl, xm, ym, I.S.tau, I.S.sigma);
+    double v[2], rho, rho_m;
+    if (co_await binary_search_dev(I, rl, x, y, xm, ym, v)) {
+      rho = v[0];
+      rho_m = v[1];
+    } else {
+      rho = co_await binary_search(I, rl, x, y, I.S.tau, I.S.sigma);
+      rho_m = co_await binary_search(I, rl, xm, ym, I.S.tau, I.S.sigma);
+    }
     I.ndg[0] = rho;
     I.ndg[1] = rho_m;
     const double betas[2] = {0.4, 0.8};
@@ -1648,6 +1797,11 @@ void BatchSolver::reset_state() {
   }
   kernels_ = graphs_ = probes_ = rounds_ = 0;
   t_iter_ = 0.0;
+  iter_s_ = 0.0;
+  for (int t = 0; t < 16; ++t) {
+    svc_s_[t] = 0.0;
+    svc_groups_[t] = svc_insts_[t] = 0;
+  }
 }
 
 int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_limit) {
@@ -1658,6 +1812,16 @@ int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_
   t_start_ = now_s();
   schedule();
   O.attempt_limit = limit0;
+  if (O.verbose) {
+    static const char* names[] = {"none", "iterate", "converge", "probe", "mnorm", "seg",
+                                  "lin",  "spmv",    "reflect",  "bsearch"};
+    std::printf("[pdcs_b200 batch] schedule %.3f s: iteration rounds %.3f s", now_s() - t_start_, iter_s_);
+    for (int t = 0; t < 10; ++t)
+      if (svc_groups_[t])
+        std::printf(", %s %lld groups / %lld requests %.3f s", names[t], (long long)svc_groups_[t],
+                    (long long)svc_insts_[t], svc_s_[t]);
+    std::printf("\n");
+  }
   PDCS_CUDA(cudaStreamSynchronize(s_));
   // outputs: unscaled current or averaged iterate per instance, scattered to the callers' buffers
   uint8_t* hpick = stage<uint8_t>(K_);

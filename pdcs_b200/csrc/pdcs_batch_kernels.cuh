@@ -190,8 +190,8 @@ __global__ void __launch_bounds__(kThreads) seg_reduce_kernel(int64_t K, const u
 
 // Control of one batched attempt.  live_cur / live_next: the number of live
 // instances at the start of this attempt and of the next one (two slots used
-// alternately by consecutive attempts of a graph).  A warp per instance sums
-// its contributions in a fixed order and runs the shared control_step.
+// alternately by consecutive attempts of a graph).  The contributions of an
+// instance are summed in a fixed order, then the shared control_step runs.
 struct BatchCtl {
   PdhgState* sts;
   double* ps;
@@ -209,45 +209,90 @@ struct BatchCtl {
   const int64_t* n_act;
 };
 
+// Per-instance sums of the attempt's contributions (a: |dx|^2, b: |dy|^2,
+// d: dy'(G dx - G dxl)) over the instance's runs, by G lanes (lane gl of G)
+template <int G>
+__device__ __forceinline__ void control_sums(const BatchCtl& c, int64_t k, int gl, double& a, double& b, double& d) {
+  for (int q = 0; q < kMaxRuns; ++q) {
+    const int64_t s0 = c.rx.start[k * kMaxRuns + q], L = c.rx.len[k * kMaxRuns + q];
+    for (int64_t i = s0 + gl; i < s0 + L; i += G) a += c.dxsq[i];
+    const int64_t t0 = c.ry.start[k * kMaxRuns + q], M = c.ry.len[k * kMaxRuns + q];
+    for (int64_t i = t0 + gl; i < t0 + M; i += G) {
+      b += c.dysq[i];
+      d += c.dgdy[i];
+    }
+  }
+}
+
+__device__ __forceinline__ void control_apply(const BatchCtl& c, int64_t k, double a, double b, double d, int& nlive) {
+  PdhgState s = c.sts[k];
+  control_step(s, a, b, d);
+  c.sts[k] = s;
+  c.ps[k] = s.ps;
+  c.ds[k] = s.ds;
+  c.live[k] = s.active ? 1 : 0;
+  nlive += s.active ? 1 : 0;
+}
+
+// CTA_INST: a CTA per instance (few iterating instances, some of them large);
+// otherwise a warp per instance (the control steps of many instances run side by side).
+template <bool CTA_INST>
 __global__ void __launch_bounds__(kThreads) batch_control_kernel(int64_t K, BatchCtl c) {
   if (*c.live_cur == 0) {
     if (blockIdx.x == 0 && threadIdx.x == 0) *c.live_next = 0;
     return;
   }
   const int lane = threadIdx.x & 31;
-  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t nk = c.act_inst ? *c.n_act : K;
   int nlive = 0;
-  for (int64_t kk = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; kk < nk; kk += wstride) {
-    const int64_t k = c.act_inst ? (int64_t)c.act_inst[kk] : kk;
-    if (!c.live[k]) {
-      // no step ran for this instance: nothing to reflect
-      if (lane == 0) c.sts[k].do_reflect = 0;
-      continue;
-    }
-    double a = 0.0, b = 0.0, d = 0.0;
-    for (int q = 0; q < kMaxRuns; ++q) {
-      const int64_t s0 = c.rx.start[k * kMaxRuns + q], L = c.rx.len[k * kMaxRuns + q];
-      for (int64_t i = s0 + lane; i < s0 + L; i += 32) a += c.dxsq[i];
-      const int64_t t0 = c.ry.start[k * kMaxRuns + q], M = c.ry.len[k * kMaxRuns + q];
-      for (int64_t i = t0 + lane; i < t0 + M; i += 32) {
-        b += c.dysq[i];
-        d += c.dgdy[i];
+  if constexpr (CTA_INST) {
+    __shared__ double red[3][kWarps];
+    for (int64_t kk = blockIdx.x; kk < nk; kk += gridDim.x) {
+      const int64_t k = c.act_inst ? (int64_t)c.act_inst[kk] : kk;
+      if (!c.live[k]) {  // CTA-uniform; no step ran for this instance: nothing to reflect
+        if (threadIdx.x == 0) c.sts[k].do_reflect = 0;
+        continue;
       }
+      double a = 0.0, b = 0.0, d = 0.0;
+      control_sums<kThreads>(c, k, threadIdx.x, a, b, d);
+      for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(kFull, a, o);
+        b += __shfl_down_sync(kFull, b, o);
+        d += __shfl_down_sync(kFull, d, o);
+      }
+      if (lane == 0) {
+        red[0][threadIdx.x >> 5] = a;
+        red[1][threadIdx.x >> 5] = b;
+        red[2][threadIdx.x >> 5] = d;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        a = b = d = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+          a += red[0][w];
+          b += red[1][w];
+          d += red[2][w];
+        }
+        control_apply(c, k, a, b, d, nlive);
+      }
+      __syncthreads();  // red is reused; live[k] was read by every thread before thread 0 wrote it
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_down_sync(kFull, a, o);
-      b += __shfl_down_sync(kFull, b, o);
-      d += __shfl_down_sync(kFull, d, o);
-    }
-    if (lane == 0) {
-      PdhgState s = c.sts[k];
-      control_step(s, a, b, d);
-      c.sts[k] = s;
-      c.ps[k] = s.ps;
-      c.ds[k] = s.ds;
-      c.live[k] = s.active ? 1 : 0;
-      nlive += s.active ? 1 : 0;
+  } else {
+    const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t kk = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; kk < nk; kk += wstride) {
+      const int64_t k = c.act_inst ? (int64_t)c.act_inst[kk] : kk;
+      if (!c.live[k]) {
+        if (lane == 0) c.sts[k].do_reflect = 0;
+        continue;
+      }
+      double a = 0.0, b = 0.0, d = 0.0;
+      control_sums<32>(c, k, lane, a, b, d);
+      for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(kFull, a, o);
+        b += __shfl_down_sync(kFull, b, o);
+        d += __shfl_down_sync(kFull, d, o);
+      }
+      if (lane == 0) control_apply(c, k, a, b, d, nlive);
     }
   }
   // count the instances still live; the last CTA publishes the count
