@@ -235,6 +235,9 @@ class BatchSolver : public Solver {
     for (int t = 0; t < 2; ++t) {
       if (bgraph_exec_[t]) cudaGraphExecDestroy(bgraph_exec_[t]);
       if (bgraph_[t]) cudaGraphDestroy(bgraph_[t]);
+      for (cudaEvent_t e : gev_[t])
+        if (e) cudaEventDestroy(e);
+      if (round_ev_[t]) cudaEventDestroy(round_ev_[t]);
     }
     if (pin_) cudaFreeHost(pin_);
   }
@@ -323,6 +326,13 @@ class BatchSolver : public Solver {
   cudaGraph_t bgraph_[2] = {};
   cudaGraphExec_t bgraph_exec_[2] = {};
   static constexpr int kTailBinCtas = 64;     // SpMV CTAs per row bin
+  // verbose timing: device time of each round (round_ev_), and with verbose >= 2
+  // event nodes around the 6 kernels of every graph's last attempt (gev_)
+  cudaEvent_t round_ev_[2] = {};
+  cudaEvent_t gev_[2][7] = {};
+  double gev_ms_[2][6] = {};
+  int64_t gev_n_[2] = {};
+  double dev_ms_ = 0.0;
   static constexpr int kTailCtas = 148;       // CTAs per part of the other kernels
   // the tail graph runs while fewer than kTailNnz nonzeros, and 1/16 of the batch's, iterate
   static constexpr int64_t kTailNnz = 1 << 20;
@@ -944,38 +954,53 @@ void BatchSolver::capture_batch_graph(int tail) {
   const int ctl_grid = tail ? (int)std::max<int64_t>(1, std::min<int64_t>(K_, cap))
                             : (int)std::max<int64_t>(1, std::min<int64_t>((K_ * 32 + kThreads - 1) / kThreads, 148 * 16));
   const int refl_grid = std::min(grid_reflect_, cap);
+  const bool timed = O.verbose >= 2;
+  if (timed)
+    for (cudaEvent_t& e : gev_[tail])
+      if (!e) PDCS_CUDA(cudaEventCreate(&e));
   PDCS_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-  for (int a = 0; a < attempts_per_graph_ && fp32_; ++a) {
+  for (int a = 0; a < attempts_per_graph_; ++a) {
     int32_t* cur = live_cnt_ + (a & 1);
     int32_t* nxt = live_cnt_ + ((a + 1) & 1);
-    launch_spmv<1, false, float>(Gt32, dyl32_, nullptr, aty32_, nullptr, cur, s_);
-    OpPrimalStep32B op1{xa_, dxp32_, qa_, aty32_, x, ix_, live_, ps_, dxsq_};
-    launch_update_project(op1, XI, part_x, cur, s_);
-    launch_spmv<kPair, false, float>(G32, &dxp32_->x, nullptr, gx32_, gxl32_, cur, s_);
-    OpDualStep32B op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_};
-    launch_update_project(op2, YI, part_y, cur, s_);
+    const bool ev = timed && a == attempts_per_graph_ - 1;
+    auto mark = [&](int i) {
+      if (ev) PDCS_CUDA(cudaEventRecordWithFlags(gev_[tail][i], s_, cudaEventRecordExternal));  // a node of the graph
+    };
     BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,
                  dgdy_, cur,  nxt,     done_ctas_, live_cnt_ + 2, act_inst_, n_act_};
+    mark(0);
+    if (fp32_) {
+      launch_spmv<1, false, float>(Gt32, dyl32_, nullptr, aty32_, nullptr, cur, s_);
+      mark(1);
+      OpPrimalStep32B op1{xa_, dxp32_, qa_, aty32_, x, ix_, live_, ps_, dxsq_};
+      launch_update_project(op1, XI, part_x, cur, s_);
+      mark(2);
+      launch_spmv<kPair, false, float>(G32, &dxp32_->x, nullptr, gx32_, gxl32_, cur, s_);
+      mark(3);
+      OpDualStep32B op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_};
+      launch_update_project(op2, YI, part_y, cur, s_);
+    } else {
+      launch_spmv<1>(Gt, yl, nullptr, aty, nullptr, cur, s_);
+      mark(1);
+      OpPrimalStepB op1{xl, aty, c_s, x, ix_, live_, ps_, dxsq_};
+      launch_update_project(op1, XI, part_x, cur, s_);
+      mark(2);
+      launch_spmv<2>(G, x, xl, gx, gxl, cur, s_);
+      mark(3);
+      OpDualStepB op2{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_};
+      launch_update_project(op2, YI, part_y, cur, s_);
+    }
+    mark(4);
     if (tail) batch_control_kernel<true><<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
     else batch_control_kernel<false><<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
-    batch_reflect32_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dxp32_, dxm_, dy32_, dyl32_, dym_,
-                                                           rchunk_, n_rchunk_);
-  }
-  for (int a = 0; a < attempts_per_graph_ && !fp32_; ++a) {
-    int32_t* cur = live_cnt_ + (a & 1);
-    int32_t* nxt = live_cnt_ + ((a + 1) & 1);
-    launch_spmv<1>(Gt, yl, nullptr, aty, nullptr, cur, s_);
-    OpPrimalStepB op1{xl, aty, c_s, x, ix_, live_, ps_, dxsq_};
-    launch_update_project(op1, XI, part_x, cur, s_);
-    launch_spmv<2>(G, x, xl, gx, gxl, cur, s_);
-    OpDualStepB op2{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_};
-    launch_update_project(op2, YI, part_y, cur, s_);
-    BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,
-                 dgdy_, cur,  nxt,     done_ctas_, live_cnt_ + 2, act_inst_, n_act_};
-    if (tail) batch_control_kernel<true><<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
-    else batch_control_kernel<false><<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
-    batch_reflect_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, x, xl, xm, y, yl, ym, rchunk_,
-                                                         n_rchunk_);
+    mark(5);
+    if (fp32_)
+      batch_reflect32_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dxp32_, dxm_, dy32_, dyl32_, dym_,
+                                                             rchunk_, n_rchunk_);
+    else
+      batch_reflect_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, x, xl, xm, y, yl, ym, rchunk_,
+                                                           n_rchunk_);
+    mark(6);
   }
   PDCS_CUDA(cudaStreamEndCapture(s_, &bgraph_[tail]));
   PDCS_CUDA(cudaGraphInstantiate(&bgraph_exec_[tail], bgraph_[tail], 0));
@@ -1220,18 +1245,36 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   int64_t live_nnz = 0;
   for (Inst* I : its) live_nnz += probs_[I->k].nnz;
   const int tail = (live_nnz < kTailNnz && 16 * live_nnz < nnz_) ? 1 : 0;
+  if (O.verbose) {
+    for (cudaEvent_t& e : round_ev_)
+      if (!e) PDCS_CUDA(cudaEventCreate(&e));
+    PDCS_CUDA(cudaEventRecord(round_ev_[0], s_));
+  }
   for (int64_t gi = 0; gi < graphs; ++gi) {
     PDCS_CUDA(cudaGraphLaunch(bgraph_exec_[tail], s_));
     graphs_++;
     kernels_ += 6LL * attempts_per_graph_;
   }
+  if (O.verbose) PDCS_CUDA(cudaEventRecord(round_ev_[1], s_));
   PdhgState* back = stage<PdhgState>(K_);
   PDCS_CUDA(cudaMemcpyAsync(back, sts_, sizeof(PdhgState) * K_, cudaMemcpyDeviceToHost, s_));
   sync_reset();  // `back` stays readable: nothing is staged before the loop below ends
-  if (O.verbose)
-    std::printf("[pdcs_b200 batch] %.3f s: %zu of %lld instances iterating, %lld attempts in %.3f ms%s\n",
+  if (O.verbose) {
+    float dev = 0.0f;
+    PDCS_CUDA(cudaEventElapsedTime(&dev, round_ev_[0], round_ev_[1]));
+    dev_ms_ += dev;
+    if (O.verbose >= 2 && gev_[tail][0]) {  // the kernels of the round's last attempt
+      for (int i = 0; i < 6; ++i) {
+        float e = 0.0f;
+        PDCS_CUDA(cudaEventElapsedTime(&e, gev_[tail][i], gev_[tail][i + 1]));
+        gev_ms_[tail][i] += e;
+      }
+      gev_n_[tail]++;
+    }
+    std::printf("[pdcs_b200 batch] %.3f s: %zu of %lld instances iterating, %lld attempts in %.3f ms (device %.3f ms)%s\n",
                 now_s() - t_start_, its.size(), (long long)K_, (long long)(graphs * attempts_per_graph_),
-                1e3 * (now_s() - t_round), tail ? " (tail graph)" : "");
+                1e3 * (now_s() - t_round), dev, tail ? " (tail graph)" : "");
+  }
   const bool timeout = O.time_limit > 0 && now_s() - t_start_ > O.time_limit;
   std::vector<Inst*> halted;
   for (Inst* I : its) {
@@ -1798,6 +1841,11 @@ void BatchSolver::reset_state() {
   kernels_ = graphs_ = probes_ = rounds_ = 0;
   t_iter_ = 0.0;
   iter_s_ = 0.0;
+  dev_ms_ = 0.0;
+  for (int t = 0; t < 2; ++t) {
+    gev_n_[t] = 0;
+    for (double& v : gev_ms_[t]) v = 0.0;
+  }
   for (int t = 0; t < 16; ++t) {
     svc_s_[t] = 0.0;
     svc_groups_[t] = svc_insts_[t] = 0;
@@ -1820,7 +1868,15 @@ int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_
       if (svc_groups_[t])
         std::printf(", %s %lld groups / %lld requests %.3f s", names[t], (long long)svc_groups_[t],
                     (long long)svc_insts_[t], svc_s_[t]);
-    std::printf("\n");
+    std::printf("\n[pdcs_b200 batch] iteration graphs: device time %.3f s\n", 1e-3 * dev_ms_);
+    static const char* kn[6] = {"G'y", "primal", "Gx", "dual", "control", "reflect"};
+    for (int t = 0; t < 2; ++t)
+      if (gev_n_[t]) {
+        std::printf("[pdcs_b200 batch] %s graph, last attempt of %lld rounds, mean us:", t ? "tail" : "full",
+                    (long long)gev_n_[t]);
+        for (int i = 0; i < 6; ++i) std::printf(" %s %.1f", kn[i], 1e3 * gev_ms_[t][i] / gev_n_[t]);
+        std::printf("\n");
+      }
   }
   PDCS_CUDA(cudaStreamSynchronize(s_));
   // outputs: unscaled current or averaged iterate per instance, scattered to the callers' buffers
