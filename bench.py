@@ -72,12 +72,13 @@ def workload(args, rank=0):
     return batch, cfg, (n, m, nnz, nb)
 
 
-def bytes_per_attempt(n, m, nnz, n1, w):
+def bytes_per_attempt(n, m, nnz, n1, w, ib=4):
     """Algorithmic HBM bytes of one PDHG attempt of the whole batch: G and G'
-    (values + int32 column indices) once each, both row pointers, the primal /
+    (w-byte values + ib-byte column indices: 4 for the binned SpMV, 2 for the
+    instance tiles' local columns) once each, both row pointers, the primal /
     dual vector streams, the box bounds and the averaged iterates, with w-byte
     values."""
-    return 2 * nnz * (w + 4) + 4 * (m + 1) + 4 * (n + 1) + w * (4 * n + 2 * n1 + 4 * m) + w * 2 * (n + m)
+    return 2 * nnz * (w + ib) + 4 * (m + 1) + 4 * (n + 1) + w * (4 * n + 2 * n1 + 4 * m) + w * 2 * (n + m)
 
 
 class Clocks:
@@ -305,14 +306,14 @@ def run_ours(args):
     it_rate = replicas.sum_over_ranks(iters, world) / t_max
     iters_per_inst = [s.info.iter for s in sols]
 
-    lanes = list(sols[0].info.spmv_lane_nnz)
+    tiled = bool(info.spmv_tiled)
 
     # ---- per-attempt time with every instance iterating (no checkpoint below 2000 attempts) ----
     (_, _), t1 = timed(stream, lambda: h.solve(attempt_limit=64))
     (_, _), t2 = timed(stream, lambda: h.solve(attempt_limit=320))
     t_att = (t2 - t1) / 256
     h.close()
-    B_att = bytes_per_attempt(n, m, nnz, nb, 4)
+    B_att = bytes_per_attempt(n, m, nnz, nb, 4, 2 if tiled else 4)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -331,17 +332,20 @@ def run_ours(args):
                 "algorithmic_bytes_per_attempt": B_att, "attempt_ms": t_att * 1e3,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"}
 
-    # ---- the autotuned SpMV schedule against one fixed schedule (4 nonzeros per lane) ----
-    hf = solver.BatchHandle(batch, precision="fp32", stream=stream.cuda_stream, spmv_lane_nnz=4)
-    timed(stream, lambda: hf.solve(attempt_limit=64))
-    (_, _), tf1 = timed(stream, lambda: hf.solve(attempt_limit=64))
-    (_, _), tf2 = timed(stream, lambda: hf.solve(attempt_limit=320))
-    (sf, _), tf = timed(stream, hf.solve)
-    hf.close()
-    schedule = {"autotuned_lane_nnz_G_Gt": lanes, "autotuned_attempt_ms": t_att * 1e3,
-                "fixed_lane_nnz": 4, "fixed_attempt_ms": (tf2 - tf1) / 256 * 1e3,
-                "fixed_time_to_1e-6_ms": 1e3 * tf,
-                "fixed_optimal": sum(1 for s in sf if s.info.exit_status == "optimal")}
+    # ---- the SpMV of the iteration graph: instance tiles (the default) against the binned
+    # row schedule, autotuned and on one fixed schedule (4 nonzeros per lane) ----
+    def spmv_variant(**kw):
+        hv = solver.BatchHandle(batch, precision="fp32", stream=stream.cuda_stream, **kw)
+        timed(stream, lambda: hv.solve(attempt_limit=64))
+        (_, _), a1 = timed(stream, lambda: hv.solve(attempt_limit=64))
+        (_, _), a2 = timed(stream, lambda: hv.solve(attempt_limit=320))
+        (sv, _), tv = timed(stream, hv.solve)
+        hv.close()
+        return {"lane_nnz_G_Gt": list(sv[0].info.spmv_lane_nnz), "attempt_ms": (a2 - a1) / 256 * 1e3,
+                "time_to_1e-6_ms": 1e3 * tv, "optimal": sum(1 for x in sv if x.info.exit_status == "optimal")}
+    schedule = {"headline": "instance tiles" if tiled else "binned rows", "headline_attempt_ms": t_att * 1e3,
+                "binned_autotuned": spmv_variant(spmv_tiles=False),
+                "binned_fixed": spmv_variant(spmv_tiles=False, spmv_lane_nnz=4)}
 
     # ---- the same batch, batched FP64 (one timed solve) ----
     h64 = solver.BatchHandle(batch, precision="fp64", stream=stream.cuda_stream)

@@ -112,6 +112,13 @@ typedef struct {
                                     1..16); 0 (default) = autotuned per matrix at setup for matrices of
                                     2^20 or more nonzeros, 4 below */
   int32_t differentiable;        /* keep the unscaled data the solution-map adjoint (pdcs_batch_grad) needs */
+  int32_t spmv_tiles;            /* batched solver's iteration SpMVs: 0 (default) instance tiles -- each CTA
+                                    stages one instance's column segment in shared memory, 16-bit local
+                                    column indices -- when every instance has at most 65535 variables and
+                                    65535 constraint rows; > 0 the same with at most this many nonzeros
+                                    per tile (default 65536); -1 the binned row schedule (spmv_lane_nnz).
+                                    Rounds with few nonzeros left iterating run the binned schedule */
+  int32_t reserved;
 } pdcs_options;
 
 typedef struct {
@@ -156,6 +163,8 @@ typedef struct {
   int64_t graph_launches;
   int64_t service_rounds;   /* batched checkpoint operations (exit checks, restart probes, copies) */
   int64_t single_fallbacks; /* instances re-solved alone for the resolving fallback */
+  int32_t spmv_tiled;       /* 1: the iteration graph ran the instance-tiled SpMV, 0: the binned one */
+  int32_t reserved;
 } pdcs_batch_info;
 
 /* Solve `count` independent conic programs together.  No counterpart in the

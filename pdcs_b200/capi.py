@@ -65,7 +65,8 @@ class PdcsOptions(C.Structure):
                 ("use_duality_gap_restart", C.c_int32), ("precision", C.c_int32),
                 ("duality_gap_restart_freq", C.c_int64), ("attempt_limit", C.c_int64),
                 ("stream", _vp), ("attempts_per_graph", C.c_int32), ("force_resolving", C.c_int32),
-                ("spmv_lane_nnz", C.c_int32), ("differentiable", C.c_int32)]
+                ("spmv_lane_nnz", C.c_int32), ("differentiable", C.c_int32),
+                ("spmv_tiles", C.c_int32), ("reserved", C.c_int32)]
 
 
 class PdcsResult(C.Structure):
@@ -87,7 +88,8 @@ class PdcsResult(C.Structure):
 class PdcsBatchInfo(C.Structure):
     _fields_ = [("setup_time", C.c_double), ("solve_time", C.c_double), ("time_iterations", C.c_double),
                 ("kernel_launches", C.c_int64), ("graph_launches", C.c_int64),
-                ("service_rounds", C.c_int64), ("single_fallbacks", C.c_int64)]
+                ("service_rounds", C.c_int64), ("single_fallbacks", C.c_int64),
+                ("spmv_tiled", C.c_int32), ("reserved", C.c_int32)]
 
 
 class PdcsGradOptions(C.Structure):

@@ -30,6 +30,7 @@
 #include "pdcs_adjoint.cuh"
 #include "pdcs_batch_kernels.cuh"
 #include "pdcs_bsearch.cuh"
+#include "pdcs_tiles.cuh"
 
 namespace pdcs {
 
@@ -320,6 +321,23 @@ class BatchSolver : public Solver {
   double* bs_prm_ = nullptr;    // K * 4
   double* bs_out_ = nullptr;    // K * 5
   int32_t* bs_list_ = nullptr;  // K
+  // instance-tiled SpMVs of the iteration graph: [0] G (rows y, columns x), [1] G'
+  struct Tiles {
+    TileCsr T{};
+    std::vector<int64_t> first;  // K + 1: tile range of every instance
+    std::vector<int64_t> nnz;    // nonzeros of every tile
+    int grid = 1;
+  } tl_[2];
+  bool tiled_ = false;
+  // a tile holds up to kTileNnz nonzeros (spmv_tiles > 0 sets it): small enough that
+  // the largest tiles do not leave SMs idle at the end, large enough that staging the
+  // instance's columns (from L2) stays a fraction of the stream; tiles of instances
+  // with few columns may hold up to 16 x their columns
+  static constexpr int64_t kTileNnz = 65536;
+  static constexpr int64_t kTileSmallNnz = 8192;
+  static constexpr int64_t kTileMaxRows = 4096;
+  static constexpr size_t kTileMaxSmem = 160 * 1024;
+  void setup_tiles();
   // iteration graphs: [0] grids for the whole batch, [1] the tail graph, grids
   // capped for rounds in which few nonzeros iterate (most CTAs of the full
   // grids would find no work and return, at the cost of their launch)
@@ -786,6 +804,104 @@ void BatchSolver::setup_compaction() {
   }
 }
 
+// Tiles of the instances' rows for both matrices (instance-tiled SpMV), when every
+// instance has at most kTileMaxCols columns in either matrix and its column
+// segment fits the shared-memory budget; otherwise the graph keeps the binned SpMV.
+void BatchSolver::setup_tiles() {
+  tiled_ = false;
+  if (O.spmv_tiles < 0) return;
+  int64_t maxc[2] = {0, 0};  // G: the instance's x; G': its y
+  for (int64_t k = 0; k < K_; ++k) {
+    maxc[0] = std::max<int64_t>(maxc[0], probs_[k].n);
+    maxc[1] = std::max<int64_t>(maxc[1], probs_[k].m);
+  }
+  if (maxc[0] > kTileMaxCols || maxc[1] > kTileMaxCols) return;
+  const size_t eb = fp32_ ? sizeof(float) : sizeof(double);
+  const size_t smem[2] = {2 * eb * (size_t)maxc[0], eb * (size_t)maxc[1]};  // G stages (x, x_lag) pairs
+  if (smem[0] > kTileMaxSmem || smem[1] > kTileMaxSmem) return;
+  auto up32 = [&](const std::vector<int64_t>& v) {
+    std::vector<int32_t> h(v.begin(), v.end());
+    int32_t* d = A.alloc<int32_t>(h.size());
+    PDCS_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));  // h is a temporary
+    return d;
+  };
+  int32_t* xloc = up32(xloc_);
+  int32_t* yloc = up32(yloc_);
+  std::vector<int32_t> rpt(n_ + 1);
+  PDCS_CUDA(cudaMemcpyAsync(rpt.data(), Gt_.rp, sizeof(int32_t) * (n_ + 1), cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  int dev = 0, sms = 148;
+  PDCS_CUDA(cudaGetDevice(&dev));
+  PDCS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  for (int w = 0; w < 2; ++w) {
+    Tiles& t = tl_[w];
+    const CsrDev& F = w ? Gt_ : G_;
+    const std::vector<int32_t>& rp = w ? rpt : h_rp_;
+    const std::vector<int64_t>& rs = w ? xrun_start_ : yrun_start_;  // row side
+    const std::vector<int64_t>& rl = w ? xrun_len_ : yrun_len_;
+    const std::vector<int64_t>& cs = w ? yrun_start_ : xrun_start_;  // column side
+    const int64_t R = w ? n_ : m_;
+    uint16_t* cl = A.alloc<uint16_t>(std::max<int64_t>(nnz_, 1));
+    RegionStarts reg{};
+    for (int q = 0; q < kMaxRuns; ++q) reg.s[q] = cs[q];  // instance 0 opens every type region
+    local_cols_kernel<<<grid_for(R), kThreads, 0, s_>>>(R, F.rp, F.ci, w ? ix_ : iy_, reg, w ? ry_.start : rx_.start,
+                                                        w ? yloc : xloc, cl);
+    std::vector<int4> tiles;
+    t.first.assign(K_ + 1, 0);
+    t.nnz.clear();
+    for (int64_t k = 0; k < K_; ++k) {
+      t.first[k] = (int64_t)tiles.size();
+      const int64_t ncols = w ? probs_[k].m : probs_[k].n;
+      const int64_t big = O.spmv_tiles > 0 ? (int64_t)O.spmv_tiles : kTileNnz;
+      const int64_t cap = std::min(big, std::max(kTileSmallNnz, 16 * ncols));
+      int64_t o = 0, ob = 0, acc = 0;
+      auto cut = [&](int64_t end) {
+        const int64_t rows = end - ob;
+        int g = 1;
+        while (g < 32 && kTileLN * g * rows < acc) g *= 2;  // about kTileLN nonzeros per lane
+        tiles.push_back(make_int4((int32_t)k, (int32_t)ob, (int32_t)end, g));
+        t.nnz.push_back(acc);
+        ob = end;
+        acc = 0;
+      };
+      for (int q = 0; q < kMaxRuns; ++q)
+        for (int64_t i = 0; i < rl[k * kMaxRuns + q]; ++i, ++o) {
+          const int64_t row = rs[k * kMaxRuns + q] + i;
+          acc += rp[row + 1] - rp[row];
+          if (acc >= cap || o + 1 - ob >= kTileMaxRows) cut(o + 1);
+        }
+      if (o > ob) cut(o);
+    }
+    t.first[K_] = (int64_t)tiles.size();
+    int4* dt = A.alloc<int4>(std::max<size_t>(tiles.size(), 1));
+    PDCS_CUDA(cudaMemcpyAsync(dt, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));  // tiles is a temporary
+    TileCsr& T = t.T;
+    T.rp = F.rp;
+    T.cl = cl;
+    T.tiles = dt;
+    T.ntiles = (int64_t)tiles.size();
+    T.act = A.alloc<int32_t>(std::max<size_t>(tiles.size(), 1));
+    T.n_act = A.alloc<int64_t>(1);
+    T.rows = w ? rx_ : ry_;
+    T.cols = w ? ry_ : rx_;
+    T.rloc = w ? xloc : yloc;
+    T.cloc = w ? yloc : xloc;
+    T.max_cols = (int32_t)maxc[w];
+    const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(2048 / kTileThreads, (size_t)(228 * 1024) / (smem[w] + 1024)));
+    t.grid = (int)std::max<int64_t>(1, std::min<int64_t>(T.ntiles, (int64_t)sms * per_sm));
+  }
+  if (fp32_) {
+    tile_prepare<float, kPair>(tl_[0].T);
+    tile_prepare<float, 1>(tl_[1].T);
+  } else {
+    tile_prepare<double, 2>(tl_[0].T);
+    tile_prepare<double, 1>(tl_[1].T);
+  }
+  tiled_ = true;
+}
+
 // Device buffers of the active work lists, sized for every instance iterating.
 void BatchSolver::setup_act_lists() {
   auto nchunks = [](int64_t len) { return (len + kThreads - 1) / kThreads; };
@@ -811,6 +927,7 @@ void BatchSolver::setup_act_lists() {
   act_inst_ = A.alloc<int32_t>(K_);
   n_act_ = A.alloc<int64_t>(1);
   bytes += nr * sizeof(int4) + K_ * sizeof(int32_t) + 2 * sizeof(int64_t) + 16 * 256;
+  if (tiled_) bytes += (size_t)(tl_[0].T.ntiles + tl_[1].T.ntiles) * sizeof(int32_t) + 4 * 256;
   act_bytes_ = bytes;
   const size_t need = pin_cap_ + bytes;
   PDCS_CUDA(cudaStreamSynchronize(s_));
@@ -911,6 +1028,21 @@ void BatchSolver::build_act_lists(const std::vector<Inst*>& its) {
   int32_t* hi = stage<int32_t>(std::max<size_t>(its.size(), 1));
   for (size_t i = 0; i < its.size(); ++i) hi[i] = (int32_t)its[i]->k;
   PDCS_CUDA(cudaMemcpyAsync(act_inst_, hi, sizeof(int32_t) * its.size(), cudaMemcpyHostToDevice, s_));
+  if (tiled_)
+    for (int w = 0; w < 2; ++w) {  // the iterating instances' tiles, largest first
+      const Tiles& t = tl_[w];
+      size_t cnt = 0;
+      for (Inst* I : its) cnt += (size_t)(t.first[I->k + 1] - t.first[I->k]);
+      int32_t* ht = stage<int32_t>(std::max<size_t>(cnt, 1));
+      int64_t* hnt = stage<int64_t>(1);
+      size_t j = 0;
+      for (Inst* I : its)
+        for (int64_t q = t.first[I->k]; q < t.first[I->k + 1]; ++q) ht[j++] = (int32_t)q;
+      std::stable_sort(ht, ht + cnt, [&](int32_t a, int32_t b) { return t.nnz[a] > t.nnz[b]; });
+      hnt[0] = (int64_t)cnt;
+      PDCS_CUDA(cudaMemcpyAsync(const_cast<int32_t*>(t.T.act), ht, sizeof(int32_t) * cnt, cudaMemcpyHostToDevice, s_));
+      PDCS_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(t.T.n_act), hnt, sizeof(int64_t), cudaMemcpyHostToDevice, s_));
+    }
 }
 
 // Rebuild the iteration graph's row lists from the rows of the masked instances.
@@ -954,6 +1086,7 @@ void BatchSolver::capture_batch_graph(int tail) {
   const int ctl_grid = tail ? (int)std::max<int64_t>(1, std::min<int64_t>(K_, cap))
                             : (int)std::max<int64_t>(1, std::min<int64_t>((K_ * 32 + kThreads - 1) / kThreads, 148 * 16));
   const int refl_grid = std::min(grid_reflect_, cap);
+  const int tgrid[2] = {std::min(tl_[0].grid, cap), std::min(tl_[1].grid, cap)};
   const bool timed = O.verbose >= 2;
   if (timed)
     for (cudaEvent_t& e : gev_[tail])
@@ -970,22 +1103,27 @@ void BatchSolver::capture_batch_graph(int tail) {
                  dgdy_, cur,  nxt,     done_ctas_, live_cnt_ + 2, act_inst_, n_act_};
     mark(0);
     if (fp32_) {
-      launch_spmv<1, false, float>(Gt32, dyl32_, nullptr, aty32_, nullptr, cur, s_);
+      if (tiled_ && !tail) launch_spmv_tile<float, 1>(tl_[1].T, tgrid[1], Gt32_.v, dyl32_, nullptr, aty32_, nullptr, cur, s_);
+      else launch_spmv<1, false, float>(Gt32, dyl32_, nullptr, aty32_, nullptr, cur, s_);
       mark(1);
       OpPrimalStep32B op1{xa_, dxp32_, qa_, aty32_, x, ix_, live_, ps_, dxsq_};
       launch_update_project(op1, XI, part_x, cur, s_);
       mark(2);
-      launch_spmv<kPair, false, float>(G32, &dxp32_->x, nullptr, gx32_, gxl32_, cur, s_);
+      if (tiled_ && !tail)
+        launch_spmv_tile<float, kPair>(tl_[0].T, tgrid[0], G32_.v, &dxp32_->x, nullptr, gx32_, gxl32_, cur, s_);
+      else launch_spmv<kPair, false, float>(G32, &dxp32_->x, nullptr, gx32_, gxl32_, cur, s_);
       mark(3);
       OpDualStep32B op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_};
       launch_update_project(op2, YI, part_y, cur, s_);
     } else {
-      launch_spmv<1>(Gt, yl, nullptr, aty, nullptr, cur, s_);
+      if (tiled_ && !tail) launch_spmv_tile<double, 1>(tl_[1].T, tgrid[1], Gt_.v, yl, nullptr, aty, nullptr, cur, s_);
+      else launch_spmv<1>(Gt, yl, nullptr, aty, nullptr, cur, s_);
       mark(1);
       OpPrimalStepB op1{xl, aty, c_s, x, ix_, live_, ps_, dxsq_};
       launch_update_project(op1, XI, part_x, cur, s_);
       mark(2);
-      launch_spmv<2>(G, x, xl, gx, gxl, cur, s_);
+      if (tiled_ && !tail) launch_spmv_tile<double, 2>(tl_[0].T, tgrid[0], G_.v, x, xl, gx, gxl, cur, s_);
+      else launch_spmv<2>(G, x, xl, gx, gxl, cur, s_);
       mark(3);
       OpDualStepB op2{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_};
       launch_update_project(op2, YI, part_y, cur, s_);
@@ -1226,7 +1364,12 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   // the graph's SpMVs run over the rows of the iterating instances only (rows of
   // instances that halt during these graphs are still computed; their products
   // are not read before the next attempt or anchor recomputes them)
-  compact(live_);
+  int64_t live_nnz = 0;
+  for (Inst* I : its) live_nnz += probs_[I->k].nnz;
+  // the tail graph (few nonzeros left) runs the binned SpMV over compacted rows;
+  // the full graph runs the instance tiles when the batch has them
+  const int tail = (live_nnz < kTailNnz && 16 * live_nnz < nnz_) ? 1 : 0;
+  if (!tiled_ || tail) compact(live_);
   build_act_lists(its);
   if (fp32_) {
     // FP64 anchors at the current iterates: for instances that (re)start
@@ -1242,9 +1385,6 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   int64_t graphs = (to_check + attempts_per_graph_ - 1) / attempts_per_graph_;
   graphs = std::max<int64_t>(1, std::min<int64_t>(graphs, 4));
   const double t_round = now_s();
-  int64_t live_nnz = 0;
-  for (Inst* I : its) live_nnz += probs_[I->k].nnz;
-  const int tail = (live_nnz < kTailNnz && 16 * live_nnz < nnz_) ? 1 : 0;
   if (O.verbose) {
     for (cudaEvent_t& e : round_ev_)
       if (!e) PDCS_CUDA(cudaEventCreate(&e));
@@ -1785,6 +1925,7 @@ int BatchSolver::prepare() {
   setup();
   setup_batch();
   setup_compaction();
+  setup_tiles();
   setup_act_lists();
   // the merged matrix lives on the device now (its row pointers stay for the adjoint's scatter)
   std::vector<int32_t>().swap(h_ci_);
@@ -1966,6 +2107,7 @@ int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_
     info->service_rounds = rounds_;
     info->single_fallbacks = fallbacks;
     info->time_iterations = t_iter_;
+    info->spmv_tiled = tiled_ ? 1 : 0;
   }
   return PDCS_OK;
 }

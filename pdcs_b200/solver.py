@@ -172,12 +172,15 @@ def _options_struct(L, hold: _Holder, *, n=0, m=0, rescaling_method: str = "ruiz
                     kkt_restart_freq: int = 2000, use_duality_gap_restart: bool = True,
                     duality_gap_restart_freq: int = 2000, attempt_limit: int = 0, attempts_per_graph: int = 32,
                     stream=None, force_resolving: bool = False, precision="fp64", spmv_lane_nnz: int = 0,
-                    differentiable: bool = False):
+                    differentiable: bool = False, spmv_tiles=True):
     """Fill a PdcsOptions from the reference's keyword arguments (rpdhg_alg_gpu_gen.jl:1219-1268).
 
     precision: "fp64" (the reference's arithmetic) or "fp32" (FP32 matrices and iterate deltas
     between FP64 anchors; FP64 projections, averages and termination checks).
-    spmv_lane_nnz: 0 autotunes the SpMV schedule per matrix; 1..16 fixes it (nonzeros per lane)."""
+    spmv_lane_nnz: 0 autotunes the SpMV schedule per matrix; 1..16 fixes it (nonzeros per lane).
+    spmv_tiles: batched solves run the instance-tiled SpMV (instance column segments staged in
+    shared memory) when every instance fits it; False keeps the binned row schedule; an int
+    sets the nonzeros per tile."""
     if method not in ("average", "halpern"):
         raise ValueError("method only available for :average and :halpern")
     if method == "halpern":
@@ -222,6 +225,12 @@ def _options_struct(L, hold: _Holder, *, n=0, m=0, rescaling_method: str = "ruiz
         raise ValueError("spmv_lane_nnz must be 0 (autotune) or a power of two up to 16")
     O.spmv_lane_nnz = spmv_lane_nnz
     O.differentiable = int(differentiable)
+    if spmv_tiles is True or spmv_tiles is False:
+        O.spmv_tiles = 0 if spmv_tiles else -1
+    elif int(spmv_tiles) > 0:
+        O.spmv_tiles = int(spmv_tiles)
+    else:
+        raise ValueError("spmv_tiles must be True, False or a positive number of nonzeros per tile")
     return O
 
 
@@ -274,6 +283,7 @@ class BatchInfo:
     graph_launches: int
     service_rounds: int
     single_fallbacks: int
+    spmv_tiled: bool = False
 
 
 class BatchHandle:
@@ -402,7 +412,8 @@ def rpdhg_gpu_grad(problem, x, y, dldx, dldy=None, rel_tol=1e-10, restart=100, m
 def _batch_info(B) -> "BatchInfo":
     return BatchInfo(setup_time=B.setup_time, solve_time=B.solve_time, time_iterations=B.time_iterations,
                      kernel_launches=B.kernel_launches, graph_launches=B.graph_launches,
-                     service_rounds=B.service_rounds, single_fallbacks=B.single_fallbacks)
+                     service_rounds=B.service_rounds, single_fallbacks=B.single_fallbacks,
+                     spmv_tiled=bool(B.spmv_tiled))
 
 
 def rpdhg_gpu_solve_batch(problems, **options):

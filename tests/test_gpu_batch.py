@@ -122,3 +122,25 @@ def test_batch_handle_resolves_identically(cuda):
         assert np.array_equal(x.primal, y.primal) and x.info.iter == 50  # cold start each time
         assert z.info.exit_status == w.info.exit_status == "optimal"
         assert z.info.iter == w.info.iter and np.array_equal(z.primal, w.primal)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_tiled_spmv_matches_binned(cuda, precision):
+    """The instance-tiled SpMV (column segments in shared memory, 16-bit local
+    columns, FP64 sums) and the binned row schedule give the same iterates up to
+    summation order, and the same solutions."""
+    batch = _mixed_batch() + problems.batch_socp_c3(count=12, seed=3, nmin=50, nmax=1500)
+    # FP32: the binned kernel sums in FP32, the tiled one in FP64; the adaptive
+    # steps amplify that difference over attempts, so FP32 compares early iterates
+    attempts, tol = (60, 1e-10) if precision == "fp64" else (7, 2e-5)
+    a, ia = solver.rpdhg_gpu_solve_batch(batch, attempt_limit=attempts, precision=precision)
+    b, ib = solver.rpdhg_gpu_solve_batch(batch, attempt_limit=attempts, precision=precision, spmv_tiles=False)
+    assert ia.spmv_tiled and not ib.spmv_tiled
+    for p, g, h in zip(batch, a, b):
+        for u, v in ((g.primal, h.primal), (g.dual, h.dual)):
+            assert np.abs(u - v).max() <= tol * max(1.0, np.abs(v).max()), (p.name, np.abs(u - v).max())
+    a, _ = solver.rpdhg_gpu_solve_batch(batch, precision=precision)
+    b, _ = solver.rpdhg_gpu_solve_batch(batch, precision=precision, spmv_tiles=False)
+    for p, g, h in zip(batch, a, b):
+        assert g.info.exit_status == h.info.exit_status == "optimal", p.name
+        assert abs(g.info.pObj - h.info.pObj) <= 1e-4 * (1.0 + abs(h.info.pObj)), p.name
