@@ -1013,7 +1013,7 @@ void BatchSolver::build_act_lists(const std::vector<Inst*>& its) {
       const std::vector<int64_t>& rl = w ? yrun_len_ : xrun_len_;
       for (int q = 0; q < kMaxRuns; ++q)
         chunks(rs[I->k * kMaxRuns + q], rl[I->k * kMaxRuns + q],
-               [&](int64_t a, int64_t l) { rc.push_back(make_int4((int32_t)a, (int32_t)l, w, 0)); });
+               [&](int64_t a, int64_t l) { rc.push_back(make_int4((int32_t)a, (int32_t)l, w, (int32_t)I->k)); });
     }
   int64_t* hn = stage<int64_t>(2);
   hn[0] = (int64_t)rc.size();
@@ -1133,11 +1133,10 @@ void BatchSolver::capture_batch_graph(int tail) {
     else batch_control_kernel<false><<<ctl_grid, kThreads, 0, s_>>>(K_, ctl);
     mark(5);
     if (fp32_)
-      batch_reflect32_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, dxp32_, dxm_, dy32_, dyl32_, dym_,
-                                                             rchunk_, n_rchunk_);
+      batch_reflect32_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, dxp32_, dxm_, dy32_, dyl32_, dym_, rchunk_,
+                                                             n_rchunk_);
     else
-      batch_reflect_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, ix_, iy_, x, xl, xm, y, yl, ym, rchunk_,
-                                                           n_rchunk_);
+      batch_reflect_kernel<<<refl_grid, kThreads, 0, s_>>>(cur, sts_, x, xl, xm, y, yl, ym, rchunk_, n_rchunk_);
     mark(6);
   }
   PDCS_CUDA(cudaStreamEndCapture(s_, &bgraph_[tail]));

@@ -315,12 +315,10 @@ __global__ void __launch_bounds__(kThreads) batch_control_kernel(int64_t K, Batc
 
 // Reflection + eta-weighted averaging with per-instance coefficients
 // (reflect_kernel per instance); runs when the attempt's control step ran.
-// Work: the chunks {first element, length <= kThreads, 0 = x / 1 = y} of the
-// iterating instances, a CTA per chunk.
+// Work: the chunks {first element, length <= kThreads, 0 = x / 1 = y, instance}
+// of the iterating instances, a warp per chunk.
 __global__ void __launch_bounds__(kThreads) batch_reflect_kernel(const int32_t* __restrict__ live_cur,
                                                                 const PdhgState* __restrict__ sts,
-                                                                const int32_t* __restrict__ ix,
-                                                                const int32_t* __restrict__ iy,
                                                                 double* __restrict__ x, double* __restrict__ xl,
                                                                 double* __restrict__ xm, double* __restrict__ y,
                                                                 double* __restrict__ yl, double* __restrict__ ym,
@@ -328,22 +326,24 @@ __global__ void __launch_bounds__(kThreads) batch_reflect_kernel(const int32_t* 
                                                                 const int64_t* __restrict__ n_rchunk) {
   if (*live_cur == 0) return;
   const int64_t nch = *n_rchunk;
-  for (int64_t q = blockIdx.x; q < nch; q += gridDim.x) {
-    const int4 ch = rchunk[q];
-    if ((int)threadIdx.x >= ch.y) continue;
-    const bool isx = ch.z == 0;
-    const int64_t j = (int64_t)ch.x + threadIdx.x;
-    const PdhgState& s = sts[isx ? ix[j] : iy[j]];
+  const int lane = threadIdx.x & 31;
+  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nch; q += wstride) {
+    const int4 ch = rchunk[q];  // {first element, length, 0 = x / 1 = y, instance}: a warp per chunk
+    const PdhgState& s = sts[ch.w];
     if (!s.do_reflect) continue;
-    double* v = isx ? x : y;
-    double* vl = isx ? xl : yl;
-    double* vm = isx ? xm : ym;
+    double* v = ch.z == 0 ? x : y;
+    double* vl = ch.z == 0 ? xl : yl;
+    double* vm = ch.z == 0 ? xm : ym;
     const double tmp = s.refl_tmp, inv = s.refl_inv, e = s.refl_extra, eta = s.refl_eta, cum = s.refl_cum;
-    const double cur = v[j];
-    const double nv = tmp * ((1.0 + e) * cur - e * vl[j]) + inv * cur;
-    vm[j] = (vm[j] * cum + nv * eta) / (cum + eta);
-    v[j] = nv;
-    vl[j] = nv;
+    for (int i = lane; i < ch.y; i += 32) {
+      const int64_t j = (int64_t)ch.x + i;
+      const double cur = v[j];
+      const double nv = tmp * ((1.0 + e) * cur - e * vl[j]) + inv * cur;
+      vm[j] = (vm[j] * cum + nv * eta) / (cum + eta);
+      v[j] = nv;
+      vl[j] = nv;
+    }
   }
 }
 

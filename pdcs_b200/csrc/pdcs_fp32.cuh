@@ -167,11 +167,9 @@ __global__ void __launch_bounds__(kThreads) reflect32_kernel(const PdhgState* __
   }
 }
 
-// batch_reflect_kernel on the deltas: the chunks of the iterating instances, a CTA per chunk
+// batch_reflect_kernel on the deltas: the chunks of the iterating instances, a warp per chunk
 __global__ void __launch_bounds__(kThreads) batch_reflect32_kernel(const int32_t* __restrict__ live_cur,
                                                                   const PdhgState* __restrict__ sts,
-                                                                  const int32_t* __restrict__ ix,
-                                                                  const int32_t* __restrict__ iy,
                                                                   float2* __restrict__ dxp,
                                                                   double* __restrict__ dxm, float* __restrict__ dy,
                                                                   float* __restrict__ dyl, double* __restrict__ dym,
@@ -179,15 +177,17 @@ __global__ void __launch_bounds__(kThreads) batch_reflect32_kernel(const int32_t
                                                                   const int64_t* __restrict__ n_rchunk) {
   if (*live_cur == 0) return;
   const int64_t nch = *n_rchunk;
-  for (int64_t q = blockIdx.x; q < nch; q += gridDim.x) {
-    const int4 ch = rchunk[q];
-    if ((int)threadIdx.x >= ch.y) continue;
-    const bool isx = ch.z == 0;
-    const int64_t j = (int64_t)ch.x + threadIdx.x;
-    const PdhgState& s = sts[isx ? ix[j] : iy[j]];
+  const int lane = threadIdx.x & 31;
+  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nch; q += wstride) {
+    const int4 ch = rchunk[q];  // {first element, length, 0 = x / 1 = y, instance}
+    const PdhgState& s = sts[ch.w];
     if (!s.do_reflect) continue;
-    if (isx) reflect32_x(s, dxp, dxm, j);
-    else reflect32_y(s, dy, dyl, dym, j);
+    for (int i = lane; i < ch.y; i += 32) {
+      const int64_t j = (int64_t)ch.x + i;
+      if (ch.z == 0) reflect32_x(s, dxp, dxm, j);
+      else reflect32_y(s, dy, dyl, dym, j);
+    }
   }
 }
 
