@@ -31,6 +31,7 @@
 #include "pdcs_batch_kernels.cuh"
 #include "pdcs_bsearch.cuh"
 #include "pdcs_tiles.cuh"
+#include "pdcs_tail.cuh"
 
 namespace pdcs {
 
@@ -354,6 +355,9 @@ class BatchSolver : public Solver {
   static constexpr int kTailCtas = 148;       // CTAs per part of the other kernels
   // the tail graph runs while fewer than kTailNnz nonzeros, and 1/16 of the batch's, iterate
   static constexpr int64_t kTailNnz = 1 << 20;
+  // ... and when none of the iterating instances has more than kTailCtaNnz nonzeros,
+  // tail_attempts_kernel runs them instead, a CTA per instance looping over its attempts
+  static constexpr int64_t kTailCtaNnz = 32768;
   // active-row lists of G (0) and G' (1) for the iteration graph
   struct Compact {
     int4* rows = nullptr;
@@ -1368,7 +1372,10 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   // the tail graph (few nonzeros left) runs the binned SpMV over compacted rows;
   // the full graph runs the instance tiles when the batch has them
   const int tail = (live_nnz < kTailNnz && 16 * live_nnz < nnz_) ? 1 : 0;
-  if (!tiled_ || tail) compact(live_);
+  int64_t max_nnz = 0;
+  for (Inst* I : its) max_nnz = std::max<int64_t>(max_nnz, probs_[I->k].nnz);
+  const bool cta_tail = tail && max_nnz <= kTailCtaNnz;
+  if (!cta_tail && (!tiled_ || tail)) compact(live_);
   build_act_lists(its);
   if (fp32_) {
     // FP64 anchors at the current iterates: for instances that (re)start
@@ -1389,10 +1396,37 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
       if (!e) PDCS_CUDA(cudaEventCreate(&e));
     PDCS_CUDA(cudaEventRecord(round_ev_[0], s_));
   }
-  for (int64_t gi = 0; gi < graphs; ++gi) {
-    PDCS_CUDA(cudaGraphLaunch(bgraph_exec_[tail], s_));
-    graphs_++;
-    kernels_ += 6LL * attempts_per_graph_;
+  if (cta_tail) {
+    TailArgs T{};
+    T.list = act_inst_;
+    T.max_attempts = (int32_t)(graphs * attempts_per_graph_);
+    T.ctl = BatchCtl{sts_,   ps_,     ds_,         live_, rx_,    ry_,       dxsq_,  dysq_,
+                     dgdy_,  nullptr, nullptr,     nullptr, nullptr, act_inst_, n_act_};
+    T.X = XI;
+    T.Y = YI;
+    T.cones_x = cones_dev_[0];
+    T.cones_y = cones_dev_[1];
+    const int grid = (int)its.size();
+    if (fp32_) {
+      TailFP32 pk{Gt32_, G32_,
+                  OpPrimalStep32B{xa_, dxp32_, qa_, aty32_, x, ix_, live_, ps_, dxsq_},
+                  OpDualStep32B{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_},
+                  dxp32_, dxm_, dy32_, dyl32_, dym_, aty32_, gx32_, gxl32_};
+      tail_attempts_kernel<TailFP32><<<grid, kThreads, 0, s_>>>(T, pk);
+    } else {
+      TailFP64 pk{Gt_, G_, OpPrimalStepB{xl, aty, c_s, x, ix_, live_, ps_, dxsq_},
+                  OpDualStepB{yl, gx, gxl, h_s, y, iy_, live_, ds_, dysq_, dgdy_},
+                  x, xl, xm, y, yl, ym, aty, gx, gxl};
+      tail_attempts_kernel<TailFP64><<<grid, kThreads, 0, s_>>>(T, pk);
+    }
+    PDCS_CUDA(cudaGetLastError());
+    kernels_++;
+  } else {
+    for (int64_t gi = 0; gi < graphs; ++gi) {
+      PDCS_CUDA(cudaGraphLaunch(bgraph_exec_[tail], s_));
+      graphs_++;
+      kernels_ += 6LL * attempts_per_graph_;
+    }
   }
   if (O.verbose) PDCS_CUDA(cudaEventRecord(round_ev_[1], s_));
   PdhgState* back = stage<PdhgState>(K_);
@@ -1402,7 +1436,7 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
     float dev = 0.0f;
     PDCS_CUDA(cudaEventElapsedTime(&dev, round_ev_[0], round_ev_[1]));
     dev_ms_ += dev;
-    if (O.verbose >= 2 && gev_[tail][0]) {  // the kernels of the round's last attempt
+    if (O.verbose >= 2 && gev_[tail][0] && !cta_tail) {  // the kernels of the round's last attempt
       for (int i = 0; i < 6; ++i) {
         float e = 0.0f;
         PDCS_CUDA(cudaEventElapsedTime(&e, gev_[tail][i], gev_[tail][i + 1]));
@@ -1412,7 +1446,7 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
     }
     std::printf("[pdcs_b200 batch] %.3f s: %zu of %lld instances iterating, %lld attempts in %.3f ms (device %.3f ms)%s\n",
                 now_s() - t_start_, its.size(), (long long)K_, (long long)(graphs * attempts_per_graph_),
-                1e3 * (now_s() - t_round), dev, tail ? " (tail graph)" : "");
+                1e3 * (now_s() - t_round), dev, cta_tail ? " (tail kernel)" : tail ? " (tail graph)" : "");
   }
   const bool timeout = O.time_limit > 0 && now_s() - t_start_ > O.time_limit;
   std::vector<Inst*> halted;
