@@ -178,17 +178,31 @@ __device__ void bs_project(const Op& op, const ConeTable& T, const RunTable& R, 
 }
 
 // out[i] = A_i . v (then scaled: a out[i] + b w[i]) for the rows in runs r0 .. r1 - 1 of
-// instance k, a warp per row; CTA-collective, ends with a barrier.
+// instance k: groups of g lanes per row (about two nonzeros per lane from the rows'
+// mean length), so short rows keep the CTA's lanes busy; CTA-collective, ends with a barrier.
 __device__ void bs_rows(const CsrDev& A, const RunTable& R, int r0, int r1, int64_t k, const double* v, double* out,
                         double a, double b, const double* w) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t rows = 0, nz = 0;
   for (int q = r0; q < r1; ++q) {
     const int64_t s0 = R.start[k * kMaxRuns + q], L = R.len[k * kMaxRuns + q];
-    for (int64_t i = s0 + warp; i < s0 + L; i += kWarps) {
+    rows += L;
+    if (L) nz += A.rp[s0 + L] - A.rp[s0];
+  }
+  int g = 1;
+  while (g < 32 && 2 * g * rows < nz) g *= 2;
+  const int gl = lane & (g - 1), per = 32 / g;
+  for (int q = r0; q < r1; ++q) {
+    const int64_t s0 = R.start[k * kMaxRuns + q], s1 = s0 + R.len[k * kMaxRuns + q];
+    // the loop bound is uniform across the warp (every lane reaches the shuffles)
+    for (int64_t ib = s0 + (int64_t)warp * per; ib < s1; ib += (int64_t)kWarps * per) {
+      const int64_t i = ib + lane / g;
+      const bool valid = i < s1;
       double s = 0.0;
-      for (int32_t e = A.rp[i] + lane; e < A.rp[i + 1]; e += 32) s = fma(A.v[e], v[A.ci[e]], s);
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
-      if (lane == 0) out[i] = w ? a * s + b * w[i] : s;
+      if (valid)
+        for (int32_t e = A.rp[i] + gl; e < A.rp[i + 1]; e += g) s = fma(A.v[e], v[A.ci[e]], s);
+      for (int o = g >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o, g);
+      if (valid && gl == 0) out[i] = w ? a * s + b * w[i] : s;
     }
   }
   __syncthreads();
