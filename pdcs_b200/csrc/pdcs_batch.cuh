@@ -272,8 +272,12 @@ class BatchSolver : public Solver {
   int64_t K_;
   const pdcs_problem* probs_;
   // merged host problem
-  std::vector<int32_t> h_rp_, h_ci_;
-  std::vector<double> h_v_, h_c_, h_h_, h_bl_, h_bu_;
+  std::vector<int32_t> h_rp_;
+  std::vector<int64_t> h_src_, nnz_off_;  // per merged row: its first nonzero in the instance-concatenated arrays
+  std::vector<double> h_c_, h_h_, h_bl_, h_bu_;
+  int32_t dummy_ci_ = 0;  // the merged matrix is assembled on the device (upload_matrix);
+  double dummy_v_ = 0.0;  // these only stand for its column / value arrays in the host checks
+  void upload_matrix(int32_t* g_rp, int32_t* g_ci, double* g_v) override;
   std::vector<int64_t> h_socx_, h_rsocx_, h_socG_, h_rsocG_;
   // per instance: offsets of its runs in the merged vectors and local starts
   std::vector<int64_t> xrun_start_, xrun_len_, yrun_start_, yrun_len_;  // K * kMaxRuns
@@ -534,12 +538,16 @@ void BatchSolver::merge() {
     }
   }
   // row lengths in merged order, then the merged CSR
-  std::vector<int64_t> nnz_off(K + 1, 0);
-  for (int64_t k = 0; k < K; ++k) nnz_off[k + 1] = nnz_off[k] + probs_[k].nnz;
+  std::vector<int64_t>& nnz_off = nnz_off_;
+  nnz_off.assign(K + 1, 0);
+  for (int64_t k = 0; k < K; ++k) {
+    const pdcs_problem& q = probs_[k];
+    if (q.m > 0 && q.G_rowptr[q.m] - q.G_rowptr[0] != q.nnz) throw std::invalid_argument("csr");
+    nnz_off[k + 1] = nnz_off[k] + probs_[k].nnz;
+  }
   if (N > INT32_MAX || M > INT32_MAX || nnz_off[K] > INT32_MAX) throw std::invalid_argument("batch too large");
   h_rp_.assign(M + 1, 0);
-  h_ci_.resize(nnz_off[K]);
-  h_v_.resize(nnz_off[K]);
+  h_src_.assign(M, 0);
   h_c_.resize(N);
   h_h_.resize(M);
   h_ix_.resize(N);
@@ -569,7 +577,11 @@ void BatchSolver::merge() {
   };
   parallel([&](int64_t k) {
     const pdcs_problem& q = probs_[k];
-    for (int64_t i = 0; i < q.m; ++i) h_rp_[posy(k, i) + 1] = q.G_rowptr[i + 1] - q.G_rowptr[i];
+    for (int64_t i = 0; i < q.m; ++i) {
+      const int64_t r = posy(k, i);
+      h_rp_[r + 1] = q.G_rowptr[i + 1] - q.G_rowptr[i];
+      h_src_[r] = nnz_off[k] + (q.G_rowptr[i] - q.G_rowptr[0]);
+    }
     for (int64_t j = 0; j < q.n; ++j) {
       const int64_t p = posx(k, j);
       h_c_[p] = q.c[j];
@@ -586,17 +598,6 @@ void BatchSolver::merge() {
     }
   });
   for (int64_t i = 0; i < M; ++i) h_rp_[i + 1] += h_rp_[i];
-  parallel([&](int64_t k) {
-    const pdcs_problem& q = probs_[k];
-    // local column -> merged column, run by run
-    for (int64_t i = 0; i < q.m; ++i) {
-      int64_t dst = h_rp_[posy(k, i)];
-      for (int64_t e = q.G_rowptr[i]; e < q.G_rowptr[i + 1]; ++e, ++dst) {
-        h_ci_[dst] = (int32_t)posx(k, q.G_colind[e]);
-        h_v_[dst] = q.G_val[e];
-      }
-    }
-  });
   for (int w = 0; w < 2; ++w) cones_[w].assign(K, {});
   for (int64_t k = 0; k < K; ++k) {
     const pdcs_problem& q = probs_[k];
@@ -652,8 +653,8 @@ void BatchSolver::merge() {
   mp.nb = NB;
   mp.nnz = nnz_off[K];
   mp.G_rowptr = h_rp_.data();
-  mp.G_colind = h_ci_.data();
-  mp.G_val = h_v_.data();
+  mp.G_colind = &dummy_ci_;
+  mp.G_val = &dummy_v_;
   mp.c = h_c_.data();
   mp.h = h_h_.data();
   mp.bl = h_bl_.data();
@@ -676,6 +677,48 @@ void BatchSolver::merge() {
   mp.n_rsoc_x = (int64_t)h_rsocx_.size();
   mp.on_device = 0;
   P = mp;
+}
+
+// The merged CSR of G, assembled on the device: every instance's column
+// indices and values are uploaded as they are (concatenated in instance
+// order), then merge_cols_kernel moves each merged row's nonzeros into place
+// with the columns mapped to their merged positions (and checked against the
+// instance's column count).
+void BatchSolver::upload_matrix(int32_t* g_rp, int32_t* g_ci, double* g_v) {
+  const int64_t K = K_;
+  PDCS_CUDA(cudaMemcpyAsync(g_rp, h_rp_.data(), sizeof(int32_t) * (m_ + 1), cudaMemcpyHostToDevice, s_));
+  if (nnz_ == 0) return;
+  int32_t* ci_in = A.alloc<int32_t>(nnz_);
+  double* v_in = A.alloc<double>(nnz_);
+  for (int64_t k = 0; k < K; ++k) {
+    const pdcs_problem& q = probs_[k];
+    if (!q.nnz) continue;
+    const int64_t o = q.G_rowptr[0];
+    PDCS_CUDA(cudaMemcpyAsync(ci_in + nnz_off_[k], q.G_colind + o, sizeof(int32_t) * q.nnz, cudaMemcpyHostToDevice, s_));
+    PDCS_CUDA(cudaMemcpyAsync(v_in + nnz_off_[k], q.G_val + o, sizeof(double) * q.nnz, cudaMemcpyHostToDevice, s_));
+  }
+  std::vector<int64_t> ncol(K);
+  for (int64_t k = 0; k < K; ++k) ncol[k] = probs_[k].n;
+  int64_t* src = A.alloc<int64_t>(m_);
+  int32_t* row_inst = A.alloc<int32_t>(m_);
+  int64_t* xs = A.alloc<int64_t>(K * kMaxRuns);
+  int64_t* xl = A.alloc<int64_t>(K * kMaxRuns);
+  int64_t* nc = A.alloc<int64_t>(K);
+  int32_t* err = A.alloc<int32_t>(1);
+  PDCS_CUDA(cudaMemcpyAsync(src, h_src_.data(), sizeof(int64_t) * m_, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(row_inst, h_iy_.data(), sizeof(int32_t) * m_, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(xs, xrun_start_.data(), sizeof(int64_t) * K * kMaxRuns, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(xl, xloc_.data(), sizeof(int64_t) * K * kMaxRuns, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemcpyAsync(nc, ncol.data(), sizeof(int64_t) * K, cudaMemcpyHostToDevice, s_));
+  PDCS_CUDA(cudaMemsetAsync(err, 0, sizeof(int32_t), s_));
+  merge_cols_kernel<<<warp_grid(m_), kThreads, 0, s_>>>(m_, g_rp, src, row_inst, ci_in, v_in, xs, xl, nc, g_ci, g_v, err);
+  int32_t h_err = 0;
+  PDCS_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));  // also keeps ncol alive for its copy
+  for (const void* p : {(const void*)ci_in, (const void*)v_in, (const void*)src, (const void*)row_inst,
+                        (const void*)xs, (const void*)xl, (const void*)nc, (const void*)err})
+    A.drop(p);
+  if (h_err) throw std::invalid_argument("csr");
 }
 
 void BatchSolver::setup_batch() {
@@ -1951,18 +1994,21 @@ int BatchSolver::prepare() {
   if (rc != PDCS_OK) return rc;
   const double t0 = now_s();
   merge();
+  if (O.verbose) std::printf("[pdcs_b200 setup] %-28s %8.3f ms\n", "merge (host)", 1e3 * (now_s() - t0));
   rc = validate();
   if (rc != PDCS_OK) return rc;
   inst_of_y_ = h_iy_.data();
   inst_of_x_ = h_ix_.data();
   setup();
   setup_batch();
+  phase("batch constants");
   setup_compaction();
   setup_tiles();
+  phase("compaction, tiles");
   setup_act_lists();
+  phase("active lists");
   // the merged matrix lives on the device now (its row pointers stay for the adjoint's scatter)
-  std::vector<int32_t>().swap(h_ci_);
-  std::vector<double>().swap(h_v_);
+  std::vector<int64_t>().swap(h_src_);
   if (!O.differentiable) std::vector<int32_t>().swap(h_rp_);
   if (O.differentiable) {
     xs_raw_ = A.alloc<double>(n_);

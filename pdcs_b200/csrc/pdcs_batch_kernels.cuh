@@ -188,6 +188,35 @@ __global__ void __launch_bounds__(kThreads) seg_reduce_kernel(int64_t K, const u
   }
 }
 
+// The merged CSR's nonzeros from the instance-concatenated uploads, a warp per
+// merged row: local column j of instance k -> its merged position (the last x
+// run of k starting at or before j).  err: a column outside its instance.
+__global__ void merge_cols_kernel(int64_t M, const int32_t* __restrict__ rp, const int64_t* __restrict__ src,
+                                  const int32_t* __restrict__ row_inst, const int32_t* __restrict__ ci_in,
+                                  const double* __restrict__ v_in, const int64_t* __restrict__ xrun_start,
+                                  const int64_t* __restrict__ xloc, const int64_t* __restrict__ ncol,
+                                  int32_t* __restrict__ ci, double* __restrict__ v, int32_t* __restrict__ err) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < M; r += wstride) {
+    const int64_t k = row_inst[r];
+    const int64_t s0 = src[r], d0 = rp[r], len = rp[r + 1] - rp[r];
+    for (int64_t e = lane; e < len; e += 32) {
+      const int64_t j = ci_in[s0 + e];
+      int64_t c = 0;
+      if (j < 0 || j >= ncol[k]) {
+        *err = 1;
+      } else {
+        int t = kMaxRuns - 1;
+        while (t > 0 && j < xloc[k * kMaxRuns + t]) --t;
+        c = xrun_start[k * kMaxRuns + t] + (j - xloc[k * kMaxRuns + t]);
+      }
+      ci[d0 + e] = (int32_t)c;
+      v[d0 + e] = v_in[s0 + e];
+    }
+  }
+}
+
 // Control of one batched attempt.  live_cur / live_next: the number of live
 // instances at the start of this attempt and of the next one (two slots used
 // alternately by consecutive attempts of a graph).  The contributions of an

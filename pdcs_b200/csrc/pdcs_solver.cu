@@ -475,6 +475,24 @@ class Solver {
   // ---- setup ----
   int validate();
   void setup();
+  // G's CSR arrays onto the device (the batch assembles its merged matrix there)
+  virtual void upload_matrix(int32_t* g_rp, int32_t* g_ci, double* g_v) {
+    const cudaMemcpyKind kind = P.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    PDCS_CUDA(cudaMemcpyAsync(g_rp, P.G_rowptr, sizeof(int32_t) * (m_ + 1), kind, s_));
+    if (nnz_) {
+      PDCS_CUDA(cudaMemcpyAsync(g_ci, P.G_colind, sizeof(int32_t) * nnz_, kind, s_));
+      PDCS_CUDA(cudaMemcpyAsync(g_v, P.G_val, sizeof(double) * nnz_, kind, s_));
+    }
+  }
+  // verbose: wall time of each setup phase, the stream synchronised at every mark
+  double phase_t_ = 0.0;
+  void phase(const char* name) {
+    if (!O.verbose) return;
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    const double t = now_s();
+    if (phase_t_ > 0.0) std::printf("[pdcs_b200 setup] %-28s %8.3f ms\n", name, 1e3 * (t - phase_t_));
+    phase_t_ = t;
+  }
   void build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
                   const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst, int lane_nnz);
   int tune_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp, const int32_t* d_ci,
@@ -916,6 +934,8 @@ void Solver::setup() {
     own_stream_ = true;
   }
   A.bind(s_);
+  phase_t_ = 0.0;
+  phase("start");
   PDCS_CUDA(cudaMallocHost(&host_state_, sizeof(PdhgState)));
   PDCS_CUDA(cudaMallocHost(&host_red_, 64 * sizeof(double)));
   part_r = A.alloc<double>((size_t)148 * 8 * 8);
@@ -934,13 +954,12 @@ void Solver::setup() {
   auto put = [&](void* dst, const void* src, size_t bytes) {
     if (bytes) PDCS_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, s_));
   };
-  put(g_rp, P.G_rowptr, sizeof(int32_t) * (m_ + 1));
-  put(g_ci, P.G_colind, sizeof(int32_t) * nnz_);
-  put(g_v, P.G_val, sizeof(double) * nnz_);
+  upload_matrix(g_rp, g_ci, g_v);
   put(c_raw, P.c, sizeof(double) * n_);
   put(h_raw, P.h, sizeof(double) * m_);
   put(bl_raw, P.bl, sizeof(double) * nb_);
   put(bu_raw, P.bu, sizeof(double) * nb_);
+  phase("upload");
   // ---- input checks ----
   int32_t* d_err = A.alloc<int32_t>(1);
   PDCS_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int32_t), s_));
@@ -969,6 +988,7 @@ void Solver::setup() {
     cNrm1 = r[0];
     cNrmInf = r[1];
   }
+  phase("input checks, norms");
   // ---- G' structure: stable radix sort of the column keys keeps G's row order ----
   int32_t* row_of = A.alloc<int32_t>(nnz_);
   int32_t* t_rp = A.alloc<int32_t>(n_ + 1);
@@ -991,6 +1011,7 @@ void Solver::setup() {
     if (nnz_ > 0)
       PDCS_CUDA(cub::DeviceRadixSort::SortPairs(tmp, b2, g_ci, keys_sorted, perm_in, perm_t, (int)nnz_, 0, bits, s_));
   }
+  phase("transpose");
   // ---- Ruiz (10) + Pock-Chambolle (alpha = 1) equilibration on the device ----
   c_s = A.alloc<double>(n_);
   Dr = A.alloc<double>(n_);
@@ -1042,6 +1063,7 @@ void Solver::setup() {
   bl_fin = A.alloc<double>(nb_); bu_fin = A.alloc<double>(nb_);
   if (nb_ > 0)
     box_aux_kernel<<<grid_for(nb_), kThreads, 0, s_>>>(nb_, bl_raw, bu_raw, bl_fin, bu_fin, lam_l, lam_u);
+  phase("equilibration");
   // ---- SpMV row bins (host sees only the two row-pointer arrays) ----
   std::vector<int32_t> rp_h(m_ + 1), trp_h(n_ + 1);
   PDCS_CUDA(cudaMemcpyAsync(rp_h.data(), g_rp, sizeof(int32_t) * (m_ + 1), cudaMemcpyDeviceToHost, s_));
@@ -1067,6 +1089,7 @@ void Solver::setup() {
   }
   copy(xl, x, n_); copy(xm, x, n_); copy(xbest, x, n_);
   copy(yl, y, m_); copy(ym, y, m_); copy(ybest, y, m_);
+  phase("row bins, work vectors");
   // ---- SpMV schedules: autotuned per matrix unless fixed by the options ----
   lane_G_ = tune_bins(rp_h, m_, n_, g_rp, g_ci, g_v, G_, inst_of_y_, x, tm[0]);
   lane_Gt_ = tune_bins(trp_h, n_, m_, t_rp, t_ci, t_v, Gt_, inst_of_x_, y, tn[0]);
@@ -1081,6 +1104,7 @@ void Solver::setup() {
   // cone tables
   std::vector<int64_t> soc_x(P.soc_x, P.soc_x + P.n_soc_x), rsoc_x(P.rsoc_x, P.rsoc_x + P.n_rsoc_x);
   std::vector<int64_t> socG(P.socG, P.socG + P.n_socG), rsocG(P.rsocG, P.rsocG + P.n_rsocG);
+  phase("SpMV schedules");
   build_tables(soc_x, rsoc_x, socG, rsocG);
   int maxgrid = std::max({XI.ctaA + XI.ctaB + XI.ctaC, YI.ctaA + YI.ctaB + YI.ctaC, SLK.ctaA + SLK.ctaB + SLK.ctaC,
                           CON.ctaA + CON.ctaB + CON.ctaC, 148 * 8});
@@ -1093,7 +1117,9 @@ void Solver::setup() {
   PDCS_CUDA(cudaMemsetAsync(st_dev, 0, sizeof(PdhgState), s_));
   grid_reflect_ = grid_for(std::max(n_, m_));
   attempts_per_graph_ = O.attempts_per_graph > 0 ? O.attempts_per_graph : 32;
+  phase("cone tables");
   if (O.precision == 1) setup_fp32();
+  phase("FP32 copies");
   PDCS_CUDA(cudaStreamSynchronize(s_));
 }
 
