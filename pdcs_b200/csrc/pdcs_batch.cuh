@@ -1442,7 +1442,8 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
   if (cta_tail) {
     TailArgs T{};
     T.list = act_inst_;
-    T.max_attempts = (int32_t)(graphs * attempts_per_graph_);
+    // the loop re-anchors by itself, so a tail round runs up to the next checkpoint
+    T.max_attempts = (int32_t)std::max<int64_t>(graphs * attempts_per_graph_, std::min<int64_t>(to_check, 1 << 20));
     T.ctl = BatchCtl{sts_,   ps_,     ds_,         live_, rx_,    ry_,       dxsq_,  dysq_,
                      dgdy_,  nullptr, nullptr,     nullptr, nullptr, act_inst_, n_act_};
     T.X = XI;
@@ -1454,7 +1455,8 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
       TailFP32 pk{Gt32_, G32_,
                   OpPrimalStep32B{xa_, dxp32_, qa_, aty32_, x, ix_, live_, ps_, dxsq_},
                   OpDualStep32B{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, iy_, live_, ds_, dysq_, dgdy_},
-                  dxp32_, dxm_, dy32_, dyl32_, dym_, aty32_, gx32_, gxl32_};
+                  dxp32_, dxm_, dy32_, dyl32_, dym_, aty32_, gx32_, gxl32_,
+                  Gt_, G_, x, xl, xm, y, yl, ym, xa_, ya_, qa_, ra_, c_s, h_s};
       tail_attempts_kernel<TailFP32><<<grid, kThreads, 0, s_>>>(T, pk);
     } else {
       TailFP64 pk{Gt_, G_, OpPrimalStepB{xl, aty, c_s, x, ix_, live_, ps_, dxsq_},

@@ -6,7 +6,8 @@
 // variables).  There the iteration graph's six kernels per attempt are almost
 // pure launch and dependency latency.  tail_attempts_kernel gives every
 // iterating instance one CTA that runs its attempts in a loop until the
-// instance halts (or the round's attempt budget ends): the same phases in the
+// instance halts (or the round's attempt budget ends; FP32 deltas move to new
+// FP64 anchors every kTailAnchor attempts, as between rounds of graphs): the same phases in the
 // same order as the graph -- G' y_lag over the instance's x rows, the primal
 // update + projection, G over its y rows, the dual update + projection, the
 // per-instance sums and the shared control_step, the reflection -- with
@@ -80,6 +81,51 @@ struct TailFP32 {
   __device__ void spmv_g(const RunTable& ry, int64_t k) const {
     tail_rows<float, kPair>(G, ry, k, &dxp->x, nullptr, gx, gxl);
   }
+  // re-anchoring (materialize_kernel then anchor_kernel and the anchor products of
+  // Solver::anchor, for this instance): FP64 iterates from the deltas, the anchors moved
+  // there, qa = G' ya - c, ra = G xa - h in FP64
+  CsrDev Gt64, G64;
+  double *x, *xl, *xm, *y, *yl, *ym, *xa, *ya, *qa, *ra;
+  const double *c, *h;
+  static constexpr bool kAnchored = true;
+  __device__ void reanchor(const RunTable& rx, const RunTable& ry, int64_t k) const {
+    for (int q = 0; q < kMaxRuns; ++q) {
+      const int64_t a = rx.start[k * kMaxRuns + q], L = rx.len[k * kMaxRuns + q];
+      for (int64_t j = a + threadIdx.x; j < a + L; j += kThreads) {
+        const double an = xa[j];
+        const float2 p = dxp[j];
+        const double v = an + (double)p.x, vl = an + (double)p.y, vm = an + dxm[j];
+        x[j] = v;
+        xl[j] = vl;
+        xm[j] = vm;
+        xa[j] = v;
+        dxp[j] = make_float2(0.0f, (float)(vl - v));
+        dxm[j] = vm - v;
+      }
+      const int64_t b = ry.start[k * kMaxRuns + q], M = ry.len[k * kMaxRuns + q];
+      for (int64_t i = b + threadIdx.x; i < b + M; i += kThreads) {
+        const double an = ya[i];
+        const double v = an + (double)dy[i], vl = an + (double)dyl[i], vm = an + dym[i];
+        y[i] = v;
+        yl[i] = vl;
+        ym[i] = vm;
+        ya[i] = v;
+        dy[i] = 0.0f;
+        dyl[i] = (float)(vl - v);
+        dym[i] = vm - v;
+      }
+    }
+    __syncthreads();
+    tail_rows<double, 1>(Gt64, rx, k, ya, nullptr, qa, nullptr);
+    tail_rows<double, 1>(G64, ry, k, xa, nullptr, ra, nullptr);
+    for (int q = 0; q < kMaxRuns; ++q) {
+      const int64_t a = rx.start[k * kMaxRuns + q], L = rx.len[k * kMaxRuns + q];
+      for (int64_t j = a + threadIdx.x; j < a + L; j += kThreads) qa[j] = qa[j] - c[j];
+      const int64_t b = ry.start[k * kMaxRuns + q], M = ry.len[k * kMaxRuns + q];
+      for (int64_t i = b + threadIdx.x; i < b + M; i += kThreads) ra[i] = ra[i] - h[i];
+    }
+    __syncthreads();
+  }
   __device__ void reflect(const PdhgState& s, const RunTable& rx, const RunTable& ry, int64_t k) const {
     for (int q = 0; q < kMaxRuns; ++q) {
       const int64_t a = rx.start[k * kMaxRuns + q], L = rx.len[k * kMaxRuns + q];
@@ -96,6 +142,8 @@ struct TailFP64 {
   OpPrimalStepB p;
   OpDualStepB d;
   double *x, *xl, *xm, *y, *yl, *ym, *aty, *gx, *gxl;
+  static constexpr bool kAnchored = false;
+  __device__ void reanchor(const RunTable&, const RunTable&, int64_t) const {}
   __device__ void spmv_t(const RunTable& rx, int64_t k) const { tail_rows<double, 1>(Gt, rx, k, yl, nullptr, aty, nullptr); }
   __device__ void spmv_g(const RunTable& ry, int64_t k) const { tail_rows<double, 2>(G, ry, k, x, xl, gx, gxl); }
   __device__ void reflect(const PdhgState& s, const RunTable& rx, const RunTable& ry, int64_t k) const {
@@ -115,6 +163,10 @@ struct TailFP64 {
     }
   }
 };
+
+// FP32 deltas are re-anchored every kTailAnchor attempts of a CTA's loop, the
+// iteration graph's cadence (a round of graphs, then the host re-anchors)
+constexpr int kTailAnchor = 128;
 
 struct TailArgs {
   const int32_t* list;    // iterating instances, a CTA each
@@ -139,6 +191,7 @@ __global__ void __launch_bounds__(kThreads) tail_attempts_kernel(TailArgs A, P p
   double unused[3];
   for (int att = 0; att < A.max_attempts; ++att) {
     if (!ss.active) break;  // CTA-uniform (read after a barrier)
+    if (P::kAnchored && att > 0 && att % kTailAnchor == 0) pk.reanchor(c.rx, c.ry, k);
     pk.spmv_t(c.rx, k);
     bs_project(pk.p, A.X, c.rx, 0, 1, cx, k, unused);
     pk.spmv_g(c.ry, k);
