@@ -118,8 +118,9 @@ def _problem_struct(hold: _Holder, *, n, m, nb, c, G, h, mGzero, mGnonnegative, 
     """Validate like the reference (rpdhg_alg_gpu_gen.jl:1331-1375, :84, :94) and fill a PdcsProblem."""
     on_device = _is_torch_cuda(c)
     if not on_device:
-        G = sp.csr_matrix(G)
-        G.sort_indices()
+        if not (sp.issparse(G) and G.format == "csr"):
+            G = sp.csr_matrix(G)
+        G.sort_indices()  # scipy remembers the answer on the matrix, so repeated solves skip the scan
         if G.shape[0] != m:
             raise ValueError("m does not match the size of G")
         if G.shape[1] != n:
