@@ -164,7 +164,7 @@ typedef struct {
   int64_t service_rounds;   /* batched checkpoint operations (exit checks, restart probes, copies) */
   int64_t single_fallbacks; /* instances re-solved alone for the resolving fallback */
   int32_t spmv_tiled;       /* 1: the iteration graph ran the instance-tiled SpMV, 0: the binned one */
-  int32_t reserved;
+  int32_t tail_rounds;      /* iteration rounds run by the tail kernel (a CTA per remaining instance) */
 } pdcs_batch_info;
 
 /* Solve `count` independent conic programs together.  No counterpart in the

@@ -89,7 +89,7 @@ class PdcsBatchInfo(C.Structure):
     _fields_ = [("setup_time", C.c_double), ("solve_time", C.c_double), ("time_iterations", C.c_double),
                 ("kernel_launches", C.c_int64), ("graph_launches", C.c_int64),
                 ("service_rounds", C.c_int64), ("single_fallbacks", C.c_int64),
-                ("spmv_tiled", C.c_int32), ("reserved", C.c_int32)]
+                ("spmv_tiled", C.c_int32), ("tail_rounds", C.c_int32)]
 
 
 class PdcsGradOptions(C.Structure):

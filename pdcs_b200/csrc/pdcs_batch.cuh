@@ -381,6 +381,7 @@ class BatchSolver : public Solver {
   size_t pin_cap_ = 0, pin_off_ = 0;
   std::vector<Inst> inst_;
   int64_t rounds_ = 0;
+  int64_t tail_rounds_ = 0;  // iteration rounds run by tail_attempts_kernel
   // host wall time per service request type (verbose report)
   double svc_s_[16] = {};
   int64_t svc_groups_[16] = {}, svc_insts_[16] = {};
@@ -1466,6 +1467,7 @@ void BatchSolver::exec_iterate(std::vector<Inst*>& its) {
     }
     PDCS_CUDA(cudaGetLastError());
     kernels_++;
+    tail_rounds_++;
   } else {
     for (int64_t gi = 0; gi < graphs; ++gi) {
       PDCS_CUDA(cudaGraphLaunch(bgraph_exec_[tail], s_));
@@ -2060,7 +2062,7 @@ void BatchSolver::reset_state() {
     I.ginf = c.ginf;
     I.omega0 = c.omega0;
   }
-  kernels_ = graphs_ = probes_ = rounds_ = 0;
+  kernels_ = graphs_ = probes_ = rounds_ = tail_rounds_ = 0;
   t_iter_ = 0.0;
   iter_s_ = 0.0;
   dev_ms_ = 0.0;
@@ -2189,6 +2191,7 @@ int BatchSolver::solve(pdcs_result* res, pdcs_batch_info* info, int64_t attempt_
     info->single_fallbacks = fallbacks;
     info->time_iterations = t_iter_;
     info->spmv_tiled = tiled_ ? 1 : 0;
+    info->tail_rounds = (int32_t)tail_rounds_;
   }
   return PDCS_OK;
 }

@@ -285,6 +285,7 @@ class BatchInfo:
     service_rounds: int
     single_fallbacks: int
     spmv_tiled: bool = False
+    tail_rounds: int = 0
 
 
 class BatchHandle:
@@ -414,7 +415,7 @@ def _batch_info(B) -> "BatchInfo":
     return BatchInfo(setup_time=B.setup_time, solve_time=B.solve_time, time_iterations=B.time_iterations,
                      kernel_launches=B.kernel_launches, graph_launches=B.graph_launches,
                      service_rounds=B.service_rounds, single_fallbacks=B.single_fallbacks,
-                     spmv_tiled=bool(B.spmv_tiled))
+                     spmv_tiled=bool(B.spmv_tiled), tail_rounds=B.tail_rounds)
 
 
 def rpdhg_gpu_solve_batch(problems, **options):

@@ -144,3 +144,19 @@ def test_batch_tiled_spmv_matches_binned(cuda, precision):
     for p, g, h in zip(batch, a, b):
         assert g.info.exit_status == h.info.exit_status == "optimal", p.name
         assert abs(g.info.pObj - h.info.pObj) <= 1e-4 * (1.0 + abs(h.info.pObj)), p.name
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_tail_kernel_solutions(cuda, precision):
+    """Uneven batch whose last instances run in the tail kernel (a CTA per
+    instance looping over its attempts): every instance reaches the criteria
+    under the oracle's evaluator and matches its single-instance solve."""
+    batch = problems.batch_socp_c3(count=48, seed=7, nmin=40, nmax=600)
+    sols, info = solver.rpdhg_gpu_solve_batch(batch, precision=precision, time_limit=300)
+    assert info.tail_rounds > 0, info
+    for p, g in zip(batch, sols):
+        assert g.info.exit_status == "optimal", (p.name, g)
+        e = B.evaluate(p, g.primal, g.dual)
+        assert max(e["primal_res_gpu_form"], e["dual_res"], e["rel_gap"]) < 1.05e-6, (p.name, e)
+        s = solver.solve_problem(p)
+        assert abs(g.info.pObj - s.info.pObj) <= 2e-6 * (1.0 + abs(s.info.pObj)), (p.name, g.info.pObj, s.info.pObj)
