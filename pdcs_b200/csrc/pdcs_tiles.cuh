@@ -19,7 +19,7 @@
 namespace pdcs {
 
 constexpr int64_t kTileMaxCols = 65535;  // 16-bit local column indices
-constexpr int kTileLN = 8;               // nonzeros a lane loads at once
+constexpr int kTileLN = 16;              // nonzeros a lane loads at once
 constexpr int kTileThreads = 512;        // a tile's CTA: 16 warps share one staged column segment
 constexpr int kTileWarps = kTileThreads / 32;
 
