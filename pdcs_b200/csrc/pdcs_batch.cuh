@@ -395,8 +395,10 @@ class BatchSolver : public Solver {
     int2* chunk = nullptr;
     int64_t* meta = nullptr;
     int64_t* sched = nullptr;
+    int4* desc = nullptr;  // the scheduled cones' records (ConeTable::act_desc)
     int32_t* exp = nullptr;
   } act_[2];
+  std::vector<int4> cone_desc_[2];  // per warp cone: {start, length | RSOC << 30, cone, instance}
   int4* rchunk_ = nullptr;
   int64_t* n_rchunk_ = nullptr;
   int32_t* act_inst_ = nullptr;
@@ -967,8 +969,29 @@ void BatchSolver::setup_act_lists() {
     act_[w].chunk = A.alloc<int2>(std::max<int64_t>(nc, 1));
     act_[w].meta = A.alloc<int64_t>(2 * kCls + 4);
     act_[w].sched = A.alloc<int64_t>(std::max<int64_t>(T[w]->nwc, 1));
+    act_[w].desc = A.alloc<int4>(std::max<int64_t>(T[w]->nwc, 1));
+    {  // cone records in cone order (SOC list, then RSOC list, as the cone tables)
+      const std::vector<int64_t>& soc = w ? h_socG_ : h_socx_;
+      const std::vector<int64_t>& rsoc = w ? h_rsocG_ : h_rsocx_;
+      std::vector<int4>& cd = cone_desc_[w];
+      cd.assign(T[w]->nwc, make_int4(0, 0, 0, 0));
+      int64_t st = w ? (int64_t)(P.mGzero + P.mGnonnegative) : nb_;
+      int64_t i = 0;
+      for (const std::vector<int64_t>* L : {&soc, &rsoc})
+        for (int64_t d : *L) {
+          cd[i] = make_int4((int32_t)st, (int32_t)(d | (L == &rsoc ? (1 << 30) : 0)), (int32_t)i, 0);
+          st += d;
+          ++i;
+        }
+      for (int64_t k = 0; k < K_; ++k) {
+        const std::array<int64_t, 8>& c = cones_[w][k];
+        for (int64_t q = c[0]; q < c[1]; ++q) cd[q].w = (int32_t)k;
+        for (int64_t q = c[2]; q < c[3]; ++q) cd[q].w = (int32_t)k;
+      }
+    }
     act_[w].exp = A.alloc<int32_t>(std::max<int64_t>(ne, 1));
-    bytes += nc * sizeof(int2) + (2 * kCls + 4) * sizeof(int64_t) + T[w]->nwc * sizeof(int64_t) + ne * sizeof(int32_t);
+    bytes += nc * sizeof(int2) + (2 * kCls + 4) * sizeof(int64_t) + T[w]->nwc * (sizeof(int64_t) + sizeof(int4)) +
+             ne * sizeof(int32_t) + 256;
   }
   rchunk_ = A.alloc<int4>(std::max<int64_t>(nr, 1));
   n_rchunk_ = A.alloc<int64_t>(1);
@@ -989,11 +1012,13 @@ void BatchSolver::setup_act_lists() {
   XIg_.act_meta = act_[0].meta;
   XIg_.act_sched = act_[0].sched;
   XIg_.act_exp = act_[0].exp;
+  XIg_.act_desc = act_[0].desc;
   YIg_ = YI;
   YIg_.act_chunk = act_[1].chunk;
   YIg_.act_meta = act_[1].meta;
   YIg_.act_sched = act_[1].sched;
   YIg_.act_exp = act_[1].exp;
+  YIg_.act_desc = act_[1].desc;
 }
 
 // Lists of the work of the iterating instances: elementwise chunks, warp cones
@@ -1029,10 +1054,12 @@ void BatchSolver::build_act_lists(const std::vector<Inst*>& its) {
     size_t total = 0;
     for (int c = 0; c < kCls; ++c) total += bycls[c].size();
     int64_t* sched = stage<int64_t>(std::max<size_t>(total, 1));
+    int4* desc = stage<int4>(std::max<size_t>(total, 1));
     for (int c = 0; c < kCls; ++c) {
       meta[1 + c] = task;
       meta[kCls + 2 + c] = off;
       std::memcpy(sched + off, bycls[c].data(), bycls[c].size() * sizeof(int64_t));
+      for (size_t q = 0; q < bycls[c].size(); ++q) desc[off + q] = cone_desc_[w][bycls[c][q]];
       const int64_t per = (c < kCls - 1) ? 32 / (2 << c) : 1;
       task += ((int64_t)bycls[c].size() + per - 1) / per;
       off += (int64_t)bycls[c].size();
@@ -1041,8 +1068,10 @@ void BatchSolver::build_act_lists(const std::vector<Inst*>& its) {
     meta[2 * kCls + 2] = off;
     meta[2 * kCls + 3] = (int64_t)ex.size();
     PDCS_CUDA(cudaMemcpyAsync(act_[w].meta, meta, sizeof(int64_t) * (2 * kCls + 4), cudaMemcpyHostToDevice, s_));
-    if (total)
+    if (total) {
       PDCS_CUDA(cudaMemcpyAsync(act_[w].sched, sched, sizeof(int64_t) * total, cudaMemcpyHostToDevice, s_));
+      PDCS_CUDA(cudaMemcpyAsync(act_[w].desc, desc, sizeof(int4) * total, cudaMemcpyHostToDevice, s_));
+    }
     if (!ch.empty()) {
       int2* hc = stage<int2>(ch.size());
       std::memcpy(hc, ch.data(), ch.size() * sizeof(int2));

@@ -307,6 +307,8 @@ struct ConeTable {
   const int64_t* act_meta;
   const int64_t* act_sched;   // warp-cone indices, class by class
   const int32_t* act_exp;     // exp / dual-exp cone ordinals (0 .. exp_count + dexp_count)
+  const int4* act_desc;       // with act_sched: per scheduled cone {start, length | RSOC << 30, cone,
+                              // instance}, so a lane group reads one record (NULL: the wc_* tables)
   int64_t elem_total;        // sum of seg_len
   int32_t ctaA, ctaB, ctaC;  // CTAs for elementwise / warp cones / exp cones
 };
@@ -502,13 +504,27 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
         const int gl = lane & (g - 1);
         const int64_t idx = cls_off[c] + (task - task0[c]) * (32 / g) + lane / g;
         bool have = idx < cls_off[c + 1];
-        const int64_t k = have ? sched[idx] : 0;
-        const int64_t st = have ? T.wc_start[k] : 0;
-        if constexpr (MaskedOp<Op>) {
-          if (have && !op.live(st)) have = false;  // group-uniform: a block belongs to one instance
+        int64_t k = 0, st = 0;
+        int d = 0;
+        bool rsoc = false;
+        if (have && T.act_desc) {
+          const int4 de = T.act_desc[idx];
+          k = de.z;
+          st = de.x;
+          if constexpr (MaskedOp<Op>) {
+            if (!op.mask[de.w]) have = false;  // group-uniform: a block belongs to one instance
+          }
+          d = have ? (de.y & 0x3fffffff) : 0;
+          rsoc = have && (de.y >> 30) != 0;
+        } else if (have) {
+          k = sched[idx];
+          st = T.wc_start[k];
+          if constexpr (MaskedOp<Op>) {
+            if (!op.live(st)) have = false;  // group-uniform: a block belongs to one instance
+          }
+          d = have ? T.wc_len[k] : 0;
+          rsoc = have && T.wc_kind[k] == PK_RSOC;
         }
-        const int d = have ? T.wc_len[k] : 0;
-        const bool rsoc = have && T.wc_kind[k] == PK_RSOC;
         const double* S = (T.S && have) ? T.S + st : nullptr;
         const double z = (gl < d) ? op.z(st + gl) : 0.0;
         double v = z;
@@ -532,13 +548,27 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
         if (gl < d) op.fin(st + gl, z, v, acc);
       } else {
         // blocks of more than 32 elements: a warp each, values staged in op.out
-        const int64_t k = sched[cls_off[c] + (task - task0[c])];
-        const int64_t st = T.wc_start[k];
-        if constexpr (MaskedOp<Op>) {
-          if (!op.live(st)) continue;  // warp-uniform
+        int64_t k, st;
+        int32_t d;
+        bool rsoc;
+        if (T.act_desc) {
+          const int4 de = T.act_desc[cls_off[c] + (task - task0[c])];
+          if constexpr (MaskedOp<Op>) {
+            if (!op.mask[de.w]) continue;  // warp-uniform
+          }
+          k = de.z;
+          st = de.x;
+          d = de.y & 0x3fffffff;
+          rsoc = (de.y >> 30) != 0;
+        } else {
+          k = sched[cls_off[c] + (task - task0[c])];
+          st = T.wc_start[k];
+          if constexpr (MaskedOp<Op>) {
+            if (!op.live(st)) continue;  // warp-uniform
+          }
+          d = T.wc_len[k];
+          rsoc = T.wc_kind[k] == PK_RSOC;
         }
-        const int32_t d = T.wc_len[k];
-        const bool rsoc = T.wc_kind[k] == PK_RSOC;
         const double* S = T.S ? T.S + st : nullptr;
         double* p = op.out + st;
         for (int64_t i = lane; i < d; i += 32) p[i] = op.z(st + i);
