@@ -906,10 +906,11 @@ void BatchSolver::setup_tiles() {
       const int64_t big = O.spmv_tiles > 0 ? (int64_t)O.spmv_tiles : kTileNnz;
       const int64_t cap = std::min(big, std::max(kTileSmallNnz, 16 * ncols));
       int64_t o = 0, ob = 0, acc = 0;
+      const int64_t ln = fp32_ ? kTileLN<float> : kTileLN<double>;
       auto cut = [&](int64_t end) {
         const int64_t rows = end - ob;
         int g = 1;
-        while (g < 32 && kTileLN * g * rows < acc) g *= 2;  // about kTileLN nonzeros per lane
+        while (g < 32 && ln * g * rows < acc) g *= 2;  // about ln nonzeros per lane
         tiles.push_back(make_int4((int32_t)k, (int32_t)ob, (int32_t)end, g));
         t.nnz.push_back(acc);
         ob = end;

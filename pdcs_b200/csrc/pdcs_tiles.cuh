@@ -19,7 +19,10 @@
 namespace pdcs {
 
 constexpr int64_t kTileMaxCols = 65535;  // 16-bit local column indices
-constexpr int kTileLN = 16;              // nonzeros a lane loads at once
+// nonzeros a lane loads at once: 16 FP32 values (more bytes in flight per warp),
+// 8 FP64 ones (16 doubles per lane spill registers)
+template <class T>
+constexpr int kTileLN = sizeof(T) == 4 ? 16 : 8;
 constexpr int kTileThreads = 512;        // a tile's CTA: 16 warps share one staged column segment
 constexpr int kTileWarps = kTileThreads / 32;
 
@@ -118,18 +121,18 @@ __global__ void __launch_bounds__(kTileThreads) spmv_tile_kernel(TileCsr A, cons
       // a lane's partial sums in T (FP32 rows sum in FP32, as the binned kernel's
       // short rows do), widened to FP64 for the lane group's butterfly
       T p0 = T(0), p1 = T(0);
-      for (int32_t e0 = kb + gl; e0 < ke; e0 += kTileLN * g) {
-        T v[kTileLN];
-        uint16_t c[kTileLN];
+      for (int32_t e0 = kb + gl; e0 < ke; e0 += kTileLN<T> * g) {
+        T v[kTileLN<T>];
+        uint16_t c[kTileLN<T>];
 #pragma unroll
-        for (int u = 0; u < kTileLN; ++u) {  // every load of the chunk in flight together
+        for (int u = 0; u < kTileLN<T>; ++u) {  // every load of the chunk in flight together
           const int32_t e = e0 + u * g;
           const bool ok = e < ke;
           v[u] = ok ? vals[e] : T(0);
           c[u] = ok ? A.cl[e] : (uint16_t)0;
         }
 #pragma unroll
-        for (int u = 0; u < kTileLN; ++u) {
+        for (int u = 0; u < kTileLN<T>; ++u) {
           if (e0 + u * g < ke) {
             const V xv = sx[c[u]];
             if constexpr (NV == 1) {
