@@ -176,15 +176,19 @@ __device__ __forceinline__ int32_t inst_of_z(int64_t i, int64_t n, const int32_t
 }
 
 // out[k * ld + p] = <V_p, w> over instance k's elements, p = p0 .. p0 + np - 1 (np <= 8);
-// a CTA per instance, fixed-order block reduction
-__global__ void __launch_bounds__(kThreads) adj_dots_kernel(int64_t K, const uint8_t* __restrict__ mask, RunTable rx,
-                                                           RunTable ry, int64_t n, const double* __restrict__ V,
-                                                           int64_t ldV, int p0, int np,
-                                                           const double* __restrict__ w, double* __restrict__ out,
-                                                           int ld) {
+// Per-instance dot products <V_{p0+p}, w> (p < np <= 8), split over S CTAs per
+// instance: CTA (k, s) sums the instance's elements s, s + S, ... (in blocks of
+// kThreads) into part[(k * S + s) * 8 + p]; adj_dots_reduce_kernel adds the S
+// partials in order, so the result does not depend on scheduling.
+__global__ void __launch_bounds__(kThreads) adj_dots_kernel(int64_t K, int S, const uint8_t* __restrict__ mask,
+                                                           RunTable rx, RunTable ry, int64_t n,
+                                                           const double* __restrict__ V, int64_t ldV, int p0, int np,
+                                                           const double* __restrict__ w, double* __restrict__ part) {
   __shared__ double sh[8][kWarps];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int64_t k = blockIdx.x; k < K; k += gridDim.x) {
+  for (int64_t ks = blockIdx.x; ks < K * S; ks += gridDim.x) {
+    const int64_t k = ks / S;
+    const int s = (int)(ks % S);
     if (mask && !mask[k]) continue;  // CTA-uniform
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int side = 0; side < 2; ++side) {
@@ -192,7 +196,7 @@ __global__ void __launch_bounds__(kThreads) adj_dots_kernel(int64_t K, const uin
       const int64_t off = side ? n : 0;
       for (int q = 0; q < kMaxRuns; ++q) {
         const int64_t s0 = off + rt.start[k * kMaxRuns + q], L = rt.len[k * kMaxRuns + q];
-        for (int64_t i = s0 + threadIdx.x; i < s0 + L; i += kThreads) {
+        for (int64_t i = s0 + (int64_t)s * kThreads + threadIdx.x; i < s0 + L; i += (int64_t)S * kThreads) {
           const double wi = w[i];
 #pragma unroll
           for (int p = 0; p < 8; ++p)
@@ -210,9 +214,22 @@ __global__ void __launch_bounds__(kThreads) adj_dots_kernel(int64_t K, const uin
     if (threadIdx.x < np) {
       double v = 0.0;
       for (int q = 0; q < kWarps; ++q) v += sh[threadIdx.x][q];
-      out[k * ld + p0 + threadIdx.x] = v;
+      part[ks * 8 + threadIdx.x] = v;
     }
     __syncthreads();
+  }
+}
+
+__global__ void adj_dots_reduce_kernel(int64_t K, int S, const uint8_t* __restrict__ mask, int p0, int np,
+                                       const double* __restrict__ part, double* __restrict__ out, int ld) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < K * np; t += stride) {
+    const int64_t k = t / np;
+    const int p = (int)(t % np);
+    if (mask && !mask[k]) continue;
+    double v = 0.0;
+    for (int s = 0; s < S; ++s) v += part[(k * S + s) * 8 + p];
+    out[k * ld + p0 + p] = v;
   }
 }
 

@@ -298,8 +298,10 @@ class BatchSolver : public Solver {
     double *a = nullptr, *b = nullptr, *xp = nullptr, *tw = nullptr, *tsw = nullptr, *tt = nullptr, *tq = nullptr,
            *tr = nullptr, *ttr = nullptr, *ts = nullptr, *dG = nullptr, *Tx = nullptr, *Sy = nullptr;
     double *dots1 = nullptr, *dots2 = nullptr, *dotsn = nullptr;
+    double* dpart = nullptr;  // partial dot products: K x kAdjSplit x 8
     uint8_t* mask = nullptr;
   } adj_;
+  static constexpr int kAdjSplit = 16;  // at most this many CTAs per instance in the adjoint's dot products
   void setup_adjoint(int mr);
   void apply_AT(const double* u, double* out, const uint8_t* mask);
   void scatter_x(const double* merged, double* const* out) const;
@@ -2277,6 +2279,7 @@ void BatchSolver::setup_adjoint(int mr) {
     adj_.mask = A.alloc<uint8_t>(K_);
   }
   for (double** v : {&adj_.coef, &adj_.dots1, &adj_.dots2, &adj_.dotsn}) *v = A.alloc<double>((size_t)K_ * (mr + 1));
+  if (!adj_.dpart) adj_.dpart = A.alloc<double>((size_t)K_ * kAdjSplit * 8);
 }
 
 // out = (I - M') u on the masked instances
@@ -2339,12 +2342,17 @@ int BatchSolver::grad(const double* const* dldx, const double* const* dldy, doub
     PDCS_CUDA(cudaMemsetAsync(adj_.u, 0, sizeof(double) * N, s_));
     PDCS_CUDA(cudaStreamSynchronize(s_));
   }
-  const int dgrid = (int)std::max<int64_t>(1, std::min<int64_t>(K, 148 * 8));  // a CTA per instance
+  // CTAs per instance in the dot products: enough CTAs to fill the GPU (a CTA per instance
+  // when the batch is large), capped at kAdjSplit
+  const int split = (int)std::max<int64_t>(1, std::min<int64_t>(kAdjSplit, (148 * 8 + K - 1) / K));
+  const int dgrid = (int)std::max<int64_t>(1, std::min<int64_t>(K * split, 148 * 8));
   // per-instance dot products <V_p, w>, p < np, into out (device; no synchronisation)
   auto dots = [&](const uint8_t* mask, const double* V, int np, const double* w, double* out) {
     for (int q = 0; q < np; q += 8) {
-      adj_dots_kernel<<<dgrid, kThreads, 0, s_>>>(K, mask, rx_, ry_, n_, V, N, q, std::min(8, np - q), w, out, ld);
-      kernels_++;
+      const int c = std::min(8, np - q);
+      adj_dots_kernel<<<dgrid, kThreads, 0, s_>>>(K, split, mask, rx_, ry_, n_, V, N, q, c, w, adj_.dpart);
+      adj_dots_reduce_kernel<<<grid_for(K * c), kThreads, 0, s_>>>(K, split, mask, q, c, adj_.dpart, out, ld);
+      kernels_ += 2;
     }
   };
   auto fetch = [&](const double* dev) {
