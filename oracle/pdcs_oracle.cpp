@@ -263,11 +263,13 @@ struct ExpRootCtx {
   double N2(double x) const { return ds * r - dr * s * x; }
   // f(x) e^{-|x|}: same sign as f, no overflow for any finite x
   // zero_mask bit 1: x is the root of N1, bit 2: root of N2 (use exact zeros)
-  double fs(double x, int zero_mask = 0) const {
+  double fs(double x, int zero_mask = 0, double* mag = nullptr) const {
     double ax = std::fabs(x);
     double n1 = (zero_mask & 1) ? 0.0 : N1(x);
     double n2 = (zero_mask & 2) ? 0.0 : N2(x);
-    return n1 * dt * std::exp(x - ax) - dr * ds * n2 * std::exp(-x - ax) / dt - t * Q(x) * std::exp(-ax);
+    double a = n1 * dt * std::exp(x - ax), b = dr * ds * n2 * std::exp(-x - ax) / dt, c = t * Q(x) * std::exp(-ax);
+    if (mag) *mag = std::fabs(a) + std::fabs(b) + std::fabs(c);
+    return a - b - c;
   }
   // d/dx [f(x) e^{-|x|}]
   double dfs(double x) const {
@@ -325,8 +327,17 @@ bool exp_root(const ExpRootCtx& C, double* rho_out) {
         ga = g(a);
       }
     } else {
+      // An endpoint at a root of N1 (sp = 0: v on the polar's boundary) or N2
+      // (lam = 0: v on the cone's boundary) where f vanishes to rounding is
+      // the root itself: v lies on a boundary within rounding of the
+      // membership tests above, and the sign of f there is noise.
+      double mag;
       a = lo;
-      ga = sg * C.fs(a, tlo & 3);
+      ga = sg * C.fs(a, tlo & 3, &mag);
+      if ((tlo & 3) && std::fabs(ga) <= 16.0 * std::numeric_limits<double>::epsilon() * mag) {
+        *rho_out = a;
+        return true;
+      }
     }
     if (std::isinf(hi)) {  // g -> +inf as x -> +inf
       double base = std::max(p, a);
@@ -339,8 +350,13 @@ bool exp_root(const ExpRootCtx& C, double* rho_out) {
         gb = g(bb);
       }
     } else {
+      double mag;
       bb = hi;
-      gb = sg * C.fs(bb, thi & 3);
+      gb = sg * C.fs(bb, thi & 3, &mag);
+      if ((thi & 3) && std::fabs(gb) <= 16.0 * std::numeric_limits<double>::epsilon() * mag) {
+        *rho_out = bb;
+        return true;
+      }
     }
     if (!(std::isfinite(ga) && std::isfinite(gb))) continue;
     if (!((ga <= 0.0 && gb >= 0.0) || (ga >= 0.0 && gb <= 0.0))) continue;

@@ -115,3 +115,69 @@ def soc_project_reference(v, Dw=None):
     y = x / (1 + mu * D * D)
     s = np.linalg.norm(D * y)
     return np.concatenate([[s], y])
+
+
+# ---------------------------------------------------------------------------
+# KKT residual of a candidate projection p of v onto a scaled cone C = S o K
+# (the sets the solver's block projections use: p / S in K).  p is the
+# projection iff p in C, q = p - v in the dual cone C* = (1/S) o K*, and
+# <p, q> = 0.  kkt_residual returns the largest of the three violations,
+# relative to max(1, ||v||) (squared for the products), so two differing
+# candidates can be ranked: the exact projection has a residual at the
+# rounding level, an approximate one (a root search stopped at a tolerance, a
+# wrong branch) a larger one.
+# ---------------------------------------------------------------------------
+
+def _soc_in(u, D):     # {t >= ||D x||}
+    return max(0.0, float(np.linalg.norm(D * u[1:])) - u[0])
+
+
+def _rsoc_in(u, D):    # {2 x y >= ||D z||^2, x, y >= 0}, as a length
+    quad = float(np.sum((D * u[2:]) ** 2)) - 2.0 * u[0] * u[1]
+    return max(0.0, -u[0], -u[1], quad / max(1e-300, abs(u[0]) + abs(u[1]) + float(np.linalg.norm(D * u[2:]))))
+
+
+def _kexp_in(u):       # K_exp = cl{s > 0, s e^{r/s} <= t}
+    r, s_, t = (float(x) for x in u)
+    if s_ > 0.0:
+        with np.errstate(over="ignore"):
+            return max(0.0, s_ * math.exp(min(r / s_, 700.0)) - t)
+    return max(0.0, r, -t, -s_)
+
+
+def _kexp_dual_in(u):  # K_exp^* = cl{a < 0, -a e^{b/a} <= e c}
+    a, b, c = (float(x) for x in u)
+    if a < 0.0:
+        return max(0.0, -a * math.exp(min(b / a, 700.0)) - math.e * c)
+    return max(0.0, a, -b, -c)
+
+
+def kkt_residual(kind, v, p, S=None):
+    v = np.asarray(v, float)
+    p = np.asarray(p, float)
+    if not np.all(np.isfinite(p)):
+        return math.inf
+    d = v.size
+    S = np.ones(d) if S is None else np.asarray(S, float)
+    q = p - v
+    sc = max(1.0, float(np.linalg.norm(v)))
+    if kind == "soc":
+        D = S[0] / S[1:]
+        prim, dual = _soc_in(p, D), _soc_in(q, 1.0 / D)
+    elif kind == "rsoc":
+        D = math.sqrt(S[0] * S[1]) / S[2:]
+        prim, dual = _rsoc_in(p, D), _rsoc_in(q, 1.0 / D)
+    elif kind == "exp":
+        prim, dual = _kexp_in(p / S), _kexp_dual_in(q * S)
+    elif kind == "dexp":  # C = S o K*, C* = (1/S) o K
+        prim, dual = _kexp_dual_in(p / S), _kexp_in(q * S)
+    else:
+        raise ValueError(kind)
+    return max(prim / sc, dual / sc, abs(float(p @ q)) / sc ** 2)
+
+
+def better_projection(kind, v, S, p_good, p_other, floor=1e-13):
+    """p_good is the valid projection where p_other differs: p_good's KKT
+    residual is at the rounding floor or no larger than p_other's."""
+    rg = kkt_residual(kind, v, p_good, S)
+    return rg <= floor or rg <= kkt_residual(kind, v, p_other, S)
