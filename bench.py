@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--count", type=int, default=4096, help="instances per batch")
     ap.add_argument("--plain-sample", type=int, default=24, help="instances timed with the plain FP64 solver")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the bounded CPU sample")
+    ap.add_argument("--cpu-sample", type=int, default=256, help="instances in the GPU arm's CPU-baseline sample")
+    ap.add_argument("--ref-per-step", type=int, default=96, help="instances per step of --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-single", action="store_true",
@@ -134,59 +135,144 @@ class Clocks:
 # CPU: the oracle (C++ restatement of the reference's algorithm), one instance
 # per worker process over all host cores (spawned: no GPU state is inherited)
 # ---------------------------------------------------------------------------
-def _oracle_solve_one(p):
+def _oracle_solve_one(item):
     from oracle import binding as B
+    i, p = item
     t = time.perf_counter()
     r = B.solve(p, threads=1)
-    return r["iter"], r["exit_code"], time.perf_counter() - t
+    return i, r["iter"], r["exit_code"], time.perf_counter() - t, r["primal_objective"]
 
 
-def cpu_batch_rate(batch, seconds, rng_seed=7):
-    """Instances/s of the oracle over all host cores on a seeded sample of the batch,
-    sized so the run takes about `seconds`."""
-    import multiprocessing as mp
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_sample(batch, size, seed=7):
+    """A fixed, seeded sample of `size` instances stratified by size: the batch
+    sorted by nonzeros is cut into `size` equal strata and one instance is
+    drawn from each, so the sample has the batch's size distribution; the
+    sample is returned in a seeded random order."""
     import numpy as np
-    cores = os.cpu_count() or 1
-    order = np.random.default_rng(rng_seed).permutation(len(batch))
-    ctx = mp.get_context("spawn")
-    done, iters, t0 = 0, 0, time.perf_counter()
-    with ctx.Pool(cores) as pool:
-        pos = 0
-        while time.perf_counter() - t0 < seconds and pos < len(order):
-            chunk = [batch[i] for i in order[pos:pos + cores]]
-            pos += len(chunk)
-            for it, code, _ in pool.map(_oracle_solve_one, chunk):
-                done += 1
-                iters += it
-    wall = time.perf_counter() - t0
-    return {"value": done / wall, "unit": "instances/s", "cores": cores, "kind": "port",
-            "iter_per_s": iters / wall,
-            "sample": f"{done} seeded instances of the same batch solved to 1e-6 by the oracle "
-                      f"(FP64, one instance per core) in {wall:.1f} s"}
+    rng = np.random.default_rng(seed)
+    order = np.argsort([p.nnz for p in batch], kind="stable")
+    edges = np.linspace(0, len(order), size + 1).astype(int)
+    pick = [int(order[rng.integers(edges[k], max(edges[k] + 1, edges[k + 1]))]) for k in range(size)]
+    return [pick[k] for k in rng.permutation(size)]  # shuffled: every slice of the sample is mixed in size
+
+
+class CpuPool:
+    """The oracle over all host cores: one instance per worker process
+    (spawned, so no GPU state is inherited), instances handed out largest
+    first through imap_unordered, so no core waits on another between
+    instances; a step ends when its last instance is solved."""
+
+    def __init__(self, cores=None):
+        import multiprocessing as mp
+        self.cores = cores or host_cores()
+        self.pool = mp.get_context("spawn").Pool(self.cores)
+
+    def run(self, items):
+        """items: (key, problem) pairs; returns wall, iterations, exit codes and {key: objective}."""
+        work = sorted(items, key=lambda kp: -kp[1].nnz)
+        t0 = time.perf_counter()
+        iters, codes, objs = 0, {}, {}
+        for key, it, code, _, pobj in self.pool.imap_unordered(_oracle_solve_one, work):
+            iters += it
+            codes[code] = codes.get(code, 0) + 1
+            objs[key] = pobj
+        return time.perf_counter() - t0, iters, codes, objs
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_batch_rate(batch, size=256, gpu_sols=None):
+    """Instances/s of the oracle over all host cores on a fixed stratified
+    sample of the batch (one timed pass over the sample).  With the GPU
+    batch's solutions, also their error against the FP64 oracle on the same
+    instances: objective error relative to 1 + |oracle objective| and the
+    three criteria of the GPU solutions under the oracle's evaluator."""
+    import numpy as np
+    idx = cpu_sample(batch, size)
+    pool = CpuPool()
+    try:
+        pool.run([(None, batch[idx[0]])] * pool.cores)  # start the workers
+        wall, iters, codes, objs = pool.run([(i, batch[i]) for i in idx])
+    finally:
+        pool.close()
+    err = None
+    if gpu_sols is not None:
+        from oracle import binding as B
+        oe, crit = [], []
+        for i in idx:
+            oe.append(abs(gpu_sols[i].info.pObj - objs[i]) / (1.0 + abs(objs[i])))
+            e = B.evaluate(batch[i], gpu_sols[i].primal, gpu_sols[i].dual)
+            crit.append((e["primal_res_gpu_form"], e["primal_res"], e["dual_res"], e["rel_gap"]))
+        crit = np.array(crit)
+        err = {"instances": len(idx), "objective_rel_err_max": float(max(oe)),
+               "objective_rel_err_median": float(np.median(oe)),
+               "primal_res_max": float(crit[:, 0].max()), "primal_res_readme_form_max": float(crit[:, 1].max()),
+               "dual_res_max": float(crit[:, 2].max()), "rel_gap_max": float(crit[:, 3].max()),
+               "what": "FP32-bulk batch solutions vs the FP64 oracle's solve of the same instances "
+                       "(|pObj - pObj_oracle| / (1 + |pObj_oracle|)) and their criteria under the oracle's "
+                       "FP64 evaluator"}
+    return {"value": len(idx) / wall, "unit": "instances/s", "cores": pool.cores, "kind": "port",
+            "iter_per_s": iters / wall, "optimal": codes.get(0, 0), "error_vs_fp64_oracle": err,
+            "sample": f"{len(idx)} instances of the same batch (a fixed seeded sample stratified by size) "
+                      f"solved to 1e-6 by the oracle (FP64, one instance per core, largest first) in {wall:.1f} s"}
 
 
 def run_reference(args):
+    """The reference's algorithm on the host cores (its C++ restatement: the
+    reference itself is Julia + CUDA.jl and cannot run here).  A fixed seeded
+    sample of the batch, stratified by size, is cut into slices; every step
+    solves one slice over all cores, warm-up steps included, and the step's
+    wall time is its ms_per_step."""
     from pdcs_b200 import replicas
     rank, world, _ = replicas.env()
     if rank != 0:
         return 0
     batch, cfg, _ = workload(args)
-    for _ in range(min(args.warmup, 1)):
-        _oracle_solve_one(batch[0])
-    vals, its, secs = [], 0.0, 0.0
-    for _ in range(args.steps):
-        r = cpu_batch_rate(batch, args.cpu_seconds / max(1, args.steps) * 2)
-        vals.append(r["value"])
-        its += r["iter_per_s"]
-        secs += 1.0 / r["value"]
-    v = statistics.mean(vals)
+    cfg = {**cfg, "parallelism": f"{args.gpus} GPUs, one batch each" if args.gpus > 1 else "single GPU"}
+    per_step = args.ref_per_step
+    idx = cpu_sample(batch, max(per_step * 8, 1024))
+    pool = CpuPool()
+    try:
+        pos = 0
+
+        def step():
+            nonlocal pos
+            sl = [(k, batch[idx[(pos + k) % len(idx)]]) for k in range(per_step)]
+            pos += per_step
+            return pool.run(sl)
+        for _ in range(args.warmup):
+            step()
+        walls, iters, codes = [], 0, {}
+        for _ in range(args.steps):
+            w, it, cd, _ = step()
+            walls.append(w)
+            iters += it
+            for k, v in cd.items():
+                codes[k] = codes.get(k, 0) + v
+    finally:
+        pool.close()
+    total = sum(walls)
+    v = per_step * args.steps / total
+    sample = (f"each step: {per_step} instances of the same batch (consecutive slices of a fixed seeded "
+              f"sample of {len(idx)} stratified by size) solved to 1e-6 by the oracle (FP64, one instance per "
+              f"core, largest first); the reference's own Julia/CUDA.jl code cannot run here, the oracle is "
+              f"the C++ restatement of its algorithm")
     line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "instances/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.count / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)", "config": cfg, "iter_per_s": its / args.steps,
-            "cpu_baseline": {"value": v, "unit": "instances/s", "cores": r["cores"], "kind": "port",
-                             "sample": "each step: " + r["sample"] + " (the reference's Julia/CUDA.jl code "
-                                       "cannot run here; this is the C++ restatement of its algorithm)"},
+            "data": "synthetic (seeded)", "config": cfg, "iter_per_s": iters / total,
+            "statuses": {str(k): c for k, c in codes.items()},
+            "cpu_baseline": {"value": v, "unit": "instances/s", "cores": pool.cores, "kind": "port",
+                             "sample": sample},
             "e2e": {"value": v, "unit": "instances/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -393,7 +479,7 @@ def run_ours(args):
     layer = None if args.no_single or rank != 0 else differentiable_section(dev, stream)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_batch_rate(batch, args.cpu_seconds)
+        cpu = cpu_batch_rate(batch, args.cpu_sample, gpu_sols=sols)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "instances/s", "n_gpus": world, "steps": args.steps,

@@ -257,8 +257,9 @@ int pdcs_spmv_csr(int64_t m, int64_t n, int64_t nnz, const int32_t* rowptr, cons
  * m + nnz must not exceed 134,217,728 (PDCS_ERR_NOALLOC_LIMIT otherwise);
  * every GPU that loads the library keeps those 768 KiB until the process
  * exits.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress, once per device); make that first call before any
- * stream capture.  All calls share the one array: calls that overlap on the
+ * (cudaGetSymbolAddress, once per device and context: the cached address is
+ * looked up again when the device's context was destroyed and recreated);
+ * make that first call before any stream capture.  All calls share the one array: calls that overlap on the
  * GPU (different streams, no ordering) race on it.  Allocates nothing:
  * no cudaMalloc, cudaFree or allocating library routine. */
 int pdcs_spmv_csr_noalloc(int64_t m, int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* colind,

@@ -6,9 +6,18 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = [os.path.join(HERE, "csrc", "pdcs_solver.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("pdcs_kernels.cuh", "pdcs_device.cuh", "pdcs_preprocess.cuh",
-                                                     "pdcs_batch.cuh", "pdcs_batch_kernels.cuh", "pdcs_fp32.cuh", "pdcs_adjoint.cuh")] + [
-    os.path.join(ROOT, "include", "pdcs.h")]
+
+
+def deps():
+    """Every file the library is built from: all of csrc/ and include/, so a
+    header added later can never be left out of the staleness check."""
+    found = []
+    for d, pats in ((os.path.join(HERE, "csrc"), (".cu", ".cuh", ".h")), (os.path.join(ROOT, "include"), (".h",))):
+        if os.path.isdir(d):
+            found += [os.path.join(d, f) for f in sorted(os.listdir(d)) if f.endswith(pats)]
+    return found
+
+
 LIB = os.path.join(HERE, "libpdcs_b200.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++20",
               "-Xcompiler", "-fPIC", "-shared"]
@@ -25,7 +34,7 @@ def up_to_date():
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(d) <= t for d in DEPS)
+    return all(os.path.getmtime(d) <= t for d in deps())
 
 
 def build(force=False, verbose=False):

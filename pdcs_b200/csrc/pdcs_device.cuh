@@ -355,8 +355,15 @@ __device__ __noinline__ bool exp_root_bracketed(const ExpCtx& C, double lo, doub
         ga = sg * C.fs(a, 0);
       }
     } else {
+      // An endpoint at a root of N1 (sp = 0: v on the polar's boundary) or N2
+      // (lam = 0: v on the cone's boundary) where f vanishes to rounding is the
+      // root itself: v lies on a boundary within rounding of the membership
+      // tests, and the sign of f there is noise.
+      double dg, mag;
       a = lo;
-      ga = sg * C.fs(a, tlo & 3);
+      C.gd(a, tlo & 3, ga, dg, mag);
+      ga *= sg;
+      if ((tlo & 3) && fabs(ga) <= 16.0 * eps * mag) { *rho_out = a; return true; }
     }
     if (isinf(hi)) {
       double base = fmax(p, a);
@@ -369,8 +376,11 @@ __device__ __noinline__ bool exp_root_bracketed(const ExpCtx& C, double lo, doub
         gb = sg * C.fs(b, 0);
       }
     } else {
+      double dg, mag;
       b = hi;
-      gb = sg * C.fs(b, thi & 3);
+      C.gd(b, thi & 3, gb, dg, mag);
+      gb *= sg;
+      if ((thi & 3) && fabs(gb) <= 16.0 * eps * mag) { *rho_out = b; return true; }
     }
     if (!(isfinite(ga) && isfinite(gb))) return false;
     if (!((ga <= 0.0 && gb >= 0.0) || (ga >= 0.0 && gb <= 0.0))) return false;

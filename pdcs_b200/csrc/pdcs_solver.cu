@@ -2122,22 +2122,48 @@ static __device__ __align__(256) unsigned char g_spmv_noalloc_scratch[kNoAllocMa
 namespace {
 constexpr int kNoAllocMaxDevices = 128;
 std::mutex g_noalloc_mu;
-void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+struct NoAllocEntry {
+  void* ctx;   // the context the address was looked up in
+  void* addr;  // device address of g_spmv_noalloc_scratch in that context
+};
+NoAllocEntry g_noalloc[kNoAllocMaxDevices] = {};
+
+// The calling thread's current context (cuCtxGetCurrent, reached through the
+// runtime's driver entry-point table, so the library needs no -lcuda).
+void* current_context() {
+  using CtxGetCurrent = int (*)(void**);
+  static CtxGetCurrent fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<CtxGetCurrent>(nullptr);
+    return reinterpret_cast<CtxGetCurrent>(p);
+  }();
+  void* ctx = nullptr;
+  if (fn) fn(&ctx);
+  return ctx;
+}
 
 // Device address of the scratch array for the current device.  In host code
-// the array's name is only a host-side stand-in; the address must come from
-// cudaGetSymbolAddress with the device current, once per device.
+// the array's name is only a host-side stand-in; the address comes from
+// cudaGetSymbolAddress with the device current, once per device and context:
+// a context destroyed and recreated (cudaDeviceReset, a host runtime's device
+// reset) gets a fresh lookup instead of a stale address.
 int noalloc_scratch(void** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return PDCS_ERR_CUDA;
   if (dev < 0 || dev >= kNoAllocMaxDevices) return PDCS_ERR_INVALID;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  NoAllocEntry& e = g_noalloc[dev];
+  void* ctx = current_context();
+  if (!e.addr || !ctx || e.ctx != ctx) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_spmv_noalloc_scratch) != cudaSuccess || !p) return PDCS_ERR_CUDA;
-    g_noalloc_addr[dev] = p;
+    e.addr = p;
+    e.ctx = current_context();  // the lookup makes the primary context current if none was
   }
-  *out = g_noalloc_addr[dev];
+  *out = e.addr;
   return PDCS_OK;
 }
 }  // namespace

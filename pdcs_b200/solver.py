@@ -120,7 +120,8 @@ def _problem_struct(hold: _Holder, *, n, m, nb, c, G, h, mGzero, mGnonnegative, 
     if not on_device:
         if not (sp.issparse(G) and G.format == "csr"):
             G = sp.csr_matrix(G)
-        G.sort_indices()  # scipy remembers the answer on the matrix, so repeated solves skip the scan
+        if not G.has_sorted_indices:  # scipy caches the check on the matrix; repeated solves skip the scan
+            G = G.sorted_indices()  # a sorted copy: the caller's arrays are never reordered
         if G.shape[0] != m:
             raise ValueError("m does not match the size of G")
         if G.shape[1] != n:

@@ -193,3 +193,42 @@ def solve_tight(p, **kw):
     every 2000 attempts; tighter requests can end in the adaptive step's divergence)."""
     r = B.solve(p, threads=1, rel_tol=1e-9, abs_tol=1e-9, **kw)
     return r["x"], r["y"], r
+
+
+def adjoint_kkt(p, x, y, gx, gy=None):
+    """Gradients of L from the conic KKT conditions, independent of any step
+    sizes: (x, y) is optimal iff F(z) = 0 with
+        F_x = x - P_X(a),      a = x - (c - G'y)   (-(c - G'y) in N_X(x)),
+        F_y = y - P_{K_d*}(b), b = y - (G x - h)   (Gx - h in K_d, y in K_d*, <y, Gx - h> = 0),
+    so dz*/dtheta = -(dF/dz)^{-1} dF/dtheta and, with v solving
+    (dF/dz)' v = g,
+        dL/dc = -D_X v_x,  dL/dh = D_K v_y,
+        dL/dG_ij = (D_X v_x)_j y_i - (D_K v_y)_i x_j,
+        dL/dl_j = v_x,j [a_j < l_j],  dL/du_j = v_x,j [a_j > u_j]
+    (D_X, D_K: the projections' Jacobians at a and b, symmetric).  Dense
+    FP64 throughout; nothing is shared with the PDHG fixed-point form but the
+    projections and their Jacobians."""
+    G = sp.csr_matrix(p.G)
+    G.sort_indices()
+    Gd = G.toarray()
+    n, m = p.n, p.m
+    a = x - (p.c - Gd.T @ y)
+    b = y - (Gd @ x - p.h)
+    DX = jacobian(p, "x", a)
+    DK = jacobian(p, "y", b)
+    J = np.zeros((n + m, n + m))
+    J[:n, :n] = np.eye(n) - DX
+    J[:n, n:] = -DX @ Gd.T
+    J[n:, :n] = DK @ Gd
+    J[n:, n:] = np.eye(m) - DK
+    g = np.concatenate([gx, np.zeros(m) if gy is None else gy])
+    v = np.linalg.lstsq(J.T, g, rcond=None)[0]
+    vx, vy = v[:n], v[n:]
+    ax = DX @ vx
+    ky = DK @ vy
+    rows = np.repeat(np.arange(m), np.diff(G.indptr))
+    cols = G.indices
+    lo = a[:p.nb] < p.bl
+    hi = a[:p.nb] > p.bu
+    return {"c": -ax, "h": ky, "G": ax[cols] * y[rows] - ky[rows] * x[cols],
+            "bl": vx[:p.nb] * lo, "bu": vx[:p.nb] * hi}

@@ -59,3 +59,13 @@ def test_validation_errors_mirror_reference():
         solver.rpdhg_gpu_solve(**{**kw, "bl": bl})
     with pytest.raises(ValueError, match="does not match the size of G"):
         solver.rpdhg_gpu_solve(**{**kw, "m": kw["m"] + 3, "mGzero": kw["mGzero"] + 3})
+
+
+def test_build_staleness_check_covers_every_source():
+    """Every file under csrc/ and include/ takes part in the library's
+    staleness check, so editing any header triggers a rebuild."""
+    listed = set(build.deps())
+    for d in (os.path.join(ROOT, "pdcs_b200", "csrc"), os.path.join(ROOT, "include")):
+        for f in os.listdir(d):
+            if f.endswith((".cu", ".cuh", ".h")):
+                assert os.path.join(d, f) in listed, f

@@ -1,0 +1,82 @@
+"""Exit paths of termination.jl other than optimality and infeasibility
+(src/pdcs_gpu/termination.jl:74-90, :181-258), made on the host: NaN or Inf in
+the data (exit 8, numerical_error_nan: the objectives turn NaN by the first
+check), the iteration limit max_outer_iter * max_inner_iter (exit 1) and the
+time limit (exit 6), both on an instance that needs more than one check
+interval (2000 attempts).  The oracle (CPU) pins the expected codes; the
+GPU single solver and the batch must report the same, and a failing member of
+a batch must leave the other members' solutions untouched.
+
+Exit 9 (numerical_error_inf) needs |pObj - dObj| to overflow while both
+objectives stay finite (opposite-signed objectives near DBL_MAX); no data
+reaches it through the preconditioner, so it is not exercised here."""
+import copy
+
+import numpy as np
+import pytest
+
+from oracle import binding as B
+from pdcs_b200 import problems
+
+
+def _nan_c():
+    p = problems.mixed_small()
+    p.c = p.c.copy()
+    p.c[3] = np.nan
+    p.name = "nan_c"
+    return p
+
+
+def _inf_h():
+    p = problems.mixed_small()
+    p.h = p.h.copy()
+    p.h[2] = np.inf
+    p.name = "inf_h"
+    return p
+
+
+def _slow():
+    # 10000 attempts to 1e-6 in the oracle: the first check (2000) is not optimal
+    return problems.logreg_exp_c1(samples=300, features=30, density=0.3)
+
+
+CASES = [("nan_c", _nan_c, {}, 8), ("inf_h", _inf_h, {}, 8),
+         ("max_iter", _slow, dict(max_outer_iter=1, max_inner_iter=100), 1),
+         ("time_limit", _slow, dict(time_limit=1e-3), 6)]
+
+
+@pytest.mark.parametrize("name,make,opts,code", CASES, ids=[c[0] for c in CASES])
+def test_oracle_exit_codes(name, make, opts, code):
+    o = B.solve(make(), threads=1, **opts)
+    assert o["exit_code"] == code, (name, o["exit_code"])
+    assert o["iter"] == 2000  # decided at the first check
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,make,opts,code", CASES, ids=[c[0] for c in CASES])
+def test_gpu_exit_codes_match_oracle(cuda, name, make, opts, code):
+    from pdcs_b200 import solver
+    g = solver.solve_problem(make(), **opts)
+    assert g.info.exit_code == code, (name, g)
+    assert g.info.iter == 2000
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_member_with_nan_leaves_the_others_optimal(cuda, precision):
+    from _parity import assert_objective
+    from pdcs_b200 import solver
+    good = [problems.mixed_small(seed=7)] + problems.batch_socp_c3(count=4, seed=13, nmin=50, nmax=300)
+    batch = good[:2] + [_nan_c()] + good[2:] + [_inf_h()]
+    sols, _ = solver.rpdhg_gpu_solve_batch(batch, precision=precision, time_limit=300)
+    alone, _ = solver.rpdhg_gpu_solve_batch(good, precision=precision, time_limit=300)
+    assert sols[2].info.exit_code == 8 and sols[-1].info.exit_code == 8
+    rest = sols[:2] + sols[3:-1]
+    for p, g, a in zip(good, rest, alone):
+        assert g.info.exit_status == "optimal", (p.name, g)
+        assert np.all(np.isfinite(g.primal)) and np.all(np.isfinite(g.dual))
+        e = B.evaluate(p, g.primal, g.dual)
+        assert max(e["primal_res_gpu_form"], e["dual_res"], e["rel_gap"]) < 1.05e-6, (p.name, e)
+        assert_objective(p, g.info.pObj, "with failing members")
+        # a member's trajectory does not depend on its neighbours
+        assert g.info.iter == a.info.iter, (p.name, g.info.iter, a.info.iter)

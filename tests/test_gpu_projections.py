@@ -71,3 +71,32 @@ def test_unscaled_codes_match_oracle(cuda):
         sl = slice(h, h + d)
         ref = B.project_block(kmap[c], v[sl], None, bl[sl], bu[sl])
         assert np.abs(out[sl] - ref).max() <= 1e-12 * max(1.0, np.abs(v[sl]).max()), (c, v[sl], out[sl], ref)
+
+
+REF_GOLDEN = "tests/golden/ref_projections.npz"
+REF_TAGS = {"soc_u": 20, "soc_s": 22, "rsoc_u": 23, "rsoc_s": 25, "exp_u": 26, "exp_s": 27, "dexp_u": 28,
+            "dexp_s": 29}
+
+
+@pytest.mark.parametrize("tag", sorted(REF_TAGS))
+def test_codes_match_reference_and_high_precision(cuda, tag):
+    """pdcs_block_proj against the reference's own kernel outputs (oracle/_ref,
+    frozen in tests/golden/ref_projections.npz) and the 60-400 digit KKT
+    projections: equal to 1e-12 relative to the block's magnitude on every
+    block, and to the reference on every block where the reference's output is
+    the projection."""
+    g = np.load(REF_GOLDEN)
+    lens = g[tag + "_len"]
+    heads, ns = _blocks_from_lengths(lens)
+    v, S, pr, pt = g[tag + "_v"], g[tag + "_S"], g[tag + "_ref"], g[tag + "_truth"]
+    scaled = tag.endswith("_s")
+    out = _run(cuda, v, S if scaled else None, heads, ns, [REF_TAGS[tag]] * len(lens))
+    exact = 0
+    for i, (h, d) in enumerate(zip(heads, ns)):
+        sl = slice(h, h + d)
+        scale = max(1.0, np.abs(v[sl]).max())
+        assert np.abs(out[sl] - pt[sl]).max() <= 1e-12 * scale, (tag, i, v[sl], out[sl], pt[sl])
+        if not g[tag + "_hang"][i] and np.abs(pr[sl] - pt[sl]).max() <= 1e-12 * scale:
+            exact += 1
+            assert np.abs(out[sl] - pr[sl]).max() <= 2e-12 * scale, (tag, i)
+    assert exact >= 0.4 * len(lens)

@@ -3,6 +3,7 @@ import numpy as np
 import pytest
 
 from oracle import binding as B
+from _parity import assert_objective
 from pdcs_b200 import problems, solver
 
 pytestmark = pytest.mark.gpu
@@ -42,8 +43,8 @@ def test_solution_parity(cuda, name):
     # with a small allowance for the evaluator's own rounding
     for e in (eg, eo):
         assert max(e["primal_res_gpu_form"], e["dual_res"], e["rel_gap"]) < 1.05e-6, e
-    rel = abs(eg["pobj"] - eo["pobj"]) / (1 + abs(eo["pobj"]))
-    assert rel <= 2e-6, (eg["pobj"], eo["pobj"])
+    assert_objective(p, eg["pobj"], "gpu")
+    assert_objective(p, eo["pobj"], "oracle")
     assert abs(g.info.pObj - eg["pobj"]) <= 1e-9 * (1 + abs(eg["pobj"]))
 
 
@@ -78,7 +79,8 @@ def test_kkt_restart_variant(cuda):
     g = solver.solve_problem(p, time_limit=120, use_kkt_restart=True, use_duality_gap_restart=False)
     o = B.solve(p, threads=2, use_kkt_restart=1, use_duality_gap_restart=0)
     assert g.info.exit_status == "optimal" and o["exit_code"] == 0
-    assert abs(g.info.pObj - o["primal_objective"]) <= 2e-6 * (1 + abs(o["primal_objective"]))
+    assert_objective(p, g.info.pObj, "gpu")
+    assert_objective(p, o["primal_objective"], "oracle")
 
 
 @pytest.mark.parametrize("name", ["primal_infeasible_lp", "dual_infeasible_lp"])
@@ -103,7 +105,8 @@ def test_resolving_fallback_matches_oracle(cuda, name):
     g = solver.solve_problem(p, force_resolving=True, time_limit=120)
     o = B.solve(p, threads=2, force_resolving=1, time_limit=120)
     assert g.info.exit_status == "optimal" and o["exit_code"] == 0
-    assert abs(g.info.pObj - o["primal_objective"]) <= 2e-6 * (1 + abs(o["primal_objective"]))
+    assert_objective(p, g.info.pObj, "gpu")
+    assert_objective(p, o["primal_objective"], "oracle")
 
 
 def test_spmv_schedules_agree(cuda):

@@ -64,3 +64,38 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):
     rc = lib.pdcs_spmv_csr_noalloc(m, 1, 1, ibuf.data_ptr(), ibuf.data_ptr(), buf.data_ptr(), buf.data_ptr(),
                                    buf.data_ptr(), None)
     assert rc == LIMIT_STATUS
+
+
+def test_noalloc_empty_rows_at_cta_boundaries_and_no_nonzeros(cuda):
+    """Rows without nonzeros where the merge path splits CTAs (2048 merge
+    items, one per row end and one per nonzero, per CTA), a row that spans
+    several CTAs, and a matrix with no nonzeros at all (NULL column indices,
+    values and x).  Each result is compared with pdcs_spmv_csr and A @ x."""
+    import torch
+    from pdcs_b200 import capi
+    lib = capi.load()
+    rng = np.random.default_rng(7)
+    lens = [0] * 2040 + [5] + [0] * 10 + [4000] + [0] * 3000 + [1] * 100 + [0] * 2100 + [3] + [0] * 2047
+    n = 6000
+    indptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    indices = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for k in lens if k]).astype(np.int32)
+    A = sp.csr_matrix((rng.standard_normal(indptr[-1]), indices, indptr), shape=(len(lens), n))
+    x = rng.standard_normal(n)
+    bufs = _device_csr(A, x, cuda)
+    for _ in range(2):
+        y_ref = torch.full((A.shape[0],), float("nan"), dtype=torch.float64, device=cuda)
+        y_new = torch.full((A.shape[0],), float("nan"), dtype=torch.float64, device=cuda)
+        assert _call(lib.pdcs_spmv_csr, A, bufs, y_ref) == 0
+        assert _call(lib.pdcs_spmv_csr_noalloc, A, bufs, y_new) == 0
+        torch.cuda.synchronize()
+        a, b = y_new.cpu().numpy(), y_ref.cpu().numpy()
+        assert np.all(np.isfinite(a))
+        assert np.allclose(a, b, rtol=1e-12, atol=1e-12 * max(1.0, np.abs(b).max()))
+        assert np.allclose(a, A @ x, rtol=1e-12, atol=1e-12 * max(1.0, np.abs(b).max()))
+    m = 5000
+    rp = torch.zeros(m + 1, dtype=torch.int32, device=cuda)
+    for _ in range(2):
+        y = torch.full((m,), float("nan"), dtype=torch.float64, device=cuda)
+        assert lib.pdcs_spmv_csr_noalloc(m, 7, 0, rp.data_ptr(), None, None, None, y.data_ptr(), None) == 0
+        torch.cuda.synchronize()
+        assert torch.count_nonzero(y).item() == 0
