@@ -1,10 +1,13 @@
 """Objective parity at the north star's bar (test helper).
 
 A solve stopped at the 1e-6 criteria is compared with the problem's optimum,
-taken from the oracle run to 1e-9 on the same instance: every reported
+taken from the oracle run to 1e-8 on the same instance: every reported
 objective must lie within 1e-6 (relative, 1 + |optimum|) of it.  Two 1e-6
 solutions can differ from each other by up to twice that, so solutions are
-never compared with each other at 1e-6, only each with the optimum."""
+never compared with each other at 1e-6, only each with the optimum.  The
+reference's algorithm can run past an almost exact solution and diverge when
+asked for 1e-9 or less on some instances (an exit check finds NaN or a false
+infeasibility certificate), so 1e-8 is tried first, then 1e-9 and 1e-7."""
 from oracle import binding as B
 
 OBJ_TOL = 1e-6
@@ -14,8 +17,13 @@ _cache = {}
 def optimum(p):
     key = id(p)
     if key not in _cache:
-        o = B.solve(p, threads=0, rel_tol=1e-9, abs_tol=1e-9, time_limit=600)
-        assert o["exit_code"] == 0, (getattr(p, "name", p), o["exit_code"])
+        codes = []
+        for tol in (1e-8, 1e-9, 1e-7):
+            o = B.solve(p, threads=0, rel_tol=tol, abs_tol=tol, time_limit=600)
+            codes.append(o["exit_code"])
+            if o["exit_code"] == 0:
+                break
+        assert o["exit_code"] == 0, (getattr(p, "name", p), codes)
         _cache[key] = (p, o["primal_objective"])  # keep p alive so its id stays unique
     return _cache[key][1]
 

@@ -2,8 +2,8 @@
 (src/pdcs_gpu/termination.jl:74-90, :181-258), made on the host: NaN or Inf in
 the data (exit 8, numerical_error_nan: the objectives turn NaN by the first
 check), the iteration limit max_outer_iter * max_inner_iter (exit 1) and the
-time limit (exit 6), both on an instance that needs more than one check
-interval (2000 attempts).  The oracle (CPU) pins the expected codes; the
+time limit (exit 6), both on an instance with a 1e-12 tolerance, which no
+solver meets at the first check (2000 attempts).  The oracle (CPU) pins the expected codes; the
 GPU single solver and the batch must report the same, and a failing member of
 a batch must leave the other members' solutions untouched.
 
@@ -36,13 +36,15 @@ def _inf_h():
 
 
 def _slow():
-    # 10000 attempts to 1e-6 in the oracle: the first check (2000) is not optimal
+    # far from a 1e-12 solution at the first check (2000 attempts)
     return problems.logreg_exp_c1(samples=300, features=30, density=0.3)
 
 
+# a 1e-12 tolerance keeps every solver short of optimality at the first check
+HARD = dict(rel_tol=1e-12, abs_tol=1e-12)
 CASES = [("nan_c", _nan_c, {}, 8), ("inf_h", _inf_h, {}, 8),
-         ("max_iter", _slow, dict(max_outer_iter=1, max_inner_iter=100), 1),
-         ("time_limit", _slow, dict(time_limit=1e-3), 6)]
+         ("max_iter", _slow, dict(max_outer_iter=1, max_inner_iter=100, **HARD), 1),
+         ("time_limit", _slow, dict(time_limit=1e-3, **HARD), 6)]
 
 
 @pytest.mark.parametrize("name,make,opts,code", CASES, ids=[c[0] for c in CASES])
@@ -58,7 +60,12 @@ def test_gpu_exit_codes_match_oracle(cuda, name, make, opts, code):
     from pdcs_b200 import solver
     g = solver.solve_problem(make(), **opts)
     assert g.info.exit_code == code, (name, g)
-    assert g.info.iter == 2000
+    if name == "time_limit":
+        # the GPU solver also reads the clock between its CUDA graphs of attempts,
+        # so it stops at the first graph after the limit, not only at a check
+        assert 0 < g.info.iter <= 2000
+    else:
+        assert g.info.iter == 2000
 
 
 @pytest.mark.gpu
