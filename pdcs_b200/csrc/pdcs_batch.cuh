@@ -31,6 +31,7 @@
 #include "pdcs_batch_kernels.cuh"
 #include "pdcs_bsearch.cuh"
 #include "pdcs_tiles.cuh"
+#include "pdcs_fused.cuh"
 #include "pdcs_tail.cuh"
 
 namespace pdcs {
@@ -345,6 +346,25 @@ class BatchSolver : public Solver {
   static constexpr int64_t kTileMaxRows = 4096;
   static constexpr size_t kTileMaxSmem = 160 * 1024;
   void setup_tiles();
+  // fused tile kernels of the full iteration graph (SELL-32 rows, the step and
+  // projections of the tile's rows, per-tile partial sums): [0] G, the dual
+  // step of y's rows; [1] G', the primal step of x's rows.  Used when the
+  // batch has instance tiles and every SOC / RSOC block has at most 32 elements.
+  struct Fused {
+    FusedCsr F{};
+    std::vector<int64_t> first;    // K + 1: tile range of every instance
+    std::vector<int64_t> nnz;      // nonzeros of every tile
+    int64_t* first_dev = nullptr;  // the same on the device (control sums)
+    double* tpart = nullptr;       // per-tile partial sums (1 for G', 2 for G)
+    float* sv32 = nullptr;         // SELL values: FP32 bulk ...
+    double* sv64 = nullptr;        // ... or FP64
+    int grid = 1;
+  } fu_[2];
+  bool fused_ = false;
+  static constexpr int64_t kFusedMaxRows = 2048;
+  void setup_fused();
+  template <class T, int NV, class Op>
+  int fused_grid(const FusedCsr& F, bool exp);
   // iteration graphs: [0] grids for the whole batch, [1] the tail graph, grids
   // capped for rounds in which few nonzeros iterate (most CTAs of the full
   // grids would find no work and return, at the cost of their launch)
@@ -955,6 +975,313 @@ void BatchSolver::setup_tiles() {
   tiled_ = true;
 }
 
+// Fused tiles (fused_tile_kernel) for both matrices.  A tile is a range of one
+// instance's rows in the instance's own order, cut only between cones: its
+// elementwise rows come first, then whole SOC / RSOC blocks, exponential and
+// dual-exponential triples.  Per tile: the SELL-32 slices of its rows (sorted
+// by length), the lane-group tasks of its blocks by size class, its exp records.
+void BatchSolver::setup_fused() {
+  fused_ = false;
+  if (!tiled_) return;
+  for (int w = 0; w < 2; ++w)
+    for (int8_t c : cone_cls_[w])
+      if (c >= kCls - 1) return;  // a block of more than 32 elements: the unfused kernels
+  std::vector<int32_t> rpt(n_ + 1);
+  PDCS_CUDA(cudaMemcpyAsync(rpt.data(), Gt_.rp, sizeof(int32_t) * (n_ + 1), cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  // the layout of one instance, with instance-local offsets (concatenated below)
+  struct Part {
+    std::vector<FusedTile> tiles;
+    std::vector<int64_t> sb, nnz;
+    std::vector<int32_t> sl, srow;
+    std::vector<int16_t> so;
+    std::vector<int4> task, crec, xrec;
+    int64_t pad = 0;
+    int32_t max_rows = 1;
+  };
+  for (int w = 0; w < 2; ++w) {
+    // w = 0: G, rows are y's elements (side 1 of the cone lists); w = 1: G', rows are x's (side 0)
+    const int cs = w == 0 ? 1 : 0;
+    const ConeTable& CT = w == 0 ? YI : XI;
+    const std::vector<int32_t>& rp = w == 0 ? h_rp_ : rpt;
+    const std::vector<int64_t>& rs = w == 0 ? yrun_start_ : xrun_start_;
+    const std::vector<int64_t>& rl = w == 0 ? yrun_len_ : xrun_len_;
+    const std::vector<int64_t>& lc = w == 0 ? yloc_ : xloc_;
+    const int nelem_runs = w == 0 ? 2 : 1;  // y: zero, nonneg; x: box
+    auto build = [&](int64_t k, Part& P) {
+      struct Atom {
+        int64_t ord, j;                 // instance-local ordinal and merged index of the first element
+        int32_t size, type, id, flags;  // type 0 elementwise, 1 SOC / RSOC block, 2 exp triple
+      };
+      const int64_t nk = w == 0 ? probs_[k].m : probs_[k].n;
+      std::vector<int64_t> mrow(nk), rlen(nk);  // merged row and length of every instance row
+      for (int q = 0; q < kMaxRuns; ++q)
+        for (int64_t i = 0; i < rl[k * kMaxRuns + q]; ++i) {
+          const int64_t o = lc[k * kMaxRuns + q] + i, r = rs[k * kMaxRuns + q] + i;
+          mrow[o] = r;
+          rlen[o] = rp[r + 1] - rp[r];
+        }
+      auto ord_of = [&](int64_t j) {
+        for (int q = 0; q < kMaxRuns; ++q) {
+          const int64_t a = rs[k * kMaxRuns + q], L = rl[k * kMaxRuns + q];
+          if (j >= a && j < a + L) return lc[k * kMaxRuns + q] + (j - a);
+        }
+        throw std::logic_error("fused tiles: element outside its instance's runs");
+      };
+      std::vector<Atom> at;
+      at.reserve(nk);
+      for (int q = 0; q < nelem_runs; ++q)
+        for (int64_t i = 0; i < rl[k * kMaxRuns + q]; ++i)
+          at.push_back({lc[k * kMaxRuns + q] + i, rs[k * kMaxRuns + q] + i, 1, 0, 0, 0});
+      const std::array<int64_t, 8>& c = cones_[cs][k];
+      for (int part = 0; part < 2; ++part)
+        for (int64_t i = c[2 * part]; i < c[2 * part + 1]; ++i) {
+          const int4 d = cone_desc_[cs][i];
+          at.push_back({ord_of(d.x), d.x, d.y & 0x3fffffff, 1, (int32_t)i, d.y});
+        }
+      for (int part = 0; part < 2; ++part)
+        for (int64_t kk = c[4 + 2 * part]; kk < c[5 + 2 * part]; ++kk) {
+          const int64_t j = kk < CT.exp_count ? CT.exp_base + 3 * kk : CT.dexp_base + 3 * (kk - CT.exp_count);
+          at.push_back({ord_of(j), j, 3, 2, (int32_t)kk, 0});
+        }
+      std::stable_sort(at.begin(), at.end(), [](const Atom& a, const Atom& b) { return a.ord < b.ord; });
+      const int64_t ncols = w == 0 ? probs_[k].n : probs_[k].m;
+      const int64_t big = O.spmv_tiles > 0 ? (int64_t)O.spmv_tiles : kTileNnz;
+      const int64_t cap = std::min(big, std::max(kTileSmallNnz, 16 * ncols));
+      size_t a0 = 0;
+      int64_t rows = 0, acc = 0;
+      std::vector<int32_t> loc;
+      std::vector<int4> recs[kCls];
+      auto cut = [&](size_t a1) {  // atoms [a0, a1) form a tile
+        FusedTile T{};
+        T.inst = (int32_t)k;
+        T.o0 = (int32_t)at[a0].ord;
+        T.o1 = (int32_t)(at[a1 - 1].ord + at[a1 - 1].size);
+        int32_t ew = 0;
+        for (size_t a = a0; a < a1 && at[a].type == 0; ++a) ew++;
+        T.ew = ew;
+        const int32_t nr = T.o1 - T.o0;
+        P.max_rows = std::max(P.max_rows, nr);
+        // SELL-32 slices of the tile's rows, longest first
+        loc.resize(nr);
+        for (int32_t i = 0; i < nr; ++i) loc[i] = i;
+        std::stable_sort(loc.begin(), loc.end(), [&](int32_t a, int32_t b) { return rlen[T.o0 + a] > rlen[T.o0 + b]; });
+        T.s0 = (int32_t)P.sl.size();
+        for (int32_t i = 0; i < nr; i += kSellC) {
+          const int32_t L = (int32_t)rlen[T.o0 + loc[i]];
+          P.sb.push_back(P.pad);
+          P.sl.push_back(L);
+          for (int l = 0; l < kSellC; ++l) {
+            const bool ok = i + l < nr;
+            P.so.push_back(ok ? (int16_t)loc[i + l] : (int16_t)-1);
+            P.srow.push_back(ok ? (int32_t)mrow[T.o0 + loc[i + l]] : -1);
+          }
+          P.pad += (int64_t)L * kSellC;
+        }
+        T.s1 = (int32_t)P.sl.size();
+        // lane-group tasks of the blocks, class by class
+        for (auto& r : recs) r.clear();
+        for (size_t a = a0; a < a1; ++a)
+          if (at[a].type == 1)
+            recs[cone_cls_[cs][at[a].id]].push_back(
+                make_int4((int32_t)at[a].j, at[a].flags, at[a].id, (int32_t)(at[a].ord - T.o0)));
+        T.t0 = (int32_t)P.task.size();
+        for (int cls = 0; cls < kCls - 1; ++cls) {
+          const int g = 2 << cls, per = 32 / g;
+          for (size_t r = 0; r < recs[cls].size(); r += per) {
+            const int cnt = (int)std::min<size_t>(per, recs[cls].size() - r);
+            P.task.push_back(make_int4((int32_t)P.crec.size(), cnt, g, 0));
+            P.crec.insert(P.crec.end(), recs[cls].begin() + r, recs[cls].begin() + r + cnt);
+          }
+        }
+        T.t1 = (int32_t)P.task.size();
+        T.x0 = (int32_t)P.xrec.size();
+        for (size_t a = a0; a < a1; ++a)
+          if (at[a].type == 2) P.xrec.push_back(make_int4((int32_t)at[a].j, at[a].id, (int32_t)(at[a].ord - T.o0), 0));
+        T.x1 = (int32_t)P.xrec.size();
+        P.tiles.push_back(T);
+        P.nnz.push_back(acc);
+        a0 = a1;
+        rows = 0;
+        acc = 0;
+      };
+      for (size_t a = 0; a < at.size(); ++a) {
+        if (rows > 0 && rows + at[a].size > kFusedMaxRows) cut(a);
+        for (int32_t e = 0; e < at[a].size; ++e) acc += rlen[at[a].ord + e];
+        rows += at[a].size;
+        if (acc >= cap) cut(a + 1);
+      }
+      if (a0 < at.size()) cut(at.size());
+    };
+    // instances in parallel, then concatenated in instance order
+    std::vector<Part> parts(K_);
+    {
+      const int nth = (int)std::max<int64_t>(
+          1, std::min<int64_t>(K_ / 64, (int64_t)std::max(1u, std::thread::hardware_concurrency())));
+      std::vector<std::thread> th;
+      std::exception_ptr err = nullptr;
+      std::mutex emu;
+      for (int t = 0; t < nth; ++t)
+        th.emplace_back([&, t] {
+          try {
+            for (int64_t k = t; k < K_; k += nth) build(k, parts[k]);
+          } catch (...) {
+            std::lock_guard<std::mutex> lk(emu);
+            err = std::current_exception();
+          }
+        });
+      for (auto& x : th) x.join();
+      if (err) std::rethrow_exception(err);
+    }
+    Fused& fu = fu_[w];
+    Part all;
+    fu.first.assign(K_ + 1, 0);
+    for (int64_t k = 0; k < K_; ++k) {
+      Part& P = parts[k];
+      fu.first[k] = (int64_t)all.tiles.size();
+      const int32_t so0 = (int32_t)all.sl.size(), to0 = (int32_t)all.task.size(), xo0 = (int32_t)all.xrec.size();
+      const int32_t co0 = (int32_t)all.crec.size();
+      for (FusedTile T : P.tiles) {
+        T.s0 += so0;
+        T.s1 += so0;
+        T.t0 += to0;
+        T.t1 += to0;
+        T.x0 += xo0;
+        T.x1 += xo0;
+        all.tiles.push_back(T);
+      }
+      for (int64_t b : P.sb) all.sb.push_back(b + all.pad);
+      for (int4 t : P.task) all.task.push_back(make_int4(t.x + co0, t.y, t.z, t.w));
+      all.sl.insert(all.sl.end(), P.sl.begin(), P.sl.end());
+      all.so.insert(all.so.end(), P.so.begin(), P.so.end());
+      all.srow.insert(all.srow.end(), P.srow.begin(), P.srow.end());
+      all.crec.insert(all.crec.end(), P.crec.begin(), P.crec.end());
+      all.xrec.insert(all.xrec.end(), P.xrec.begin(), P.xrec.end());
+      all.nnz.insert(all.nnz.end(), P.nnz.begin(), P.nnz.end());
+      all.pad += P.pad;
+      all.max_rows = std::max(all.max_rows, P.max_rows);
+      P = Part();  // release as we go
+    }
+    fu.first[K_] = (int64_t)all.tiles.size();
+    fu.nnz = std::move(all.nnz);
+    std::vector<FusedTile>& tiles = all.tiles;
+    std::vector<int64_t>& sb = all.sb;
+    std::vector<int32_t>& sl = all.sl;
+    std::vector<int16_t>& so = all.so;
+    std::vector<int32_t>& srow = all.srow;
+    std::vector<int4>& task = all.task;
+    std::vector<int4>& crec = all.crec;
+    std::vector<int4>& xrec = all.xrec;
+    const int64_t pad = all.pad;
+    const int32_t max_rows = all.max_rows;
+    if (tiles.size() > (size_t)INT32_MAX || sl.size() > (size_t)INT32_MAX) return;
+    {  // the layout's invariants, checked once on the host before any kernel reads it
+      auto bad = [](const char* what) { throw std::logic_error(std::string("fused tiles: ") + what); };
+      for (int64_t k = 0; k < K_; ++k) {
+        const int64_t nk = w == 0 ? probs_[k].m : probs_[k].n;
+        int64_t o = 0;
+        for (int64_t t = fu.first[k]; t < fu.first[k + 1]; ++t) {
+          const FusedTile& T = tiles[t];
+          if (T.inst != k || T.o0 != o || T.o1 <= T.o0 || T.o1 - T.o0 > max_rows || T.ew > T.o1 - T.o0) bad("row ranges");
+          o = T.o1;
+          const int32_t nr = T.o1 - T.o0;
+          std::vector<uint8_t> seen(nr, 0);
+          for (int32_t sI = T.s0; sI < T.s1; ++sI)
+            for (int l = 0; l < kSellC; ++l) {
+              const int16_t v = so[(size_t)sI * kSellC + l];
+              if (v < -1 || v >= nr || (v >= 0 && seen[v]++)) bad("slice slots");
+            }
+          for (int32_t i = 0; i < nr; ++i)
+            if (!seen[i]) bad("a row without a slot");
+          for (int32_t q = T.t0; q < T.t1; ++q)
+            for (int r = 0; r < task[q].y; ++r) {
+              const int4 cr = crec[task[q].x + r];
+              if (cr.w < T.ew || cr.w + (cr.y & 0x3fffffff) > nr || (cr.y & 0x3fffffff) > task[q].z) bad("cone records");
+            }
+          for (int32_t q = T.x0; q < T.x1; ++q)
+            if (xrec[q].z < T.ew || xrec[q].z + 3 > nr) bad("exp records");
+        }
+        if (o != nk) bad("rows of an instance not covered");
+      }
+    }
+    // device copies
+    auto up = [&](const auto& v) {
+      using E = typename std::decay_t<decltype(v)>::value_type;
+      E* d = A.alloc<E>(std::max<size_t>(v.size(), 1));
+      if (!v.empty()) PDCS_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(E) * v.size(), cudaMemcpyHostToDevice, s_));
+      return d;
+    };
+    FusedCsr& F = fu.F;
+    F.tiles = up(tiles);
+    F.ntiles = (int64_t)tiles.size();
+    F.act = A.alloc<int32_t>(std::max<size_t>(tiles.size(), 1));
+    F.n_act = A.alloc<int64_t>(1);
+    F.sb = up(sb);
+    F.sl = up(sl);
+    F.so = up(so);
+    F.task = up(task);
+    F.crec = up(crec);
+    F.xrec = up(xrec);
+    F.rows = w == 0 ? ry_ : rx_;
+    F.cols = w == 0 ? rx_ : ry_;
+    F.rloc = tl_[w].T.rloc;
+    F.cloc = tl_[w].T.cloc;
+    F.max_cols = tl_[w].T.max_cols;
+    F.max_rows = max_rows;
+    fu.first_dev = up(fu.first);
+    fu.tpart = A.alloc<double>(std::max<size_t>(tiles.size(), 1) * (w == 0 ? 2 : 1));
+    int32_t* d_srow = up(srow);
+    uint16_t* sc = A.alloc<uint16_t>(std::max<int64_t>(pad, 1));
+    F.sc = sc;
+    const int64_t nsl = (int64_t)sl.size();
+    const int fg = (int)std::max<int64_t>(1, std::min<int64_t>((nsl * kSellC + kThreads - 1) / kThreads, 148 * 32));
+    const CsrDev& M = w == 0 ? G_ : Gt_;
+    if (fp32_) {
+      fu.sv32 = A.alloc<float>(std::max<int64_t>(pad, 1));
+      const CsrT<float>& M32 = w == 0 ? G32_ : Gt32_;
+      sell_fill_kernel<float><<<fg, kThreads, 0, s_>>>(nsl, F.sb, F.sl, d_srow, M.rp, M32.v, tl_[w].T.cl, fu.sv32, sc);
+    } else {
+      fu.sv64 = A.alloc<double>(std::max<int64_t>(pad, 1));
+      sell_fill_kernel<double><<<fg, kThreads, 0, s_>>>(nsl, F.sb, F.sl, d_srow, M.rp, M.v, tl_[w].T.cl, fu.sv64, sc);
+    }
+    PDCS_CUDA(cudaGetLastError());
+    PDCS_CUDA(cudaStreamSynchronize(s_));  // the host vectors above are temporaries
+  }
+  const bool ex = XI.exp_count + XI.dexp_count > 0, ey = YI.exp_count + YI.dexp_count > 0;
+  if (fp32_) {
+    fu_[1].grid = fused_grid<float, 1, FusedPrimal32>(fu_[1].F, ex);
+    fu_[0].grid = fused_grid<float, kPair, FusedDual32>(fu_[0].F, ey);
+  } else {
+    fu_[1].grid = fused_grid<double, 1, FusedPrimal64>(fu_[1].F, ex);
+    fu_[0].grid = fused_grid<double, 2, FusedDual64>(fu_[0].F, ey);
+  }
+  fused_ = fu_[0].grid > 0 && fu_[1].grid > 0;
+  if (O.verbose)
+    std::printf("[pdcs_b200 setup] fused tiles: G %lld tiles, grid %d; G' %lld tiles, grid %d%s\n",
+                (long long)fu_[0].F.ntiles, fu_[0].grid, (long long)fu_[1].F.ntiles, fu_[1].grid,
+                fused_ ? "" : " (not used: shared memory)");
+}
+
+// CTAs of a fused kernel: resident CTAs per SM (registers and shared memory) x SMs,
+// at most one per tile; 0 when one CTA does not fit.
+template <class T, int NV, class Op>
+int BatchSolver::fused_grid(const FusedCsr& F, bool exp) {
+  const size_t smem = fused_smem_bytes<T, NV>(F);
+  if (smem > 220 * 1024) return 0;
+  int dev = 0, sms = 148, per = 0;
+  PDCS_CUDA(cudaGetDevice(&dev));
+  PDCS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (exp) {
+    fused_prepare<T, NV, Op, true>(F);
+    PDCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fused_tile_kernel<T, NV, Op, true>, kFusedThreads, smem));
+  } else {
+    fused_prepare<T, NV, Op, false>(F);
+    PDCS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fused_tile_kernel<T, NV, Op, false>, kFusedThreads, smem));
+  }
+  if (per <= 0) return 0;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(F.ntiles, (int64_t)sms * per));
+}
+
 // Device buffers of the active work lists, sized for every instance iterating.
 void BatchSolver::setup_act_lists() {
   auto nchunks = [](int64_t len) { return (len + kThreads - 1) / kThreads; };
@@ -1108,6 +1435,21 @@ void BatchSolver::build_act_lists(const std::vector<Inst*>& its) {
   int32_t* hi = stage<int32_t>(std::max<size_t>(its.size(), 1));
   for (size_t i = 0; i < its.size(); ++i) hi[i] = (int32_t)its[i]->k;
   PDCS_CUDA(cudaMemcpyAsync(act_inst_, hi, sizeof(int32_t) * its.size(), cudaMemcpyHostToDevice, s_));
+  if (fused_)
+    for (int w = 0; w < 2; ++w) {  // the iterating instances' fused tiles, largest first
+      const Fused& f = fu_[w];
+      size_t cnt = 0;
+      for (Inst* I : its) cnt += (size_t)(f.first[I->k + 1] - f.first[I->k]);
+      int32_t* ht = stage<int32_t>(std::max<size_t>(cnt, 1));
+      int64_t* hnt = stage<int64_t>(1);
+      size_t j = 0;
+      for (Inst* I : its)
+        for (int64_t q = f.first[I->k]; q < f.first[I->k + 1]; ++q) ht[j++] = (int32_t)q;
+      std::stable_sort(ht, ht + cnt, [&](int32_t a, int32_t b) { return f.nnz[a] > f.nnz[b]; });
+      hnt[0] = (int64_t)cnt;
+      PDCS_CUDA(cudaMemcpyAsync(const_cast<int32_t*>(f.F.act), ht, sizeof(int32_t) * cnt, cudaMemcpyHostToDevice, s_));
+      PDCS_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(f.F.n_act), hnt, sizeof(int64_t), cudaMemcpyHostToDevice, s_));
+    }
   if (tiled_)
     for (int w = 0; w < 2; ++w) {  // the iterating instances' tiles, largest first
       const Tiles& t = tl_[w];
@@ -1182,7 +1524,29 @@ void BatchSolver::capture_batch_graph(int tail) {
     BatchCtl ctl{sts_, ps_,   ds_,     live_,      rx_,  ry_,         dxsq_,    dysq_,
                  dgdy_, cur,  nxt,     done_ctas_, live_cnt_ + 2, act_inst_, n_act_};
     mark(0);
-    if (fp32_) {
+    if (fused_ && !tail) {
+      // two fused tile kernels: G' rows (primal step), then G rows (dual step)
+      ctl.tpx = fu_[1].tpart;
+      ctl.tpy = fu_[0].tpart;
+      ctl.tfx = fu_[1].first_dev;
+      ctl.tfy = fu_[0].first_dev;
+      if (fp32_) {
+        launch_fused<float, 1>(fu_[1].F, fu_[1].grid, fu_[1].sv32, dyl32_, nullptr,
+                               FusedPrimal32{xa_, dxp32_, qa_, ps_, live_}, XIg_, fu_[1].tpart, cur, s_);
+        mark(1);
+        mark(2);
+        launch_fused<float, kPair>(fu_[0].F, fu_[0].grid, fu_[0].sv32, &dxp32_->x, nullptr,
+                                   FusedDual32{ya_, dyl32_, ra_, dy32_, ds_, live_}, YIg_, fu_[0].tpart, cur, s_);
+      } else {
+        launch_fused<double, 1>(fu_[1].F, fu_[1].grid, fu_[1].sv64, yl, nullptr,
+                                FusedPrimal64{xl, c_s, x, ps_, live_}, XIg_, fu_[1].tpart, cur, s_);
+        mark(1);
+        mark(2);
+        launch_fused<double, 2>(fu_[0].F, fu_[0].grid, fu_[0].sv64, x, xl,
+                                FusedDual64{yl, h_s, y, ds_, live_}, YIg_, fu_[0].tpart, cur, s_);
+      }
+      mark(3);
+    } else if (fp32_) {
       if (tiled_ && !tail) launch_spmv_tile<float, 1>(tl_[1].T, tgrid[1], Gt32_.v, dyl32_, nullptr, aty32_, nullptr, cur, s_);
       else launch_spmv<1, false, float>(Gt32, dyl32_, nullptr, aty32_, nullptr, cur, s_);
       mark(1);
@@ -2043,6 +2407,8 @@ int BatchSolver::prepare() {
   phase("compaction, tiles");
   setup_act_lists();
   phase("active lists");
+  setup_fused();
+  phase("fused tiles");
   // the merged matrix lives on the device now (its row pointers stay for the adjoint's scatter)
   std::vector<int64_t>().swap(h_src_);
   if (!O.differentiable) std::vector<int32_t>().swap(h_rp_);

@@ -236,12 +236,27 @@ struct BatchCtl {
   int32_t* live_accum;
   const int32_t* act_inst;  // instances iterating this round (NULL: all K)
   const int64_t* n_act;
+  // fused tile kernels: per-tile partial sums instead of per-element
+  // contributions (tpx: |dx|^2 per G' tile; tpy: |dy|^2, dy'(G dx - G dxl) per
+  // G tile) and every instance's tile ranges (K + 1 each); NULL: contributions
+  const double* tpx = nullptr;
+  const double* tpy = nullptr;
+  const int64_t* tfx = nullptr;
+  const int64_t* tfy = nullptr;
 };
 
 // Per-instance sums of the attempt's contributions (a: |dx|^2, b: |dy|^2,
 // d: dy'(G dx - G dxl)) over the instance's runs, by G lanes (lane gl of G)
 template <int G>
 __device__ __forceinline__ void control_sums(const BatchCtl& c, int64_t k, int gl, double& a, double& b, double& d) {
+  if (c.tpx) {  // the instance's tiles, in tile order
+    for (int64_t t = c.tfx[k] + gl; t < c.tfx[k + 1]; t += G) a += c.tpx[t];
+    for (int64_t t = c.tfy[k] + gl; t < c.tfy[k + 1]; t += G) {
+      b += c.tpy[2 * t];
+      d += c.tpy[2 * t + 1];
+    }
+    return;
+  }
   for (int q = 0; q < kMaxRuns; ++q) {
     const int64_t s0 = c.rx.start[k * kMaxRuns + q], L = c.rx.len[k * kMaxRuns + q];
     for (int64_t i = s0 + gl; i < s0 + L; i += G) a += c.dxsq[i];

@@ -1,0 +1,376 @@
+// pdcs_fused.cuh -- fused tile kernels of the batched iteration graph.
+//
+// One PDHG attempt of the batch is two matrix passes.  A tile is a range of
+// one instance's rows (its own row order across the type runs) cut only at
+// cone boundaries, so every cone of the tile's rows lies inside the tile.  Its
+// CTA
+//   1. stages the instance's column segment in shared memory (y_lag for G',
+//      the (x, x_lag) pairs for G),
+//   2. runs the tile's rows in SELL-32 layout: the rows sorted by length and
+//      cut into slices of 32, each slice stored column-major and padded to
+//      its longest row, so a warp streams a slice with one coalesced load per
+//      column (lane = row) and every gather is a shared-memory read; the
+//      products land in shared memory,
+//   3. finishes the primal (G') or dual (G) step of those rows: the update,
+//      the projection onto the instance's cones (elementwise rows a thread
+//      each, SOC / RSOC blocks of at most 32 elements in lane groups,
+//      exponential cones a thread each) and the tile's partial sums of the
+//      control step's reductions, written once per tile.
+// The products never reach HBM and no per-element contribution is stored:
+// the control kernel sums an instance's tile partials in tile order.
+// (rpdhg_alg_gpu_gen_scaling.jl:680-714: the two SpMVs, primal_update,
+// dual_update, the projections and the norms of one adaptive-step attempt.)
+#pragma once
+#include "pdcs_tiles.cuh"
+
+namespace pdcs {
+
+constexpr int kFusedThreads = 256;
+constexpr int kFusedWarps = kFusedThreads / 32;
+// resident CTAs per SM the register budget is sized for: 4 (64 registers) for
+// SOC / RSOC tables, 2 (128) when the exponential-cone root solve is compiled in
+constexpr int kFusedMinCtas = 4, kFusedMinCtasExp = 2;
+constexpr int kSellC = 32;  // rows per slice
+
+struct FusedTile {
+  int32_t inst;    // instance
+  int32_t o0, o1;  // instance-local row ordinals [o0, o1)
+  int32_t ew;      // the first ew rows are elementwise (box / zero / nonneg)
+  int32_t s0, s1;  // slices
+  int32_t t0, t1;  // cone tasks
+  int32_t x0, x1;  // exponential-cone records
+  int32_t pad0, pad1;
+};
+
+struct FusedCsr {
+  const FusedTile* tiles;
+  int64_t ntiles;
+  const int32_t* act;     // tiles of the iterating instances (NULL: every tile)
+  const int64_t* n_act;
+  const int64_t* sb;      // slice base (element offset of the slice's first column)
+  const int32_t* sl;      // slice length (its longest row)
+  const int16_t* so;      // per slice lane: tile-local row (-1: padding lane)
+  const uint16_t* sc;     // SELL column (instance-local) of every stored element
+  const int4* task;       // cone tasks {first record, records, lanes per group, 0}
+  const int4* crec;       // cone records {merged start, length | RSOC << 30, cone, tile-local offset}
+  const int4* xrec;       // exponential records {merged start, exp ordinal, tile-local offset, 0}
+  RunTable rows, cols;    // row-side / column-side runs of every instance
+  const int32_t* rloc;    // K * kMaxRuns: instance-local first row of each row run
+  const int32_t* cloc;    // K * kMaxRuns: instance-local first column of each column run
+  int32_t max_cols;       // staged elements (largest instance's column count)
+  int32_t max_rows;       // largest tile's rows (products in shared memory)
+};
+
+// ---- fused ops: z(j, a, b) is the value before the projection given the
+// row's products (a, b: G'y for the primal step; G x, G x_lag for the dual
+// one); fin(j, p, a, b, acc) stores the projection's result and adds the
+// control step's terms.
+
+// FP32 bulk, primal: z = xa + dx_lag + tau_k (qa + G' dy_lag), dx = P(z) - xa;
+// acc0 += (dx - dx_lag)^2
+struct FusedPrimal32 {
+  static constexpr int NACC = 1;
+  const double* xa;
+  float2* dxp;  // {dx, dx_lag}
+  const double* qa;
+  const double* ps;
+  const uint8_t* mask;
+  double sk = 0.0;
+  __device__ void begin(int64_t k) { sk = ps[k]; }
+  __device__ double z(int64_t j, float a, float) const { return xa[j] + (double)dxp[j].y + sk * (qa[j] + (double)a); }
+  __device__ void fin(int64_t j, double p, float, float, double* acc) const {
+    const float d = (float)(p - xa[j]);
+    dxp[j].x = d;
+    const double s = (double)d - (double)dxp[j].y;
+    acc[0] += s * s;
+  }
+};
+
+// FP32 bulk, dual: z = ya + dy_lag - sigma_k (ra + 2 G dx - G dx_lag), dy = P(z) - ya;
+// acc0 += (dy - dy_lag)^2, acc1 += (dy - dy_lag)(G dx - G dx_lag)
+struct FusedDual32 {
+  static constexpr int NACC = 2;
+  const double* ya;
+  const float* dyl;
+  const double* ra;
+  float* dy;
+  const double* ds;
+  const uint8_t* mask;
+  double sk = 0.0;
+  __device__ void begin(int64_t k) { sk = ds[k]; }
+  __device__ double z(int64_t i, float g, float gl) const {
+    return ya[i] + (double)dyl[i] - sk * (ra[i] + (2.0 * (double)g - (double)gl));
+  }
+  __device__ void fin(int64_t i, double p, float g, float gl, double* acc) const {
+    const float d = (float)(p - ya[i]);
+    dy[i] = d;
+    const double s = (double)d - (double)dyl[i];
+    acc[0] += s * s;
+    acc[1] += s * ((double)g - (double)gl);
+  }
+};
+
+// FP64, primal: x = P(x_lag + tau_k (G'y_lag - c)); acc0 += (x - x_lag)^2
+struct FusedPrimal64 {
+  static constexpr int NACC = 1;
+  const double* xl;
+  const double* c;
+  double* out;
+  const double* ps;
+  const uint8_t* mask;
+  double sk = 0.0;
+  __device__ void begin(int64_t k) { sk = ps[k]; }
+  __device__ double z(int64_t j, double a, double) const { return xl[j] + sk * (a - c[j]); }
+  __device__ void fin(int64_t j, double p, double, double, double* acc) const {
+    out[j] = p;
+    const double d = p - xl[j];
+    acc[0] += d * d;
+  }
+};
+
+// FP64, dual: y = P(y_lag - sigma_k (2 G x - G x_lag - h)); acc0 += (y - y_lag)^2,
+// acc1 += (y - y_lag)(G x - G x_lag)
+struct FusedDual64 {
+  static constexpr int NACC = 2;
+  const double* yl;
+  const double* h;
+  double* out;
+  const double* ds;
+  const uint8_t* mask;
+  double sk = 0.0;
+  __device__ void begin(int64_t k) { sk = ds[k]; }
+  __device__ double z(int64_t i, double g, double gl) const { return yl[i] - sk * ((2.0 * g - gl) - h[i]); }
+  __device__ void fin(int64_t i, double p, double g, double gl, double* acc) const {
+    out[i] = p;
+    const double d = p - yl[i];
+    acc[0] += d * d;
+    acc[1] += d * (g - gl);
+  }
+};
+
+// The fused tile kernel.  T: matrix / product type; NV: 1 (G' y) or kPair /
+// 2 (G applied to two vectors); EXP: compile the exponential-cone path.
+// Dynamic shared memory: A.max_cols staged values, then the tile's products
+// (1 or 2 per row, type T).
+template <class T, int NV, class Op, bool EXP>
+__global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFusedMinCtas)
+    fused_tile_kernel(FusedCsr A, const T* __restrict__ sv, const T* x0, const T* x1, Op op, ConeTable CT,
+                      double* __restrict__ tpart, const int32_t* active) {
+  if (active && !*active) return;
+  using V = TileVal<T, NV>;
+  constexpr int NP = NV == 1 ? 1 : 2;
+  extern __shared__ __align__(16) unsigned char fused_smem[];
+  const size_t stage = (sizeof(V) * (size_t)A.max_cols + 15) & ~size_t(15);
+  V* sx = reinterpret_cast<V*>(fused_smem);
+  T* pr0 = reinterpret_cast<T*>(fused_smem + stage);
+  T* pr1 = pr0 + A.max_rows;
+  __shared__ int64_t run_row[kMaxRuns];
+  __shared__ int32_t run_ord[kMaxRuns];
+  __shared__ double red[Op::NACC][kFusedWarps];
+  const int64_t nt = A.act ? *A.n_act : A.ntiles;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double r2 = 0.7071067811865476;
+  for (int64_t q = blockIdx.x; q < nt; q += gridDim.x) {
+    const int64_t tid = A.act ? (int64_t)A.act[q] : q;
+    const FusedTile tl = A.tiles[tid];
+    const int64_t k = tl.inst;
+    if (!op.mask[k]) continue;  // CTA-uniform: the instance does not iterate
+    if (threadIdx.x < kMaxRuns) {
+      run_row[threadIdx.x] = A.rows.start[k * kMaxRuns + threadIdx.x];
+      run_ord[threadIdx.x] = A.rloc[k * kMaxRuns + threadIdx.x];
+    }
+    for (int r = 0; r < kMaxRuns; ++r) {
+      const int64_t s0 = A.cols.start[k * kMaxRuns + r], L = A.cols.len[k * kMaxRuns + r];
+      V* dst = sx + A.cloc[k * kMaxRuns + r];
+      for (int64_t i = threadIdx.x; i < L; i += kFusedThreads) dst[i] = tile_load<T, NV>(x0, x1, s0 + i);
+    }
+    __syncthreads();
+    // ---- the tile's rows, SELL-32: lane = row, one coalesced load per column ----
+    for (int64_t s = tl.s0 + warp; s < tl.s1; s += kFusedWarps) {
+      const int64_t base = A.sb[s] + lane;
+      const int32_t len = A.sl[s];
+      const int32_t slot = A.so[s * kSellC + lane];
+      T p0 = T(0), p1 = T(0);
+      constexpr int U = sizeof(T) == 4 ? 8 : 4;
+      for (int32_t j0 = 0; j0 < len; j0 += U) {
+        T v[U];
+        uint16_t c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {  // every load of the chunk in flight together
+          const bool ok = j0 + u < len;
+          v[u] = ok ? sv[base + (int64_t)(j0 + u) * kSellC] : T(0);
+          c[u] = ok ? A.sc[base + (int64_t)(j0 + u) * kSellC] : (uint16_t)0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const V xv = sx[c[u]];
+          if constexpr (NV == 1) {
+            p0 = fma(v[u], xv, p0);
+          } else {
+            p0 = fma(v[u], xv.x, p0);
+            p1 = fma(v[u], xv.y, p1);
+          }
+        }
+      }
+      if (slot >= 0) {
+        pr0[slot] = p0;
+        if (NP == 2) pr1[slot] = p1;
+      }
+    }
+    __syncthreads();
+    // ---- the step of the tile's rows ----
+    op.begin(k);
+    double acc[Op::NACC];
+#pragma unroll
+    for (int a = 0; a < Op::NACC; ++a) acc[a] = 0.0;
+    auto merged = [&](int64_t o) {  // instance-local ordinal -> merged index
+      int r = 0;
+      for (int t = 1; t < kMaxRuns; ++t)
+        if (o >= run_ord[t]) r = t;
+      return run_row[r] + (o - run_ord[r]);
+    };
+    for (int i = threadIdx.x; i < tl.ew; i += kFusedThreads) {  // elementwise rows
+      const int64_t j = merged(tl.o0 + i);
+      int32_t kind = CT.seg_kind[0];
+      for (int s = 1; s < CT.nseg; ++s)
+        if (j >= CT.seg_start[s]) kind = CT.seg_kind[s];
+      const T a = pr0[i], b = NP == 2 ? pr1[i] : T(0);
+      const double p = elem_proj(kind, op.z(j, a, b), j, CT);
+      op.fin(j, p, a, b, acc);
+    }
+    for (int64_t t = tl.t0 + warp; t < tl.t1; t += kFusedWarps) {  // SOC / RSOC blocks, lane groups
+      const int4 tk = A.task[t];
+      const int g = tk.z, gl = lane & (g - 1);
+      const bool have = lane / g < tk.y;
+      int4 rc = make_int4(0, 0, 0, 0);
+      if (have) rc = A.crec[tk.x + lane / g];
+      const int64_t st = rc.x;
+      const int d = have ? (rc.y & 0x3fffffff) : 0;
+      const bool rsoc = have && (rc.y >> 30) != 0;
+      const int li = rc.w + gl;
+      const T a = gl < d ? pr0[li] : T(0), b = (gl < d && NP == 2) ? pr1[li] : T(0);
+      double v = gl < d ? op.z(st + gl, a, b) : 0.0;
+      double w = 1.0;
+      if (CT.S && gl < d) {
+        const double* S = CT.S + st;
+        if (rsoc) w = (gl >= 2) ? sqrt(S[0] * S[1]) / S[gl] : 1.0;
+        else w = (gl >= 1) ? S[0] / S[gl] : 1.0;
+      }
+      const bool weighted = grp_max(w != 1.0 ? 1.0 : 0.0, g) != 0.0;
+      {  // RSOC: rotate the first two elements to the SOC form (every lane shuffles)
+        const double p0 = __shfl_sync(kFull, v, 0, g), q0 = __shfl_sync(kFull, v, 1, g);
+        if (rsoc && gl == 0) v = (p0 + q0) * r2;
+        if (rsoc && gl == 1) v = (p0 - q0) * r2;
+      }
+      group_soc_reg(v, w, d, weighted, g, (have && CT.soc_ws) ? CT.soc_ws + rc.z : nullptr);
+      {
+        const double a0 = __shfl_sync(kFull, v, 0, g), b0 = __shfl_sync(kFull, v, 1, g);
+        if (rsoc && gl == 0) v = (a0 + b0) * r2;
+        if (rsoc && gl == 1) v = (a0 - b0) * r2;
+      }
+      if (gl < d) op.fin(st + gl, v, a, b, acc);
+    }
+    if constexpr (EXP) {
+      for (int64_t e = tl.x0 + threadIdx.x; e < tl.x1; e += kFusedThreads) {  // exponential cones
+        const int4 xr = A.xrec[e];
+        const int64_t j = xr.x, kk = xr.y;
+        const int li = xr.z;
+        const bool first = kk < CT.exp_count;
+        const int32_t kind = first ? CT.exp_kind : CT.dexp_kind;
+        T pa[3], pb[3];
+        double zz[3];
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+          pa[u] = pr0[li + u];
+          pb[u] = NP == 2 ? pr1[li + u] : T(0);
+          zz[u] = op.z(j + u, pa[u], pb[u]);
+        }
+        double S0 = 1.0, S1 = 1.0, S2 = 1.0;
+        if (CT.S) {
+          S0 = CT.S[j];
+          S1 = CT.S[j + 1];
+          S2 = CT.S[j + 2];
+        }
+        double* ws = CT.rho_ws ? CT.rho_ws + kk : nullptr;
+        if (kind == PK_EXP) proj_exp_scaled_dev(zz[0], zz[1], zz[2], S0, S1, S2, ws);
+        else proj_dexp_scaled_dev(zz[0], zz[1], zz[2], S0, S1, S2, ws);
+#pragma unroll
+        for (int u = 0; u < 3; ++u) op.fin(j + u, zz[u], pa[u], pb[u], acc);
+      }
+    }
+    // ---- the tile's partial sums, in a fixed order ----
+#pragma unroll
+    for (int a = 0; a < Op::NACC; ++a) {
+      double v = acc[a];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+      if (lane == 0) red[a][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < Op::NACC) {
+      double v = red[threadIdx.x][0];
+      for (int w = 1; w < kFusedWarps; ++w) v += red[threadIdx.x][w];
+      tpart[tid * Op::NACC + threadIdx.x] = v;
+    }
+    __syncthreads();  // the next tile restages sx, the products and the run tables
+  }
+}
+
+// Builds the SELL arrays on the device: slice s, lane l holds merged row
+// srow[s * 32 + l] (-1: padding); its nonzeros go to sv / sc[sb[s] + j * 32 + l]
+// for j < the row's length, zeros (column 0) to the slice's length.
+template <class T>
+__global__ void sell_fill_kernel(int64_t nslices, const int64_t* __restrict__ sb, const int32_t* __restrict__ sl,
+                                 const int32_t* __restrict__ srow, const int32_t* __restrict__ rp,
+                                 const T* __restrict__ vals, const uint16_t* __restrict__ cl, T* __restrict__ sv,
+                                 uint16_t* __restrict__ sc) {
+  const int64_t total = nslices * kSellC;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
+    const int64_t s = q / kSellC;
+    const int l = (int)(q % kSellC);
+    const int32_t r = srow[q];
+    const int64_t b = sb[s] + l;
+    const int32_t L = sl[s];
+    const int32_t e0 = r >= 0 ? rp[r] : 0, n = r >= 0 ? rp[r + 1] - rp[r] : 0;
+    for (int32_t j = 0; j < L; ++j) {
+      const bool ok = j < n;
+      sv[b + (int64_t)j * kSellC] = ok ? vals[e0 + j] : T(0);
+      sc[b + (int64_t)j * kSellC] = ok ? cl[e0 + j] : (uint16_t)0;
+    }
+  }
+}
+
+template <class T, int NV>
+inline size_t fused_smem_bytes(const FusedCsr& A) {
+  const size_t stage = (sizeof(TileVal<T, NV>) * (size_t)std::max(A.max_cols, 1) + 15) & ~size_t(15);
+  return stage + sizeof(T) * (NV == 1 ? 1 : 2) * (size_t)std::max(A.max_rows, 1);
+}
+
+// Raise the kernel's dynamic shared memory limit to what A needs (per device,
+// only ever growing: graphs captured with larger tiles stay launchable).
+template <class T, int NV, class Op, bool EXP>
+inline void fused_prepare(const FusedCsr& A) {
+  static std::mutex mu;
+  static std::map<int, size_t> set;
+  int dev = 0;
+  PDCS_CUDA(cudaGetDevice(&dev));
+  const size_t need = fused_smem_bytes<T, NV>(A);
+  std::lock_guard<std::mutex> lock(mu);
+  if (need <= set[dev]) return;
+  PDCS_CUDA(cudaFuncSetAttribute(fused_tile_kernel<T, NV, Op, EXP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)need));
+  set[dev] = need;
+}
+
+template <class T, int NV, class Op>
+inline void launch_fused(const FusedCsr& A, int grid, const T* sv, const std::type_identity_t<T>* x0,
+                         const std::type_identity_t<T>* x1, const Op& op, const ConeTable& CT, double* tpart,
+                         const int32_t* active, cudaStream_t s) {
+  const size_t smem = fused_smem_bytes<T, NV>(A);
+  if (CT.exp_count + CT.dexp_count > 0)
+    fused_tile_kernel<T, NV, Op, true><<<grid, kFusedThreads, smem, s>>>(A, sv, x0, x1, op, CT, tpart, active);
+  else
+    fused_tile_kernel<T, NV, Op, false><<<grid, kFusedThreads, smem, s>>>(A, sv, x0, x1, op, CT, tpart, active);
+}
+
+}  // namespace pdcs

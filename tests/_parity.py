@@ -19,7 +19,7 @@ def optimum(p):
     if key not in _cache:
         codes = []
         for tol in (1e-8, 1e-9, 1e-7):
-            o = B.solve(p, threads=0, rel_tol=tol, abs_tol=tol, time_limit=600)
+            o = B.solve(p, threads=1, rel_tol=tol, abs_tol=tol, time_limit=600)
             codes.append(o["exit_code"])
             if o["exit_code"] == 0:
                 break
