@@ -311,7 +311,24 @@ struct ConeTable {
                               // instance}, so a lane group reads one record (NULL: the wc_* tables)
   int64_t elem_total;        // sum of seg_len
   int32_t ctaA, ctaB, ctaC;  // CTAs for elementwise / warp cones / exp cones
+  // Huge SOC / RSOC blocks (kHugeBlock elements or more, at most kMaxHuge per
+  // table; none in the batched solver's tables): projected together by the
+  // first ctaD CTAs of the launch, which meet at bounded barriers (huge_bar)
+  // between the reductions of the Newton solve; they are not in sched.
+  int32_t ctaD;
+  int32_t nhuge;
+  int64_t huge_start[2];
+  int64_t huge_len[2];
+  int32_t huge_rsoc[2];
+  int64_t huge_wc[2];   // the block's warp-cone index (its soc_ws warm start)
+  unsigned* huge_bar;   // {arrivals, generation}
+  int32_t* huge_err;    // set when a CTA gave up waiting at a barrier
+  double* huge_red;     // 2 x ctaD x 4 partial sums (two alternating sets)
 };
+constexpr int kMaxHuge = 2;
+constexpr int64_t kHugeBlock = 16384;  // blocks of at least this many elements take part D
+constexpr int kHugeMaxCtas = 148;
+inline int table_grid(const ConeTable& T) { return T.ctaA + T.ctaB + T.ctaC + T.ctaD; }
 
 __device__ __forceinline__ double elem_proj(int32_t kind, double z, int64_t j, const ConeTable& T) {
   switch (kind) {
@@ -430,6 +447,206 @@ __device__ inline void control_block(PdhgState* st, const double* px, int nbx, c
   *st = s;
 }
 
+// Barrier of the CTAs [0, n) of a launch (part D).  Every CTA of the launch's
+// part D is resident: they have the lowest block indices, their number is at
+// most the SM count, and no other CTA of the launch waits.  The wait is still
+// bounded: a CTA that polls 2^24 times without the generation moving sets *err
+// and gives up (the solve then reports a CUDA error instead of hanging).
+__device__ inline bool huge_barrier(unsigned* bar, unsigned n, int32_t* err) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    __threadfence();
+    const unsigned gen = *((volatile unsigned*)(bar + 1));
+    if (atomicAdd(bar, 1u) == n - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long it = 0;
+      while (*((volatile unsigned*)(bar + 1)) == gen) {
+        if (++it > (1ll << 24) || *((volatile int32_t*)err)) {
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Block-wide sums / maxima of NR values (every thread receives the results).
+template <int NR>
+__device__ inline void block_reduce_n(double (&v)[NR], const bool (&is_max)[NR]) {
+  __shared__ double sh[NR][kWarps];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    double x = v[r];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_xor_sync(kFull, x, o);
+      x = is_max[r] ? fmax(x, y) : x + y;
+    }
+    if ((threadIdx.x & 31) == 0) sh[r][threadIdx.x >> 5] = x;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    double x = sh[r][0];
+    for (int w = 1; w < kWarps; ++w) x = is_max[r] ? fmax(x, sh[r][w]) : x + sh[r][w];
+    v[r] = x;
+  }
+  __syncthreads();
+}
+
+// One reduction round of part D: this CTA's NR values go to its slot of the
+// round's buffer, then every CTA sums (or maximises) all slots in CTA order,
+// so all CTAs hold bit-identical results.  Returns false if a wait gave up.
+template <int NR>
+__device__ inline bool huge_allreduce(const ConeTable& T, int cta, int& round, double (&v)[NR],
+                                      const bool (&is_max)[NR]) {
+  block_reduce_n<NR>(v, is_max);
+  double* buf = T.huge_red + (size_t)(round & 1) * T.ctaD * 4;
+  if (threadIdx.x < NR) buf[cta * 4 + threadIdx.x] = v[threadIdx.x];
+  round++;
+  if (!huge_barrier(T.huge_bar, (unsigned)T.ctaD, T.huge_err)) return false;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    double x = __ldcg(buf + r);
+    for (int c = 1; c < T.ctaD; ++c) x = is_max[r] ? fmax(x, __ldcg(buf + c * 4 + r)) : x + __ldcg(buf + c * 4 + r);
+    v[r] = x;
+  }
+  return true;
+}
+
+// Projection of huge block h of T (SOC, or RSOC through the rotation onto a
+// weighted SOC) by the ctaD CTAs of part D together: CTA `cta` owns a
+// contiguous slice of the block (elements 0 and 1 in CTA 0), the block's values
+// go through op.out, and every reduction of the scalar solve (scale, the two
+// norms, each Newton step's S1, S2) is a round of huge_allreduce.  The Newton
+// iteration is the one of group_soc_reg / warp_soc_mem, warm-started from the
+// block's previous root; its results, and so the control flow, are identical
+// in every CTA.  Each element is then finished with op.fin.
+template <class Op, int NACC>
+__device__ void huge_block_proj(const Op& op, const ConeTable& T, int h, int cta, int& round, double (&acc)[NACC]) {
+  const int64_t st = T.huge_start[h], d = T.huge_len[h];
+  const bool rsoc = T.huge_rsoc[h] != 0;
+  const int64_t chunk = (d + T.ctaD - 1) / T.ctaD;
+  const int64_t lo = (int64_t)cta * chunk, hi = lo + chunk < d ? lo + chunk : d;
+  double* u = op.out + st;
+  const double* S = T.S ? T.S + st : nullptr;
+  const double gw = S ? (rsoc ? sqrt(S[0] * S[1]) : S[0]) : 1.0;
+  auto wt = [&](int64_t i) { return (!S || (rsoc && i == 1)) ? 1.0 : gw / S[i]; };
+  const double r2 = 0.7071067811865476;
+  // values in SOC form (RSOC: rotate the first two), local max |u| and weight flag
+  double mx[2] = {0.0, 0.0};
+  for (int64_t i = lo + threadIdx.x; i < hi; i += kThreads) {
+    double v = op.z(st + i);
+    if (rsoc && i < 2) {
+      const double z0 = op.z(st), z1 = op.z(st + 1);
+      v = (i == 0) ? (z0 + z1) * r2 : (z0 - z1) * r2;
+    }
+    u[i] = v;
+    mx[0] = fmax(mx[0], fabs(v));
+    if (i >= 1 && wt(i) != 1.0) mx[1] = 1.0;
+  }
+  const bool kmax2[2] = {true, true};
+  if (!huge_allreduce<2>(T, cta, round, mx, kmax2)) return;
+  const double scale = mx[0];
+  const bool weighted = mx[1] != 0.0;
+  const bool trivial = scale == 0.0 || !isfinite(scale);
+  const double sc = trivial ? 1.0 : scale;
+  const double t = __ldcg(u) / sc;
+  double nr[2] = {0.0, 0.0};
+  for (int64_t i = (lo > 1 ? lo : 1) + threadIdx.x; i < hi; i += kThreads) {
+    const double D = wt(i), xi = __ldcg(u + i) / sc;
+    nr[0] += (D * xi) * (D * xi);
+    nr[1] += (xi / D) * (xi / D);
+  }
+  const bool ksum2[2] = {false, false};
+  if (!huge_allreduce<2>(T, cta, round, nr, ksum2)) return;
+  const double nDx = sqrt(nr[0]), nxD = sqrt(nr[1]);
+  const bool inside = trivial || nDx <= t;
+  const bool polar = !inside && nxD <= -t;
+  // the result p_i = f(u_i): inside p = u, polar p = 0, else p_0 = s0, p_i = u_i * mul(i)
+  double s0 = 0.0, mu = 0.0, cc = 0.0;
+  int mode = inside ? 0 : (polar ? 1 : (weighted ? 3 : 2));
+  if (mode == 2) {
+    cc = 0.5 * (1.0 + t / nDx);
+    s0 = cc * nDx * sc;
+  } else if (mode == 3) {
+    if (t == 0.0) {
+      double a[1] = {0.0};
+      for (int64_t i = (lo > 1 ? lo : 1) + threadIdx.x; i < hi; i += kThreads) {
+        const double D = wt(i), y0 = (__ldcg(u + i) / sc) / (1.0 + D * D);
+        a[0] += (D * y0) * (D * y0);
+      }
+      const bool ks1[1] = {false};
+      if (!huge_allreduce<1>(T, cta, round, a, ks1)) return;
+      s0 = sqrt(a[0]) * sc;
+      mu = 1.0;
+    } else {
+      const double s_lo = fmax(t, 0.0);
+      double s = s_lo;
+      double* ws = T.soc_ws ? T.soc_ws + T.huge_wc[h] : nullptr;
+      const double sw = ws ? __ldcg(ws) / sc : __longlong_as_double(0x7ff8000000000000ll);
+      bool first = isfinite(sw) && sw > s_lo;
+      if (first) s = sw;
+      for (int it = 0; it < 200; ++it) {
+        double q[2] = {0.0, 0.0};
+        for (int64_t i = (lo > 1 ? lo : 1) + threadIdx.x; i < hi; i += kThreads) {
+          const double D = wt(i), xi = __ldcg(u + i) / sc;
+          const double c = D * D * xi * xi;
+          if (c == 0.0) continue;
+          const double a = 1.0 + D * D;
+          const double iu = 1.0 / (s * a - t * D * D);
+          q[0] += c * iu * iu;
+          q[1] += c * a * iu * iu * iu;
+        }
+        if (!huge_allreduce<2>(T, cta, round, q, ksum2)) return;
+        const double Q = 1.0 / sqrt(q[0]);
+        const double dQ = Q * Q * Q * q[1];
+        const double step = (1.0 - Q) / dQ;
+        if (first) {
+          first = false;
+          if (step < 0.0) {  // warm start above the root
+            s = fmax(s + step, s_lo);
+            continue;
+          }
+        }
+        if (!(step > 0.0)) break;
+        const double sn = s + step;
+        if (!(sn > s)) break;
+        s = sn;
+        if (step <= 1e-17 * s) break;
+      }
+      mu = 1.0 - t / s;
+      s0 = s * sc;
+      if (ws && cta == 0 && threadIdx.x == 0) *ws = s * sc;
+    }
+  }
+  auto pval = [&](int64_t i, double ui) {  // the SOC-form result of element i
+    if (mode == 0) return ui;
+    if (mode == 1) return 0.0;
+    if (i == 0) return s0;
+    if (mode == 2) return ui * cc;
+    const double D = wt(i);
+    return ui / (1.0 + mu * D * D);
+  };
+  for (int64_t i = lo + threadIdx.x; i < hi; i += kThreads) {
+    double p = pval(i, __ldcg(u + i));
+    if (rsoc && i < 2) {  // rotate back (both elements live in CTA 0's slice)
+      const double p0 = pval(0, __ldcg(u)), p1 = pval(1, __ldcg(u + 1));
+      p = (i == 0) ? (p0 + p1) * r2 : (p0 - p1) * r2;
+    }
+    op.fin(st + i, op.z(st + i), p, acc);
+  }
+}
+
 // Ops of the batched solver restrict work to the elements of selected
 // instances: live(j) is false for elements that must not be read or written.
 template <class Op>
@@ -448,9 +665,12 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
   double acc[Op::NACC];
 #pragma unroll
   for (int k = 0; k < Op::NACC; ++k) acc[k] = 0.0;
-  const int b = blockIdx.x;
+  const int b = (int)blockIdx.x - T.ctaD;  // part D (huge blocks) first: the lowest block indices
   const int nblocks = gridDim.x;
-  if (b < T.ctaA && T.act_chunk) {
+  if (b < 0) {
+    int round = 0;
+    for (int h = 0; h < T.nhuge; ++h) huge_block_proj<Op, Op::NACC>(op, T, h, (int)blockIdx.x, round, acc);
+  } else if (b < T.ctaA && T.act_chunk) {
     // chunks of the elementwise segments, a CTA per chunk
     const int64_t nch = T.act_meta[0];
     for (int64_t q = b; q < nch; q += T.ctaA) {
@@ -650,7 +870,7 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
 template <class Op>
 inline void launch_update_project(const Op& op, const ConeTable& T, double* partials, const int32_t* active,
                                   cudaStream_t s) {
-  const int grid = T.ctaA + T.ctaB + T.ctaC;
+  const int grid = table_grid(T);
   if (T.exp_count + T.dexp_count > 0) update_project_kernel<Op, true><<<grid, kThreads, 0, s>>>(op, T, partials, active);
   else update_project_kernel<Op, false><<<grid, kThreads, 0, s>>>(op, T, partials, active);
 }

@@ -400,6 +400,14 @@ struct Infea {
 
 class Solver {
  public:
+  // true when a part-D barrier of the last solve gave up (its projection is invalid)
+  bool huge_failed() {
+    if (!huge_err_) return false;
+    int32_t e = 0;
+    PDCS_CUDA(cudaMemcpyAsync(&e, huge_err_, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    return e != 0;
+  }
   Solver(const pdcs_problem* p, const pdcs_options* o) : P(*p), O(*o) {}
   virtual ~Solver() {
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
@@ -443,6 +451,12 @@ class Solver {
   PdhgState* st_dev = nullptr;
   PdhgState* host_state_ = nullptr;
   double* host_red_ = nullptr;
+  // part D of the update kernels (huge SOC / RSOC blocks): barrier state, the
+  // flag a CTA sets when it gave up waiting, partial sums
+  unsigned* huge_bar_ = nullptr;
+  int32_t* huge_err_ = nullptr;
+  double* huge_red_ = nullptr;
+
   ConeTable XI{}, YI{}, CON{}, SLK{};
   int grid_reflect_ = 1, grid_vec_n_ = 1, grid_vec_m_ = 1;
   cudaGraph_t graph_ = nullptr;
@@ -594,7 +608,7 @@ class Solver {
   template <class Op>
   int launch_project(const Op& op, const ConeTable& T, double* partials) {
     update_project(op, T, partials);
-    return T.ctaA + T.ctaB + T.ctaC;
+    return table_grid(T);
   }
 
   void push_state() {
@@ -798,7 +812,25 @@ void Solver::size_table(ConeTable& T) {
   T.ctaB = tasks > 0 ? cap((tasks + kWarps - 1) / kWarps) : 0;
   int64_t ne = T.exp_count + T.dexp_count;
   T.ctaC = ne > 0 ? cap((ne + kThreads - 1) / kThreads) : 0;
-  if (T.ctaA + T.ctaB + T.ctaC == 0) T.ctaA = 1;  // at least one CTA writes the partials
+  T.ctaD = 0;
+  if (T.nhuge > 0) {
+    int64_t dmin = T.huge_len[0];
+    for (int h = 1; h < T.nhuge; ++h) dmin = std::min(dmin, T.huge_len[h]);
+    // about 4096 elements per CTA, at most one CTA per SM (every CTA of part D resident),
+    // at least 2 elements per CTA (elements 0 and 1 of a block in CTA 0)
+    T.ctaD = (int32_t)std::max<int64_t>(1, std::min<int64_t>({(dmin + 4095) / 4096, dmin / 2, (int64_t)kHugeMaxCtas}));
+    if (!huge_bar_) {
+      huge_bar_ = A.alloc<unsigned>(4);
+      huge_err_ = A.alloc<int32_t>(4);
+      huge_red_ = A.alloc<double>(2 * 4 * kHugeMaxCtas);
+      PDCS_CUDA(cudaMemsetAsync(huge_bar_, 0, 4 * sizeof(unsigned), s_));
+      PDCS_CUDA(cudaMemsetAsync(huge_err_, 0, 4 * sizeof(int32_t), s_));
+    }
+    T.huge_bar = huge_bar_;
+    T.huge_err = huge_err_;
+    T.huge_red = huge_red_;
+  }
+  if (table_grid(T) == 0) T.ctaA = 1;  // at least one CTA writes the partials
 }
 
 void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<int64_t>& rsoc_x,
@@ -814,7 +846,16 @@ void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<i
     for (int64_t d : soc) { stv.push_back(s); lv.push_back((int32_t)d); kv.push_back(PK_SOC); s += d; }
     for (int64_t d : rsoc) { stv.push_back(s); lv.push_back((int32_t)d); kv.push_back(PK_RSOC); s += d; }
     std::vector<std::vector<int64_t>> cls(kCls);
+    T.nhuge = 0;
     for (size_t k = 0; k < lv.size(); ++k) {
+      if (lv[k] >= kHugeBlock && T.nhuge < kMaxHuge) {  // part D: the launch's first CTAs together
+        T.huge_start[T.nhuge] = stv[k];
+        T.huge_len[T.nhuge] = lv[k];
+        T.huge_rsoc[T.nhuge] = kv[k] == PK_RSOC ? 1 : 0;
+        T.huge_wc[T.nhuge] = (int64_t)k;
+        T.nhuge++;
+        continue;
+      }
       int c = 0;
       while (c < kCls - 1 && lv[k] > (2 << c)) ++c;
       cls[c].push_back((int64_t)k);
@@ -833,7 +874,7 @@ void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<i
     int64_t* d_start = A.alloc<int64_t>(stv.size());
     int32_t* d_len = A.alloc<int32_t>(lv.size());
     int8_t* d_kind = A.alloc<int8_t>(kv.size());
-    int64_t* d_sched = A.alloc<int64_t>(sched.size());
+    int64_t* d_sched = A.alloc<int64_t>(std::max<size_t>(sched.size(), 1));
     if (!stv.empty()) {
       PDCS_CUDA(cudaMemcpyAsync(d_start, stv.data(), stv.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s_));
       PDCS_CUDA(cudaMemcpyAsync(d_len, lv.data(), lv.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s_));
@@ -1106,8 +1147,7 @@ void Solver::setup() {
   std::vector<int64_t> socG(P.socG, P.socG + P.n_socG), rsocG(P.rsocG, P.rsocG + P.n_rsocG);
   phase("SpMV schedules");
   build_tables(soc_x, rsoc_x, socG, rsocG);
-  int maxgrid = std::max({XI.ctaA + XI.ctaB + XI.ctaC, YI.ctaA + YI.ctaB + YI.ctaC, SLK.ctaA + SLK.ctaB + SLK.ctaC,
-                          CON.ctaA + CON.ctaB + CON.ctaC, 148 * 8});
+  int maxgrid = std::max({table_grid(XI), table_grid(YI), table_grid(SLK), table_grid(CON), 148 * 8});
   part_x = A.alloc<double>((size_t)maxgrid * 8);
   part_y = A.alloc<double>((size_t)maxgrid * 8);
   part_r = A.alloc<double>((size_t)maxgrid * 8);
@@ -1192,7 +1232,7 @@ void Solver::capture_graph() {
     OpPrimalStep32 op1{xa_, dxp32_, qa_, aty32_, x, st_dev, 0.0};
     launch_update_project(op1, XI, part_x, act, s_);
     launch_spmv<kPair, false, float>(G32_, &dxp32_->x, nullptr, gx32_, gxl32_, act, s_);
-    OpDualStep32 op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, st_dev, 0.0, part_x, XI.ctaA + XI.ctaB + XI.ctaC};
+    OpDualStep32 op2{ya_, dyl32_, ra_, gx32_, gxl32_, dy32_, y, st_dev, 0.0, part_x, table_grid(XI)};
     launch_update_project(op2, YI, part_y, act, s_);
     reflect32_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, dxp32_, dxm_, n_, dy32_, dyl32_, dym_, m_);
   }
@@ -1202,7 +1242,7 @@ void Solver::capture_graph() {
     launch_update_project(op1, XI, part_x, act, s_);
     launch_spmv<2>(G_, x, xl, gx, gxl, act, s_);
     // the dual step's last CTA runs the attempt's control step
-    OpDualStep op2{yl, gx, gxl, h_s, y, st_dev, 0.0, part_x, XI.ctaA + XI.ctaB + XI.ctaC};
+    OpDualStep op2{yl, gx, gxl, h_s, y, st_dev, 0.0, part_x, table_grid(XI)};
     launch_update_project(op2, YI, part_y, act, s_);
     reflect_kernel<<<grid_reflect_, kThreads, 0, s_>>>(st_dev, x, xl, xm, n_, y, yl, ym, m_);
   }
@@ -1934,7 +1974,12 @@ int pdcs_solve(const pdcs_problem* prob, const pdcs_options* opts, pdcs_result* 
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return PDCS_ERR_NO_DEVICE;
   try {
     pdcs::Solver s(prob, &o);
-    return s.run(res);
+    const int rc = s.run(res);
+    if (s.huge_failed()) {
+      std::fprintf(stderr, "pdcs_solve: a cooperative projection of a huge cone timed out at a barrier\n");
+      return PDCS_ERR_CUDA;
+    }
+    return rc;
   } catch (const pdcs::CudaError& e) {
     std::fprintf(stderr, "pdcs_solve: %s\n", e.what());
     return PDCS_ERR_CUDA;

@@ -276,3 +276,59 @@ def dual_infeasible_lp():
     return ConicProblem(n=2, m=2, nb=2, c=np.array([-1.0, 0.0]), G=G, h=np.zeros(2),
                         mGzero=0, mGnonnegative=2, bl=np.full(2, -np.inf), bu=np.full(2, np.inf),
                         name="dual_infeasible_lp")
+
+
+def portfolio_c2(n=1_000_000, factors=200, group=10, load_density=0.25, seed=20261205, gamma=1.0):
+    """Robust portfolio with quadratic risk through a rotated second-order cone.
+
+    Variables: the weights x (n, in [0, 1]) and the risk t >= 0 (nb = n + 1, all boxed).
+        min  -mu'x + gamma t
+        s.t. sum(x) = 1                                   (zero cone, 1 row)
+             || x_g - w_g || <= r_g  for every group g    (n / group SOC blocks of dim group + 1)
+             2 t (1/2) >= ||F'x||^2 + ||D x||^2          (one RSOC block of dim 2 + factors + n)
+    F: factor loadings, each asset loading on a factor with probability
+    load_density, values N(0, 0.1^2) (n = 1e6, 200 factors: about 5e7 nonzeros);
+    D: idiosyncratic volatilities U(0.01, 0.1); mu ~ N(0.05, 0.02^2); w = 1/n
+    (the benchmark, equal weights), r_g = 10 / n.  The equal-weight portfolio
+    with t above its risk is an interior point, x is boxed and t >= 0 with
+    gamma > 0, so the program is feasible and bounded."""
+    rng = np.random.default_rng(seed)
+    ng = n // group
+    assert ng * group == n, "n must be a multiple of group"
+    mu = rng.normal(0.05, 0.02, n)
+    dvol = rng.uniform(0.01, 0.1, n)
+    # rows of G in the layout [zero | SOC blocks | RSOC block]
+    blocks = []
+    # budget row
+    blocks.append(sp.csr_matrix((np.ones(n), (np.zeros(n, dtype=np.int64), np.arange(n))), shape=(1, n + 1)))
+    # tracking-error blocks: [r_g ; x_g - w_g] -> rows (empty, then the identity on x_g)
+    rows = np.arange(ng * (group + 1)).reshape(ng, group + 1)[:, 1:].ravel()
+    blocks.append(sp.csr_matrix((np.ones(n), (rows, np.arange(n))), shape=(ng * (group + 1), n + 1)))
+    # risk block: [t ; 1/2 ; F'x ; D x]
+    fr, fc, fv = [], [], []
+    for f in range(factors):
+        cols = np.nonzero(rng.random(n) < load_density)[0]
+        fr.append(np.full(cols.size, 2 + f, dtype=np.int64))
+        fc.append(cols)
+        fv.append(rng.normal(0.0, 0.1, cols.size))
+    r_rows = np.concatenate([[0]] + fr + [2 + factors + np.arange(n)])
+    r_cols = np.concatenate([[n]] + fc + [np.arange(n)])
+    r_vals = np.concatenate([[1.0]] + fv + [dvol])
+    blocks.append(sp.csr_matrix((r_vals, (r_rows, r_cols)), shape=(2 + factors + n, n + 1)))
+    G = sp.vstack(blocks, format="csr")
+    G.sort_indices()
+    m = G.shape[0]
+    h = np.zeros(m)
+    h[0] = 1.0
+    r_g = 10.0 / n
+    soc_rows = 1 + np.arange(ng) * (group + 1)
+    h[soc_rows] = -r_g
+    h[(soc_rows[:, None] + 1 + np.arange(group)[None, :]).ravel()] = 1.0 / n
+    rs = 1 + ng * (group + 1)
+    h[rs + 1] = -0.5
+    c = np.concatenate([-mu, [gamma]])
+    bl = np.zeros(n + 1)
+    bu = np.concatenate([np.ones(n), [np.inf]])
+    return ConicProblem(n=n + 1, m=m, nb=n + 1, c=c, G=G, h=h, mGzero=1, mGnonnegative=0,
+                        socG=[group + 1] * ng, rsocG=[2 + factors + n], bl=bl, bu=bu,
+                        name=f"portfolio_c2_{n}", seed=seed)

@@ -69,3 +69,21 @@ def test_build_staleness_check_covers_every_source():
         for f in os.listdir(d):
             if f.endswith((".cu", ".cuh", ".h")):
                 assert os.path.join(d, f) in listed, f
+
+
+def test_portfolio_generator_is_feasible_by_construction():
+    """The c2 generator's equal-weight portfolio, with t above its risk, lies
+    in the interior of every cone of the program (small instance)."""
+    n, f = 2000, 10
+    p = problems.portfolio_c2(n=n, factors=f)
+    x = np.concatenate([np.full(n, 1.0 / n), [0.0]])
+    ng = n // 10
+    rs = 1 + ng * 11
+    r = p.G @ x - p.h
+    x[-1] = 2.0 * float(np.sum(r[rs + 2:] ** 2)) + 1e-12
+    r = p.G @ x - p.h
+    assert abs(r[0]) < 1e-12                                   # budget
+    blocks = r[1:rs].reshape(ng, 11)
+    assert np.all(blocks[:, 0] > np.linalg.norm(blocks[:, 1:], axis=1))  # tracking SOC interior
+    assert 2 * r[rs] * r[rs + 1] > np.sum(r[rs + 2:] ** 2)      # risk RSOC interior
+    assert p.rsocG == [2 + f + n] and p.socG == [11] * ng and p.m == rs + 2 + f + n
