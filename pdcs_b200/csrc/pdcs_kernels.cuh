@@ -90,11 +90,21 @@ __host__ __device__ inline void after_reject(PdhgState& st) {
 // CSR SpMV with rows binned by length.  Bin b < 6 holds rows handled by a
 // group of g = 2^b lanes (rows of up to L g nonzeros for a schedule of L
 // nonzeros per lane, picked per matrix by the setup autotuner); bin 6 holds
-// longer rows, one CTA each.  One launch covers all bins: CTA ranges [cta0[b], cta0[b+1]).
+// longer rows, one CTA each; bin 7 (split rows: more than kSplitMin
+// nonzeros) holds chunks of kSplitChunk nonzeros, a CTA per chunk, whose
+// partial sums the row's last chunk to finish adds in chunk order.  One
+// launch covers all bins: CTA ranges [cta0[b], cta0[b+1]).
 // ---------------------------------------------------------------------------
-constexpr int kBins = 7;
+constexpr int kBins = 8;
+constexpr int kSplitBin = kBins - 1;
+constexpr int kRowBin = kBins - 2;
+constexpr int kSplitPer = 16;                        // nonzeros per thread of a chunk
+constexpr int kSplitChunk = kSplitPer * kThreads;   // 4096
+constexpr int64_t kSplitMin = 4 * kSplitChunk;      // rows of more nonzeros are split
 
-// rows[q] for the q-th row in bin order: {row, first nonzero, end, instance}
+// rows[q] for the q-th row in bin order: {row, first nonzero, end, instance};
+// split-row chunks: {row, first nonzero, end, chunk slot} (slots numbered
+// over all chunks, a row's chunks consecutive)
 template <class T>
 struct CsrT {
   int64_t m, n, nnz;
@@ -106,6 +116,8 @@ struct CsrT {
   int32_t lane_nnz;          // schedule: at most lane_nnz nonzeros per lane in bins 0..5
   int64_t bin_off[kBins + 1];
   int32_t cta0[kBins + 1];   // first CTA of each bin, cta0[kBins] = grid size
+  double* spart = nullptr;   // split rows: 2 partial sums per chunk slot
+  unsigned* scnt = nullptr;  // split rows: finished chunks, at the row's first slot (reset to 0 by the last)
 };
 using CsrDev = CsrT<double>;
 
@@ -171,7 +183,7 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
   const int64_t r0 = A.dbin ? A.dbin[bin] : A.bin_off[bin], r1 = A.dbin ? A.dbin[bin + 1] : A.bin_off[bin + 1];
   const int ncta = A.cta0[bin + 1] - A.cta0[bin];
   const int lcta = cta - A.cta0[bin];
-  if (bin < kBins - 1) {
+  if (bin < kRowBin) {
     const int g = 1 << bin;
     const int lane_g = threadIdx.x & (g - 1);
     const int64_t rows_per_cta = kThreads / g;
@@ -214,7 +226,7 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
         if (NV >= 2) y1[row] = s1;
       }
     }
-  } else {
+  } else if (bin == kRowBin) {
     __shared__ T red0[kWarps], red1[kWarps];
     for (int64_t q = r0 + lcta; q < r1; q += ncta) {
       const int4 ri = __ldg(A.rows + q);
@@ -222,12 +234,24 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
       if (MASK && !imask[ri.w]) continue;  // CTA-uniform
       const int32_t kb = ri.y, ke = ri.z;
       RowAcc<T> a0, a1;
-      for (int32_t k = kb + threadIdx.x; k < ke; k += kThreads) {
-        const T a = A.v[k];
-        T u0, u1;
-        spmv_gather<NV>(x0, x1, A.ci[k], u0, u1);
-        a0.add(a * u0);
-        if (NV >= 2) a1.add(a * u1);
+      // four nonzeros per thread in flight: their loads, then their gathers
+      for (int32_t kq = kb + threadIdx.x; kq < ke; kq += 4 * kThreads) {
+        T av[4];
+        int32_t cv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int32_t k = kq + u * kThreads;
+          av[u] = k < ke ? A.v[k] : T(0);
+          cv[u] = k < ke ? A.ci[k] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (cv[u] < 0) continue;
+          T u0, u1;
+          spmv_gather<NV>(x0, x1, cv[u], u0, u1);
+          a0.add(av[u] * u0);
+          if (NV >= 2) a1.add(av[u] * u1);
+        }
       }
       T s0 = a0.s, s1 = a1.s;
 #pragma unroll
@@ -249,6 +273,81 @@ __global__ void __launch_bounds__(kThreads) spmv_binned_kernel(CsrT<T> A,
         }
         y0[row] = t0.s;
         if (NV >= 2) y1[row] = t1.s;
+      }
+      __syncthreads();
+    }
+  } else if constexpr (!MASK) {
+    // split rows: a chunk of kSplitChunk nonzeros per CTA, kSplitPer per thread
+    // (all loads, then all gathers); products in T, the chunk's sum in FP64;
+    // the chunk that finishes its row last adds the row's partials in chunk
+    // order, so the result does not depend on which chunk finishes last
+    __shared__ double sr0[kWarps], sr1[kWarps];
+    __shared__ int last;
+    for (int64_t q = r0 + lcta; q < r1; q += ncta) {
+      const int4 ri = __ldg(A.rows + q);
+      const int32_t row = ri.x, kb = ri.y, ke = ri.z, slot = ri.w;
+      T av[kSplitPer];
+      int32_t cv[kSplitPer];
+#pragma unroll
+      for (int u = 0; u < kSplitPer; ++u) {
+        const int32_t k = kb + threadIdx.x + u * kThreads;
+        av[u] = k < ke ? A.v[k] : T(0);
+        cv[u] = k < ke ? A.ci[k] : -1;
+      }
+      T p0[4] = {T(0), T(0), T(0), T(0)}, p1[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+      for (int u = 0; u < kSplitPer; ++u) {
+        if (cv[u] >= 0) {
+          T a, b;
+          spmv_gather<NV>(x0, x1, cv[u], a, b);
+          p0[u & 3] = fma(av[u], a, p0[u & 3]);
+          if (NV >= 2) p1[u & 3] = fma(av[u], b, p1[u & 3]);
+        }
+      }
+      double s0 = ((double)p0[0] + (double)p0[1]) + ((double)p0[2] + (double)p0[3]);
+      double s1 = ((double)p1[0] + (double)p1[1]) + ((double)p1[2] + (double)p1[3]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(kFull, s0, o);
+        if (NV >= 2) s1 += __shfl_down_sync(kFull, s1, o);
+      }
+      if ((threadIdx.x & 31) == 0) {
+        sr0[threadIdx.x >> 5] = s0;
+        sr1[threadIdx.x >> 5] = s1;
+      }
+      __syncthreads();
+      const int32_t rb = A.rp[row], re = A.rp[row + 1];
+      const int32_t first = slot - (kb - rb) / kSplitChunk;
+      const int32_t nch = (re - rb + kSplitChunk - 1) / kSplitChunk;
+      if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+          t0 += sr0[w];
+          t1 += sr1[w];
+        }
+        A.spart[2 * (int64_t)slot] = t0;
+        A.spart[2 * (int64_t)slot + 1] = t1;
+        __threadfence();
+        last = atomicAdd(A.scnt + first, 1u) == (unsigned)(nch - 1);
+      }
+      __syncthreads();
+      if (last && threadIdx.x < 32) {  // CTA-uniform branch into warp 0
+        __threadfence();
+        double t0 = 0.0, t1 = 0.0;
+        for (int32_t c = threadIdx.x; c < nch; c += 32) {
+          t0 += __ldcg(A.spart + 2 * (int64_t)(first + c));
+          if (NV >= 2) t1 += __ldcg(A.spart + 2 * (int64_t)(first + c) + 1);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          t0 += __shfl_down_sync(kFull, t0, o);
+          if (NV >= 2) t1 += __shfl_down_sync(kFull, t1, o);
+        }
+        if (threadIdx.x == 0) {
+          y0[row] = (T)t0;
+          if (NV >= 2) y1[row] = (T)t1;
+          A.scnt[first] = 0u;
+        }
       }
       __syncthreads();
     }
@@ -324,10 +423,14 @@ struct ConeTable {
   unsigned* huge_bar;   // {arrivals, generation}
   int32_t* huge_err;    // set when a CTA gave up waiting at a barrier
   double* huge_red;     // 2 x ctaD x 4 partial sums (two alternating sets)
+  double2* huge_scr;    // per element of the huge blocks: {D_i^2 x_i^2, D_i} of the current projection
+  int64_t huge_soff[2]; // block h's first element in huge_scr
 };
 constexpr int kMaxHuge = 2;
 constexpr int64_t kHugeBlock = 16384;  // blocks of at least this many elements take part D
-constexpr int kHugeMaxCtas = 148;
+// part D CTAs: at most two per SM of a 148-SM B200, so every one of them is
+// resident (the update kernels run at least 2 CTAs per SM: <= 128 registers)
+constexpr int kHugeMaxCtas = 2 * 148;
 inline int table_grid(const ConeTable& T) { return T.ctaA + T.ctaB + T.ctaC + T.ctaD; }
 
 __device__ __forceinline__ double elem_proj(int32_t kind, double z, int64_t j, const ConeTable& T) {
@@ -504,22 +607,39 @@ __device__ inline void block_reduce_n(double (&v)[NR], const bool (&is_max)[NR])
 }
 
 // One reduction round of part D: this CTA's NR values go to its slot of the
-// round's buffer, then every CTA sums (or maximises) all slots in CTA order,
-// so all CTAs hold bit-identical results.  Returns false if a wait gave up.
+// round's buffer; after the barrier warp 0 of every CTA combines the slots
+// (lane l takes slots l, l + 32, ..., then a butterfly), the same operations in
+// the same order in every CTA, so all CTAs hold bit-identical results.
+// Returns false if a wait gave up.
 template <int NR>
 __device__ inline bool huge_allreduce(const ConeTable& T, int cta, int& round, double (&v)[NR],
                                       const bool (&is_max)[NR]) {
+  __shared__ double res[NR];
   block_reduce_n<NR>(v, is_max);
   double* buf = T.huge_red + (size_t)(round & 1) * T.ctaD * 4;
   if (threadIdx.x < NR) buf[cta * 4 + threadIdx.x] = v[threadIdx.x];
   round++;
   if (!huge_barrier(T.huge_bar, (unsigned)T.ctaD, T.huge_err)) return false;
+  if (threadIdx.x < 32) {
 #pragma unroll
-  for (int r = 0; r < NR; ++r) {
-    double x = __ldcg(buf + r);
-    for (int c = 1; c < T.ctaD; ++c) x = is_max[r] ? fmax(x, __ldcg(buf + c * 4 + r)) : x + __ldcg(buf + c * 4 + r);
-    v[r] = x;
+    for (int r = 0; r < NR; ++r) {
+      const double id = is_max[r] ? -__longlong_as_double(0x7ff0000000000000ll) : 0.0;
+      double x = id;
+#pragma unroll 4
+      for (int c = threadIdx.x; c < T.ctaD; c += 32) {
+        const double y = __ldcg(buf + c * 4 + r);
+        x = is_max[r] ? fmax(x, y) : x + y;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double y = __shfl_xor_sync(kFull, x, o);
+        x = is_max[r] ? fmax(x, y) : x + y;
+      }
+      if (threadIdx.x == 0) res[r] = x;
+    }
   }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < NR; ++r) v[r] = res[r];
   return true;
 }
 
@@ -561,11 +681,14 @@ __device__ void huge_block_proj(const Op& op, const ConeTable& T, int h, int cta
   const bool trivial = scale == 0.0 || !isfinite(scale);
   const double sc = trivial ? 1.0 : scale;
   const double t = __ldcg(u) / sc;
+  double2* scr = T.huge_scr + T.huge_soff[h];
+  const int64_t lo1 = lo > 1 ? lo : 1;
   double nr[2] = {0.0, 0.0};
-  for (int64_t i = (lo > 1 ? lo : 1) + threadIdx.x; i < hi; i += kThreads) {
+  for (int64_t i = lo1 + threadIdx.x; i < hi; i += kThreads) {
     const double D = wt(i), xi = __ldcg(u + i) / sc;
     nr[0] += (D * xi) * (D * xi);
     nr[1] += (xi / D) * (xi / D);
+    scr[i] = make_double2(D * D * xi * xi, D);  // the Newton rounds read one 16-byte record per element
   }
   const bool ksum2[2] = {false, false};
   if (!huge_allreduce<2>(T, cta, round, nr, ksum2)) return;
@@ -598,14 +721,23 @@ __device__ void huge_block_proj(const Op& op, const ConeTable& T, int h, int cta
       if (first) s = sw;
       for (int it = 0; it < 200; ++it) {
         double q[2] = {0.0, 0.0};
-        for (int64_t i = (lo > 1 ? lo : 1) + threadIdx.x; i < hi; i += kThreads) {
-          const double D = wt(i), xi = __ldcg(u + i) / sc;
-          const double c = D * D * xi * xi;
-          if (c == 0.0) continue;
-          const double a = 1.0 + D * D;
-          const double iu = 1.0 / (s * a - t * D * D);
-          q[0] += c * iu * iu;
-          q[1] += c * a * iu * iu * iu;
+        // four records per thread in flight (the same per-thread order as one at a time)
+        for (int64_t i0 = lo1 + threadIdx.x; i0 < hi; i0 += 4 * kThreads) {
+          double2 e[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int64_t i = i0 + (int64_t)k * kThreads;
+            e[k] = i < hi ? __ldcg(scr + i) : make_double2(0.0, 1.0);
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const double c = e[k].x, D = e[k].y;
+            if (c == 0.0) continue;
+            const double a = 1.0 + D * D;
+            const double iu = 1.0 / (s * a - t * D * D);
+            q[0] += c * iu * iu;
+            q[1] += c * a * iu * iu * iu;
+          }
         }
         if (!huge_allreduce<2>(T, cta, round, q, ksum2)) return;
         const double Q = 1.0 / sqrt(q[0]);
@@ -634,7 +766,7 @@ __device__ void huge_block_proj(const Op& op, const ConeTable& T, int h, int cta
     if (mode == 1) return 0.0;
     if (i == 0) return s0;
     if (mode == 2) return ui * cc;
-    const double D = wt(i);
+    const double D = __ldcg(scr + i).y;
     return ui / (1.0 + mu * D * D);
   };
   for (int64_t i = lo + threadIdx.x; i < hi; i += kThreads) {
@@ -657,7 +789,9 @@ concept MaskedOp = requires(const Op& o) { o.live(int64_t(0)); };
 //   load(): read scalars; z(j): value before projection; fin(j, z, p, acc): consume.
 // EXP: compile the exponential-cone path (its root solve sets the register
 // budget of the whole kernel; tables without exp cones use EXP = false).
-template <class Op, bool EXP = true>
+// HUGE: compile part D (tables with huge blocks only: its code raises the
+// register count of the whole kernel, 64 -> 80 without EXP).
+template <class Op, bool EXP = true, bool HUGE = false>
 __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTable T, double* partials,
                                                                  const int32_t* active) {
   if (active && !*active) return;
@@ -667,9 +801,11 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
   for (int k = 0; k < Op::NACC; ++k) acc[k] = 0.0;
   const int b = (int)blockIdx.x - T.ctaD;  // part D (huge blocks) first: the lowest block indices
   const int nblocks = gridDim.x;
-  if (b < 0) {
-    int round = 0;
-    for (int h = 0; h < T.nhuge; ++h) huge_block_proj<Op, Op::NACC>(op, T, h, (int)blockIdx.x, round, acc);
+  if (HUGE && b < 0) {
+    if constexpr (HUGE) {
+      int round = 0;
+      for (int h = 0; h < T.nhuge; ++h) huge_block_proj<Op, Op::NACC>(op, T, h, (int)blockIdx.x, round, acc);
+    }
   } else if (b < T.ctaA && T.act_chunk) {
     // chunks of the elementwise segments, a CTA per chunk
     const int64_t nch = T.act_meta[0];
@@ -871,7 +1007,15 @@ template <class Op>
 inline void launch_update_project(const Op& op, const ConeTable& T, double* partials, const int32_t* active,
                                   cudaStream_t s) {
   const int grid = table_grid(T);
-  if (T.exp_count + T.dexp_count > 0) update_project_kernel<Op, true><<<grid, kThreads, 0, s>>>(op, T, partials, active);
+  const bool exp = T.exp_count + T.dexp_count > 0;
+  if constexpr (!MaskedOp<Op>) {  // masked (batched) tables never hold huge blocks
+    if (T.nhuge > 0) {
+      if (exp) update_project_kernel<Op, true, true><<<grid, kThreads, 0, s>>>(op, T, partials, active);
+      else update_project_kernel<Op, false, true><<<grid, kThreads, 0, s>>>(op, T, partials, active);
+      return;
+    }
+  }
+  if (exp) update_project_kernel<Op, true><<<grid, kThreads, 0, s>>>(op, T, partials, active);
   else update_project_kernel<Op, false><<<grid, kThreads, 0, s>>>(op, T, partials, active);
 }
 

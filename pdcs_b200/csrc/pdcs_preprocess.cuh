@@ -32,16 +32,23 @@ __global__ void check_inputs_kernel(int64_t m, int64_t n, int64_t nnz, int64_t n
   if (e) atomicOr(err, e);
 }
 
-// row index of every nonzero and the nonzero count of every column
-__global__ void expand_rows_kernel(int64_t m, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                   int32_t* __restrict__ row_of, int32_t* __restrict__ col_cnt) {
-  const int lane = threadIdx.x & 31;
-  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += wstride)
-    for (int32_t k = rp[i] + lane; k < rp[i + 1]; k += 32) {
-      row_of[k] = (int32_t)i;
-      atomicAdd(&col_cnt[ci[k]], 1);
-    }
+// Row index of every nonzero, in two flat passes (a row of any length costs
+// the same per nonzero): each nonempty row writes its index at its first
+// nonzero (the array zeroed before), then an inclusive max-scan fills the rest.
+__global__ void row_start_kernel(int64_t m, const int32_t* __restrict__ rp, int32_t* __restrict__ start) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+    if (rp[i] < rp[i + 1]) start[rp[i]] = (int32_t)i;
+}
+
+struct MaxI32 {
+  __device__ __forceinline__ int32_t operator()(int32_t a, int32_t b) const { return a > b ? a : b; }
+};
+
+// nonzero count of every column
+__global__ void col_count_kernel(int64_t nnz, const int32_t* __restrict__ ci, int32_t* __restrict__ col_cnt) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += stride) atomicAdd(&col_cnt[ci[k]], 1);
 }
 
 __global__ void iota_kernel(int32_t* a, int64_t n) {
@@ -61,13 +68,17 @@ __global__ void gather_transpose_kernel(int64_t nnz, const int32_t* __restrict__
   }
 }
 
-// per row of a CSR (values read through an optional permutation): max |v| or sum |v|
+// per row of a CSR (values read through an optional permutation): max |v| or
+// sum |v|, a warp per row; rows of more than long_min nonzeros are left to
+// row_absstat_long_kernel (long_min < 0: none)
 template <bool SUM>
 __global__ void row_absstat_kernel(int64_t rows, const int32_t* __restrict__ rp, const double* __restrict__ v,
-                                   const int32_t* __restrict__ perm, double* __restrict__ out) {
+                                   const int32_t* __restrict__ perm, double* __restrict__ out,
+                                   int64_t long_min = -1) {
   const int lane = threadIdx.x & 31;
   const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < rows; i += wstride) {
+    if (long_min >= 0 && rp[i + 1] - rp[i] > long_min) continue;  // warp-uniform
     double a = 0.0;
     for (int32_t k = rp[i] + lane; k < rp[i + 1]; k += 32) {
       const double x = fabs(perm ? v[perm[k]] : v[k]);
@@ -81,6 +92,36 @@ __global__ void row_absstat_kernel(int64_t rows, const int32_t* __restrict__ rp,
   }
 }
 
+// the same statistic for the long rows listed in `list`, a CTA per row
+template <bool SUM>
+__global__ void __launch_bounds__(kThreads) row_absstat_long_kernel(int64_t nlist, const int32_t* __restrict__ list,
+                                                                    const int32_t* __restrict__ rp,
+                                                                    const double* __restrict__ v,
+                                                                    const int32_t* __restrict__ perm,
+                                                                    double* __restrict__ out) {
+  __shared__ double sh[kWarps];
+  for (int64_t q = blockIdx.x; q < nlist; q += gridDim.x) {
+    const int32_t i = list[q];
+    double a = 0.0;
+    for (int32_t k = rp[i] + threadIdx.x; k < rp[i + 1]; k += kThreads) {
+      const double x = fabs(perm ? v[perm[k]] : v[k]);
+      a = SUM ? a + x : fmax(a, x);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double b = __shfl_down_sync(kFull, a, o);
+      a = SUM ? a + b : fmax(a, b);
+    }
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = sh[0];
+      for (int w = 1; w < kWarps; ++w) t = SUM ? t + sh[w] : fmax(t, sh[w]);
+      out[i] = t;
+    }
+    __syncthreads();
+  }
+}
+
 // a = 1 where a == 0, sqrt(a) elsewhere
 __global__ void sqrt_or_one_kernel(double* a, int64_t n) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -88,16 +129,13 @@ __global__ void sqrt_or_one_kernel(double* a, int64_t n) {
     a[i] = (a[i] == 0.0) ? 1.0 : sqrt(a[i]);
 }
 
-// G_ij /= (con_i var_j), one warp per row
-__global__ void scale_matrix_kernel(int64_t m, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+// G_ij /= (con_i var_j), flat over the nonzeros (row_of: the row of each)
+__global__ void scale_matrix_kernel(int64_t nnz, const int32_t* __restrict__ row_of, const int32_t* __restrict__ ci,
                                     double* __restrict__ v, const double* __restrict__ con,
                                     const double* __restrict__ var) {
-  const int lane = threadIdx.x & 31;
-  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m; i += wstride) {
-    const double ci_ = con[i];
-    for (int32_t k = rp[i] + lane; k < rp[i + 1]; k += 32) v[k] /= (ci_ * var[ci[k]]);
-  }
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += stride)
+    v[k] /= (con[row_of[k]] * var[ci[k]]);
 }
 
 // c /= var, Dr *= var, [bl, bu] *= var (box part), h /= con, Dl *= con

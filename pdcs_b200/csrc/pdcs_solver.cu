@@ -510,8 +510,13 @@ class Solver {
   void build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
                   const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst, int lane_nnz);
   int tune_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp, const int32_t* d_ci,
-                const double* d_v, CsrDev& D, const int32_t* row_inst, const double* xin, double* yout);
+                const double* d_v, CsrDev& D, const int32_t* row_inst, const double* xin, double* yout,
+                const float* v32 = nullptr);
+  float* gv32_ = nullptr;  // FP32 values of G and G' (FP32-bulk mode), converted before the schedules are tuned
+  float* tv32_ = nullptr;
   int lane_G_ = 4, lane_Gt_ = 4;  // SpMV schedules in use (nonzeros per lane)
+  // split-row workspaces (chunk partials, row counters) per matrix, keyed on its row pointers
+  std::map<const int32_t*, std::pair<double*, unsigned*>> split_ws_;
   // instance of each row of G and of G' (batched solver; NULL: one instance)
   const int32_t* inst_of_y_ = nullptr;
   const int32_t* inst_of_x_ = nullptr;
@@ -679,7 +684,9 @@ int Solver::validate() {
 
 // Rows binned by length for a schedule of lane_nnz nonzeros per lane: bin b < 6
 // takes rows of at most lane_nnz * 2^b nonzeros (g = 2^b lanes each), bin 6 the
-// longer rows (a CTA each).  Counting sort: rows keep their order inside a bin.
+// longer rows (a CTA each), bin 7 the chunks of rows over kSplitMin nonzeros
+// (one instance only: the batched solver's masked SpMV keeps them in bin 6).
+// Counting sort: rows keep their order inside a bin.
 void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
                         const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst, int lane_nnz) {
   D.m = rows;
@@ -690,15 +697,21 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
   D.v = d_v;
   D.dbin = nullptr;
   D.lane_nnz = lane_nnz;
+  const bool split = row_inst == nullptr;
   auto bin_of = [&](int64_t i) {
     const int64_t L = rp[i + 1] - rp[i];
-    if (L > 32LL * lane_nnz) return kBins - 1;
+    if (split && L > kSplitMin) return kSplitBin;
+    if (L > 32LL * lane_nnz) return kRowBin;
     int b = 0;
-    while (b < kBins - 2 && ((int64_t)lane_nnz << b) < L) ++b;
+    while (b < kRowBin - 1 && ((int64_t)lane_nnz << b) < L) ++b;
     return b;
   };
+  auto chunks = [&](int64_t i) { return (rp[i + 1] - rp[i] + kSplitChunk - 1) / kSplitChunk; };
   int64_t cnt[kBins] = {};
-  for (int64_t i = 0; i < rows; ++i) cnt[bin_of(i)]++;
+  for (int64_t i = 0; i < rows; ++i) {
+    const int b = bin_of(i);
+    cnt[b] += b == kSplitBin ? chunks(i) : 1;
+  }
   int64_t off = 0;
   int32_t cta = 0;
   int64_t pos[kBins];
@@ -709,18 +722,41 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
     const int64_t R = cnt[b];
     off += R;
     if (R == 0) continue;
-    if (b < kBins - 1) {
+    if (b < kRowBin) {
       int64_t rows_per_cta = kThreads >> b;
       cta += (int32_t)std::min<int64_t>((R + rows_per_cta - 1) / rows_per_cta, 148 * 16);
-    } else {
+    } else if (b == kRowBin) {
       cta += (int32_t)std::min<int64_t>(R, 148 * 8);
+    } else {  // a CTA per chunk: resident CTAs in different phases keep the loads streaming
+      cta += (int32_t)std::min<int64_t>(R, 1 << 24);
     }
   }
   D.bin_off[kBins] = off;
   D.cta0[kBins] = std::max(cta, 1);
-  std::vector<int4> desc(rows);
-  for (int64_t i = 0; i < rows; ++i)
-    desc[pos[bin_of(i)]++] = make_int4((int32_t)i, rp[i], rp[i + 1], row_inst ? row_inst[i] : 0);
+  std::vector<int4> desc(off);
+  int32_t slot = 0;
+  for (int64_t i = 0; i < rows; ++i) {
+    const int b = bin_of(i);
+    if (b == kSplitBin) {
+      for (int64_t k = rp[i]; k < rp[i + 1]; k += kSplitChunk)
+        desc[pos[b]++] = make_int4((int32_t)i, (int32_t)k, (int32_t)std::min<int64_t>(k + kSplitChunk, rp[i + 1]), slot++);
+    } else {
+      desc[pos[b]++] = make_int4((int32_t)i, rp[i], rp[i + 1], row_inst ? row_inst[i] : 0);
+    }
+  }
+  D.spart = nullptr;
+  D.scnt = nullptr;
+  if (slot > 0) {  // one workspace per matrix, shared by its schedules (same chunks)
+    auto it = split_ws_.find(d_rp);
+    if (it == split_ws_.end()) {
+      double* p = A.alloc<double>(2 * (size_t)slot);
+      unsigned* c = A.alloc<unsigned>(slot);
+      PDCS_CUDA(cudaMemsetAsync(c, 0, sizeof(unsigned) * slot, s_));
+      it = split_ws_.emplace(d_rp, std::make_pair(p, c)).first;
+    }
+    D.spart = it->second.first;
+    D.scnt = it->second.second;
+  }
   int4* d_desc = A.alloc<int4>(std::max<size_t>(desc.size(), 1));
   if (!desc.empty())
     PDCS_CUDA(cudaMemcpyAsync(d_desc, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice, s_));
@@ -732,22 +768,45 @@ void Solver::build_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t co
 // costs more than a small solve can gain from the choice
 constexpr int64_t kTuneMinNnz = 1 << 20;
 
+// FP32 view of a CSR with the same structure and schedule
+static CsrT<float> narrow_csr(const CsrDev& D, const float* v) {
+  CsrT<float> F;
+  F.m = D.m;
+  F.n = D.n;
+  F.nnz = D.nnz;
+  F.rp = D.rp;
+  F.ci = D.ci;
+  F.v = v;
+  F.rows = D.rows;
+  F.dbin = D.dbin;
+  F.lane_nnz = D.lane_nnz;
+  F.spart = D.spart;
+  F.scnt = D.scnt;
+  for (int b = 0; b <= kBins; ++b) {
+    F.bin_off[b] = D.bin_off[b];
+    F.cta0[b] = D.cta0[b];
+  }
+  return F;
+}
+
 // SpMV schedule autotuner: time each nonzeros-per-lane target on this matrix
 // (CUDA events, best of 3 after a warm-up) and keep the fastest, leaving the
 // default (4) only for a gain of 3% or more; a fixed target (spmv_lane_nnz > 0)
 // skips the search.  The choice is remembered per device and row structure
 // for the life of the process, so repeated solves of a matrix use the same
-// schedule (and give bit-identical results).  Returns the target used.
+// schedule (and give bit-identical results).  With v32 (FP32-bulk mode) the
+// candidates are timed on the FP32 values, the precision of the iteration.
+// Returns the target used.
 int Solver::tune_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols, const int32_t* d_rp,
                       const int32_t* d_ci, const double* d_v, CsrDev& D, const int32_t* row_inst, const double* xin,
-                      double* yout) {
+                      double* yout, const float* v32) {
   if (O.spmv_lane_nnz > 0 || rp[rows] < kTuneMinNnz) {  // fixed, or too small for the search to pay off
     const int lane = O.spmv_lane_nnz > 0 ? O.spmv_lane_nnz : 4;
     build_bins(rp, rows, cols, d_rp, d_ci, d_v, D, row_inst, lane);
     return lane;
   }
   static std::mutex mu;
-  static std::map<std::array<uint64_t, 4>, int> chosen;
+  static std::map<std::array<uint64_t, 5>, int> chosen;
   int dev = 0;
   PDCS_CUDA(cudaGetDevice(&dev));
   uint64_t h = 1469598103934665603ull;
@@ -755,7 +814,7 @@ int Solver::tune_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols
     h ^= (uint64_t)(uint32_t)rp[i];
     h *= 1099511628211ull;
   }
-  const std::array<uint64_t, 4> key{(uint64_t)dev, (uint64_t)rows, (uint64_t)cols, h};
+  const std::array<uint64_t, 5> key{(uint64_t)dev, (uint64_t)rows, (uint64_t)cols, h, v32 ? 1ull : 0ull};
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = chosen.find(key);
@@ -770,21 +829,34 @@ int Solver::tune_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols
   int best = 4;
   float best_ms = 1e30f;
   CsrDev best_D{};
+  float *x32 = nullptr, *y32 = nullptr;
+  if (v32) {
+    x32 = A.alloc<float>(cols);
+    y32 = A.alloc<float>(rows);
+    PDCS_CUDA(cudaMemsetAsync(x32, 0, sizeof(float) * std::max<int64_t>(cols, 1), s_));
+  }
   for (int lane : {4, 2, 8, 16}) {  // the default first: others must beat it by 3%
     CsrDev C;
     build_bins(rp, rows, cols, d_rp, d_ci, d_v, C, row_inst, lane);
-    spmv(C, xin, yout);
+    const CsrT<float> C32 = narrow_csr(C, v32);
+    auto run = [&]() {
+      if (v32)
+        launch_spmv<1>(C32, x32, nullptr, y32, nullptr, nullptr, s_);
+      else
+        spmv(C, xin, yout);
+    };
+    run();
     float t = 1e30f;
     for (int r = 0; r < 3; ++r) {
       PDCS_CUDA(cudaEventRecord(e0, s_));
-      spmv(C, xin, yout);
+      run();
       PDCS_CUDA(cudaEventRecord(e1, s_));
       PDCS_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
       PDCS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       t = std::min(t, ms);
     }
-    kernels_ -= 4;
+    if (!v32) kernels_ -= 4;
     if (lane != 4) t *= 1.03f;
     if (t < best_ms) {
       if (best_D.rows) A.drop(best_D.rows);
@@ -797,6 +869,10 @@ int Solver::tune_bins(const std::vector<int32_t>& rp, int64_t rows, int64_t cols
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (x32) {
+    A.drop(x32);
+    A.drop(y32);
+  }
   D = best_D;
   std::lock_guard<std::mutex> lock(mu);
   chosen.emplace(key, best);
@@ -816,9 +892,9 @@ void Solver::size_table(ConeTable& T) {
   if (T.nhuge > 0) {
     int64_t dmin = T.huge_len[0];
     for (int h = 1; h < T.nhuge; ++h) dmin = std::min(dmin, T.huge_len[h]);
-    // about 4096 elements per CTA, at most one CTA per SM (every CTA of part D resident),
+    // about 2048 elements per CTA, at most two CTAs per SM (every CTA of part D resident),
     // at least 2 elements per CTA (elements 0 and 1 of a block in CTA 0)
-    T.ctaD = (int32_t)std::max<int64_t>(1, std::min<int64_t>({(dmin + 4095) / 4096, dmin / 2, (int64_t)kHugeMaxCtas}));
+    T.ctaD = (int32_t)std::max<int64_t>(1, std::min<int64_t>({(dmin + 2047) / 2048, dmin / 2, (int64_t)kHugeMaxCtas}));
     if (!huge_bar_) {
       huge_bar_ = A.alloc<unsigned>(4);
       huge_err_ = A.alloc<int32_t>(4);
@@ -829,6 +905,12 @@ void Solver::size_table(ConeTable& T) {
     T.huge_bar = huge_bar_;
     T.huge_err = huge_err_;
     T.huge_red = huge_red_;
+    int64_t tot = 0;
+    for (int h = 0; h < T.nhuge; ++h) {
+      T.huge_soff[h] = tot;
+      tot += T.huge_len[h];
+    }
+    T.huge_scr = A.alloc<double2>(tot);
   }
   if (table_grid(T) == 0) T.ctaA = 1;  // at least one CTA writes the partials
 }
@@ -848,7 +930,9 @@ void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<i
     std::vector<std::vector<int64_t>> cls(kCls);
     T.nhuge = 0;
     for (size_t k = 0; k < lv.size(); ++k) {
-      if (lv[k] >= kHugeBlock && T.nhuge < kMaxHuge) {  // part D: the launch's first CTAs together
+      // part D (the launch's first CTAs together) in the single solver; the batched
+      // solver's masked updates keep every block on a warp (part D ignores the mask)
+      if (lv[k] >= kHugeBlock && T.nhuge < kMaxHuge && inst_of_y_ == nullptr) {
         T.huge_start[T.nhuge] = stv[k];
         T.huge_len[T.nhuge] = lv[k];
         T.huge_rsoc[T.nhuge] = kv[k] == PK_RSOC ? 1 : 0;
@@ -1038,20 +1122,45 @@ void Solver::setup() {
   int32_t* perm_in = A.alloc<int32_t>(nnz_);
   int32_t* perm_t = A.alloc<int32_t>(nnz_);
   PDCS_CUDA(cudaMemsetAsync(col_cnt, 0, sizeof(int32_t) * (n_ + 1), s_));
-  expand_rows_kernel<<<warp_grid(m_), kThreads, 0, s_>>>(m_, g_rp, g_ci, row_of, col_cnt);
-  iota_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(perm_in, nnz_);
+  PDCS_CUDA(cudaMemsetAsync(perm_in, 0, sizeof(int32_t) * std::max<int64_t>(nnz_, 1), s_));
+  row_start_kernel<<<grid_for(m_), kThreads, 0, s_>>>(m_, g_rp, perm_in);
+  col_count_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(nnz_, g_ci, col_cnt);
   {
-    size_t b1 = 0, b2 = 0;
+    size_t b1 = 0, b2 = 0, b3 = 0;
     int bits = 1;
     while ((int64_t(1) << bits) <= n_) ++bits;
     PDCS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b1, col_cnt, t_rp, (int)(n_ + 1), s_));
     PDCS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b2, g_ci, keys_sorted, perm_in, perm_t, (int)nnz_, 0, bits,
                                               s_));
-    void* tmp = A.alloc<char>(std::max(b1, b2));
+    PDCS_CUDA(cub::DeviceScan::InclusiveScan(nullptr, b3, perm_in, row_of, MaxI32{}, (int)nnz_, s_));
+    void* tmp = A.alloc<char>(std::max(std::max(b1, b2), b3));
+    if (nnz_ > 0) PDCS_CUDA(cub::DeviceScan::InclusiveScan(tmp, b3, perm_in, row_of, MaxI32{}, (int)nnz_, s_));
+    iota_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(perm_in, nnz_);
     PDCS_CUDA(cub::DeviceScan::ExclusiveSum(tmp, b1, col_cnt, t_rp, (int)(n_ + 1), s_));
     if (nnz_ > 0)
       PDCS_CUDA(cub::DeviceRadixSort::SortPairs(tmp, b2, g_ci, keys_sorted, perm_in, perm_t, (int)nnz_, 0, bits, s_));
   }
+  // both row-pointer arrays on the host (row bins, and the long rows of the statistics below)
+  std::vector<int32_t> rp_h(m_ + 1), trp_h(n_ + 1);
+  PDCS_CUDA(cudaMemcpyAsync(rp_h.data(), g_rp, sizeof(int32_t) * (m_ + 1), cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaMemcpyAsync(trp_h.data(), t_rp, sizeof(int32_t) * (n_ + 1), cudaMemcpyDeviceToHost, s_));
+  PDCS_CUDA(cudaStreamSynchronize(s_));
+  // rows (of G and of G') over kStatLong nonzeros: a CTA each in the row statistics
+  constexpr int64_t kStatLong = 4096;
+  auto long_rows = [&](const std::vector<int32_t>& rp, int64_t rows, int64_t& count) -> int32_t* {
+    std::vector<int32_t> l;
+    for (int64_t i = 0; i < rows; ++i)
+      if (rp[i + 1] - rp[i] > kStatLong) l.push_back((int32_t)i);
+    count = (int64_t)l.size();
+    if (l.empty()) return nullptr;
+    int32_t* d = A.alloc<int32_t>(l.size());
+    PDCS_CUDA(cudaMemcpyAsync(d, l.data(), sizeof(int32_t) * l.size(), cudaMemcpyHostToDevice, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    return d;
+  };
+  int64_t nlong_g = 0, nlong_t = 0;
+  int32_t* long_g = long_rows(rp_h, m_, nlong_g);
+  int32_t* long_t = long_rows(trp_h, n_, nlong_t);
   phase("transpose");
   // ---- Ruiz (10) + Pock-Chambolle (alpha = 1) equilibration on the device ----
   c_s = A.alloc<double>(n_);
@@ -1073,17 +1182,25 @@ void Solver::setup() {
   fill_kernel<<<grid_for(m_), kThreads, 0, s_>>>(Dl, 1.0, m_);
   double* var = A.alloc<double>(n_);
   double* con = A.alloc<double>(m_);
+  auto stat = [&](auto sum_tag, int64_t rows, const int32_t* rp, const int32_t* perm, double* out,
+                  const int32_t* list, int64_t nlist) {
+    constexpr bool SUM = decltype(sum_tag)::value;
+    row_absstat_kernel<SUM><<<warp_grid(rows), kThreads, 0, s_>>>(rows, rp, g_v, perm, out, list ? kStatLong : -1);
+    if (list)
+      row_absstat_long_kernel<SUM><<<(int)std::min<int64_t>(nlist, 148 * 8), kThreads, 0, s_>>>(nlist, list, rp, g_v,
+                                                                                                perm, out);
+  };
   auto pass = [&](bool sum) {
     if (sum) {
-      row_absstat_kernel<true><<<warp_grid(m_), kThreads, 0, s_>>>(m_, g_rp, g_v, nullptr, con);
-      row_absstat_kernel<true><<<warp_grid(n_), kThreads, 0, s_>>>(n_, t_rp, g_v, perm_t, var);
+      stat(std::true_type{}, m_, g_rp, nullptr, con, long_g, nlong_g);
+      stat(std::true_type{}, n_, t_rp, perm_t, var, long_t, nlong_t);
     } else {
-      row_absstat_kernel<false><<<warp_grid(m_), kThreads, 0, s_>>>(m_, g_rp, g_v, nullptr, con);
-      row_absstat_kernel<false><<<warp_grid(n_), kThreads, 0, s_>>>(n_, t_rp, g_v, perm_t, var);
+      stat(std::false_type{}, m_, g_rp, nullptr, con, long_g, nlong_g);
+      stat(std::false_type{}, n_, t_rp, perm_t, var, long_t, nlong_t);
     }
     sqrt_or_one_kernel<<<grid_for(m_), kThreads, 0, s_>>>(con, m_);
     sqrt_or_one_kernel<<<grid_for(n_), kThreads, 0, s_>>>(var, n_);
-    scale_matrix_kernel<<<warp_grid(m_), kThreads, 0, s_>>>(m_, g_rp, g_ci, g_v, con, var);
+    scale_matrix_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(nnz_, row_of, g_ci, g_v, con, var);
     scale_vectors_kernel<<<grid_for(std::max(n_, m_)), kThreads, 0, s_>>>(n_, nb_, m_, var, con, c_s, Dr, bl_s, bu_s,
                                                                         h_s, Dl);
   };
@@ -1105,11 +1222,6 @@ void Solver::setup() {
   if (nb_ > 0)
     box_aux_kernel<<<grid_for(nb_), kThreads, 0, s_>>>(nb_, bl_raw, bu_raw, bl_fin, bu_fin, lam_l, lam_u);
   phase("equilibration");
-  // ---- SpMV row bins (host sees only the two row-pointer arrays) ----
-  std::vector<int32_t> rp_h(m_ + 1), trp_h(n_ + 1);
-  PDCS_CUDA(cudaMemcpyAsync(rp_h.data(), g_rp, sizeof(int32_t) * (m_ + 1), cudaMemcpyDeviceToHost, s_));
-  PDCS_CUDA(cudaMemcpyAsync(trp_h.data(), t_rp, sizeof(int32_t) * (n_ + 1), cudaMemcpyDeviceToHost, s_));
-  PDCS_CUDA(cudaStreamSynchronize(s_));
   // ---- iterates and work vectors ----
   auto vecn = [&]() { return A.alloc<double>(n_); };
   auto vecm = [&]() { return A.alloc<double>(m_); };
@@ -1132,8 +1244,14 @@ void Solver::setup() {
   copy(yl, y, m_); copy(ym, y, m_); copy(ybest, y, m_);
   phase("row bins, work vectors");
   // ---- SpMV schedules: autotuned per matrix unless fixed by the options ----
-  lane_G_ = tune_bins(rp_h, m_, n_, g_rp, g_ci, g_v, G_, inst_of_y_, x, tm[0]);
-  lane_Gt_ = tune_bins(trp_h, n_, m_, t_rp, t_ci, t_v, Gt_, inst_of_x_, y, tn[0]);
+  if (O.precision == 1) {  // the FP32 iteration sets the schedule
+    gv32_ = A.alloc<float>(nnz_);
+    tv32_ = A.alloc<float>(nnz_);
+    to_float_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(gv32_, g_v, nnz_);
+    to_float_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(tv32_, t_v, nnz_);
+  }
+  lane_G_ = tune_bins(rp_h, m_, n_, g_rp, g_ci, g_v, G_, inst_of_y_, x, tm[0], gv32_);
+  lane_Gt_ = tune_bins(trp_h, n_, m_, t_rp, t_ci, t_v, Gt_, inst_of_x_, y, tn[0], tv32_);
   if (O.differentiable) {
     double* t_v_raw = A.alloc<double>(nnz_);
     gather_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(t_v_raw, g_v_raw, perm_t, nnz_);
@@ -1165,29 +1283,14 @@ void Solver::setup() {
 
 void Solver::setup_fp32() {
   fp32_ = true;
-  float* gv = A.alloc<float>(nnz_);
-  float* tv = A.alloc<float>(nnz_);
-  to_float_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(gv, G_.v, nnz_);
-  to_float_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(tv, Gt_.v, nnz_);
-  auto narrow = [](const CsrDev& D, const float* v) {
-    CsrT<float> F;
-    F.m = D.m;
-    F.n = D.n;
-    F.nnz = D.nnz;
-    F.rp = D.rp;
-    F.ci = D.ci;
-    F.v = v;
-    F.rows = D.rows;
-    F.dbin = D.dbin;
-    F.lane_nnz = D.lane_nnz;
-    for (int b = 0; b <= kBins; ++b) {
-      F.bin_off[b] = D.bin_off[b];
-      F.cta0[b] = D.cta0[b];
-    }
-    return F;
-  };
-  G32_ = narrow(G_, gv);
-  Gt32_ = narrow(Gt_, tv);
+  if (!gv32_) {
+    gv32_ = A.alloc<float>(nnz_);
+    tv32_ = A.alloc<float>(nnz_);
+    to_float_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(gv32_, G_.v, nnz_);
+    to_float_kernel<<<grid_for(nnz_), kThreads, 0, s_>>>(tv32_, Gt_.v, nnz_);
+  }
+  G32_ = narrow_csr(G_, gv32_);
+  Gt32_ = narrow_csr(Gt_, tv32_);
   dxp32_ = A.alloc<float2>(n_);
   aty32_ = A.alloc<float>(n_);
   dy32_ = A.alloc<float>(m_);

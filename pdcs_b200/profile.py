@@ -1,5 +1,6 @@
 """Bounded solve runner for profiling:  python -m pdcs_b200.profile --workload logreg --attempts 64
-(or --workload batch --count 4096 --precision fp32: the batched uneven-SOCP workload)
+(or --workload batch --count 4096 --precision fp32: the batched uneven-SOCP workload;
+--workload portfolio --assets 1000000: the robust portfolio with its huge risk cone)
 
 Builds a seeded workload, uploads it to the GPU and runs the solver for a fixed
 number of PDHG attempts (or to convergence with --attempts 0), printing the
@@ -11,12 +12,14 @@ import sys
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="logreg", choices=["logreg", "logreg_small", "socp", "mixed", "batch"])
+    ap.add_argument("--workload", default="logreg", choices=["logreg", "logreg_small", "socp", "mixed", "batch",
+                                                                 "portfolio"])
     ap.add_argument("--count", type=int, default=4096, help="instances of the batch workload")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--attempts", type=int, default=64)
     ap.add_argument("--samples", type=int, default=20000)
     ap.add_argument("--features", type=int, default=500)
+    ap.add_argument("--assets", type=int, default=1_000_000)
     ap.add_argument("--repeat", type=int, default=1)
     a = ap.parse_args(argv)
     import numpy as np
@@ -33,6 +36,8 @@ def main(argv=None):
         p = problems.logreg_exp_c1(samples=a.samples, features=a.features)
     elif a.workload == "logreg_small":
         p = problems.logreg_exp_c1(samples=2000, features=100)
+    elif a.workload == "portfolio":
+        p = problems.portfolio_c2(n=a.assets)
     elif a.workload == "socp":
         p = problems.socp_c0()
     else:

@@ -32,6 +32,27 @@ def test_c2_first_attempts_track_oracle(cuda, c2_small, attempts):
         assert err <= 1e-9, (attempts, err)
 
 
+@pytest.fixture(scope="module")
+def c2_long_rows():
+    """Factor rows of 35000 nonzeros and a budget row of 70000: both above the
+    split-row threshold of the binned SpMV (16384), so G x runs as chunks of
+    4096 nonzeros whose partials the row's last chunk adds."""
+    return problems.portfolio_c2(n=70000, factors=8, load_density=0.5)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("attempts", [1, 7])
+def test_c2_split_rows_track_oracle(cuda, c2_long_rows, precision, attempts):
+    p = c2_long_rows
+    g = solver.solve_problem(p, precision=precision, attempt_limit=attempts)
+    o = B.solve(p, threads=1, attempt_limit=attempts)
+    assert g.info.iter == o["iter"] == attempts
+    tol = 1e-9 if precision == "fp64" else 1e-6
+    for a, b in ((g.primal, o["x"]), (g.dual, o["y"])):
+        err = np.abs(a - b).max() / max(1.0, np.abs(b).max())
+        assert err <= tol, (attempts, err)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_c2_solution_meets_criteria(cuda, c2_small, precision):
     p = c2_small
