@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-single", action="store_true",
-                    help="skip the single-instance exp-cone and differentiable-layer sections")
+                    help="skip the single-instance exp-cone, portfolio and differentiable-layer sections")
     return ap.parse_args()
 
 
@@ -316,6 +316,72 @@ def single_instance_section(dev, stream):
             "exit_status": i.exit_status, "spmv_lane_nnz": list(i.spmv_lane_nnz)}
 
 
+def portfolio_section(dev, stream):
+    """The robust portfolio (1e6 assets in [0, 1], 200 factors at 25 % density, 1e5 SOC
+    tracking blocks of dimension 11, one RSOC risk block of 1 000 202 elements, a budget
+    row; 5.3e7 nonzeros): FP32 bulk with FP64 anchors against plain FP64, one GPU, each
+    solved to the 1e-6 criteria from device-resident data; per-attempt time and HBM
+    roofline; each result's objective against the oracle's optimum of the same seeded
+    instance (tests/golden/c2_oracle.json, when its checksums match) and the two
+    precisions against each other."""
+    import numpy as np
+    import torch
+    from pdcs_b200 import problems, solver
+    p = problems.portfolio_c2()
+    G = p.G.tocsr()
+    t = lambda a, dt=torch.float64: torch.as_tensor(np.asarray(a), dtype=dt, device=dev)
+    kw = p.kwargs()
+    kw.update(c=t(p.c), h=t(p.h), bl=t(p.bl), bu=t(p.bu),
+              G=(t(G.indptr, torch.int32), t(G.indices, torch.int32), t(G.data)))
+    golden = None
+    gpath = os.path.join(ROOT, "tests", "golden", "c2_oracle.json")
+    if os.path.exists(gpath):
+        g = json.load(open(gpath))
+        cs = g.get("checksums", {})
+        if cs.get("nnz") == int(G.nnz) and np.isclose(cs.get("sum_G", np.nan), float(np.sum(G.data)), rtol=1e-12):
+            golden = g
+    pstar = golden["optimum"]["primal_objective"] if golden else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    out = {"workload": f"robust portfolio, n={p.n}, m={p.m}, nnz={p.nnz} (1e5 SOC blocks of dim 11, "
+                       f"one RSOC block of {p.m - 1 - 11 * (p.n - 1) // 10}, budget row), to 1e-6",
+           "oracle_optimum": pstar,
+           "oracle_source": "tests/golden/c2_oracle.json (oracle at 1e-8)" if golden else None}
+    sols = {}
+    for prec, w in (("fp64", 8), ("fp32", 4)):
+        run = lambda **o: solver.rpdhg_gpu_solve(**kw, precision=prec, stream=stream.cuda_stream, **o)
+        timed(stream, lambda: run(attempt_limit=64))
+        t_att = 1e30
+        for _ in range(2):  # the smaller of two differences (200 vs 600 attempts, no exit check between)
+            _, ta = timed(stream, lambda: run(attempt_limit=200))
+            _, tb = timed(stream, lambda: run(attempt_limit=600))
+            t_att = min(t_att, (tb - ta) / 400)
+        sol, dt = timed(stream, lambda: run())
+        i = sol.info
+        B_att = bytes_per_attempt(p.n, p.m, p.nnz, p.n - 1, w, 4)
+        r = {"time_to_1e-6_ms": 1e3 * dt, "setup_ms": 1e3 * i.setup_time, "iterations": i.iter,
+             "exit_status": i.exit_status, "attempt_ms": 1e3 * t_att,
+             "roofline": {"bound": "hbm", "achieved": B_att / t_att / 1e9, "peak": peak, "unit": "GB/s",
+                          "frac": B_att / t_att / 1e9 / peak, "algorithmic_bytes_per_attempt": B_att},
+             "criteria_fp64": {"rel_primal": i.l_inf_rel_primal_res, "rel_dual": i.l_inf_rel_dual_res,
+                               "rel_gap": i.rel_gap},
+             "primal_objective": i.pObj, "spmv_lane_nnz": list(i.spmv_lane_nnz)}
+        if pstar is not None:
+            r["objective_error_vs_oracle"] = abs(i.pObj - pstar) / (1.0 + abs(pstar))
+        out[prec] = r
+        sols[prec] = sol
+    x64, x32 = sols["fp64"].primal, sols["fp32"].primal
+    out["fp32_vs_fp64"] = {"max_abs_x_diff": float(np.max(np.abs(x32 - x64))),
+                           "objective_rel_diff": abs(sols["fp32"].info.pObj - sols["fp64"].info.pObj)
+                           / (1.0 + abs(sols["fp64"].info.pObj)),
+                           "speedup": out["fp64"]["time_to_1e-6_ms"] / out["fp32"]["time_to_1e-6_ms"]}
+    return out
+
+
 def differentiable_section(dev, stream):
     """256 mixed SOC + exponential-cone instances (n = 2000, m = 1500, 1% density): the torch
     conic layer's forward (batched solve) against forward + backward (solution-map adjoint),
@@ -477,6 +543,7 @@ def run_ours(args):
                "optimal": sum(1 for s in sols_h if s.info.exit_status == "optimal")}
 
     single = None if args.no_single or rank != 0 else single_instance_section(dev, stream)
+    portfolio = None if args.no_single or rank != 0 else portfolio_section(dev, stream)
     layer = None if args.no_single or rank != 0 else differentiable_section(dev, stream)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -495,7 +562,8 @@ def run_ours(args):
                 "plain_fp64": plain, "speedup_vs_plain_fp64": value / plain["instances_per_s"] / world,
                 "spmv_schedule": schedule,
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-                "cpu_baseline": cpu, "single_instance": single, "differentiable_layer": layer}
+                "cpu_baseline": cpu, "single_instance": single, "portfolio": portfolio,
+                "differentiable_layer": layer}
         print(json.dumps(line), flush=True)
     replicas.finalize(world)
     return 0
