@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
       const int32_t len = A.sl[s];
       const int32_t slot = A.so[s * kSellC + lane];
       T p0 = T(0), p1 = T(0);
-      constexpr int U = sizeof(T) == 4 ? 8 : 4;
+      constexpr int U = sizeof(T) == 4 ? 16 : 4;
       for (int32_t j0 = 0; j0 < len; j0 += U) {
         T v[U];
         uint16_t c[U];
