@@ -332,6 +332,75 @@ __global__ void adj_block_min_kernel(ConeTable T, double* __restrict__ d) {
   }
 }
 
+// One GMRES step's Hessenberg column, a thread per instance still extending its
+// Krylov basis (mask): H(i, j) = h1_i + h2_i for i <= j (the two classical
+// Gram-Schmidt passes), H(j+1, j) = |w|; the instance's earlier Givens
+// rotations applied to the column, a new rotation that zeroes H(j+1, j), the
+// rotated right-hand side gamma and the residual estimate |gamma_{j+1}| / beta0.
+// An instance whose estimate reaches tol (or whose basis breaks down: the
+// current iterate solves the system) leaves the mask, so the next step's
+// kernels skip it.  Layouts: H per instance (mr + 1) x mr row-major, cs / sn
+// per instance mr, gamma per instance mr + 1, the step's dot products at
+// k * ld + i.
+__global__ void adj_givens_kernel(int64_t K, int j, int mr, int ld, uint8_t* __restrict__ mask,
+                                  const double* __restrict__ h1, const double* __restrict__ h2,
+                                  const double* __restrict__ hn, double* __restrict__ H, double* __restrict__ cs,
+                                  double* __restrict__ sn, double* __restrict__ gam,
+                                  const double* __restrict__ beta0, double tol, int32_t* __restrict__ jk,
+                                  int64_t* __restrict__ iters, double* __restrict__ res) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += stride) {
+    if (!mask[k]) continue;
+    double* Hk = H + (size_t)k * (mr + 1) * mr;
+    double* ck = cs + (size_t)k * mr;
+    double* sk = sn + (size_t)k * mr;
+    double* gk = gam + (size_t)k * (mr + 1);
+    const double hnk = sqrt(hn[k * ld]);
+    for (int i = 0; i <= j; ++i) Hk[i * mr + j] = h1[k * ld + i] + h2[k * ld + i];
+    Hk[(j + 1) * mr + j] = hnk;
+    for (int i = 0; i < j; ++i) {
+      const double a0 = Hk[i * mr + j], a1 = Hk[(i + 1) * mr + j];
+      Hk[i * mr + j] = ck[i] * a0 + sk[i] * a1;
+      Hk[(i + 1) * mr + j] = -sk[i] * a0 + ck[i] * a1;
+    }
+    const double a0 = Hk[j * mr + j], a1 = Hk[(j + 1) * mr + j];
+    const double rr = hypot(a0, a1);
+    const double c = rr > 0.0 ? a0 / rr : 1.0, s = rr > 0.0 ? a1 / rr : 0.0;
+    ck[j] = c;
+    sk[j] = s;
+    Hk[j * mr + j] = rr;
+    Hk[(j + 1) * mr + j] = 0.0;
+    const double gj = gk[j];
+    gk[j + 1] = -s * gj;
+    gk[j] = c * gj;
+    jk[k] = j + 1;
+    iters[k]++;
+    res[k] = fabs(gk[j + 1]) / beta0[k];
+    if (res[k] <= tol || hnk <= 1e-300) mask[k] = 0;
+  }
+}
+
+// End of a GMRES cycle, a thread per instance of the cycle (run): the
+// coefficients y = H^{-1} gamma of its jk Krylov vectors by back substitution
+// (coef[k * ld + q], zero for q >= jk).
+__global__ void adj_backsub_kernel(int64_t K, int mr, int ld, const uint8_t* __restrict__ run,
+                                   const int32_t* __restrict__ jk, const double* __restrict__ H,
+                                   const double* __restrict__ gam, double* __restrict__ coef) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K; k += stride) {
+    double* y = coef + k * ld;
+    const int J = run[k] ? jk[k] : 0;
+    for (int q = J; q < ld; ++q) y[q] = 0.0;
+    const double* Hk = H + (size_t)k * (mr + 1) * mr;
+    const double* gk = gam + (size_t)k * (mr + 1);
+    for (int i = J - 1; i >= 0; --i) {
+      double v = gk[i];
+      for (int q = i + 1; q < J; ++q) v -= Hk[i * mr + q] * y[q];
+      y[i] = v / Hk[i * mr + i];
+    }
+  }
+}
+
 // w[i] *= 1 / sqrt(nrm2[k * ld]) on the masked instances' elements (Arnoldi normalisation)
 __global__ void adj_normalize_kernel(int64_t N, int64_t n, const int32_t* __restrict__ ix,
                                      const int32_t* __restrict__ iy, const uint8_t* __restrict__ mask,

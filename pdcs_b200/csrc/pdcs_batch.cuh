@@ -301,6 +301,12 @@ class BatchSolver : public Solver {
     double *dots1 = nullptr, *dots2 = nullptr, *dotsn = nullptr;
     double* dpart = nullptr;  // partial dot products: K x kAdjSplit x 8
     uint8_t* mask = nullptr;
+    // GMRES state per instance on the device: Hessenberg matrix, rotations, rotated
+    // right-hand side, initial residual norm, residual estimate, basis size, steps
+    double *H = nullptr, *cs = nullptr, *sn = nullptr, *gam = nullptr, *beta0 = nullptr, *res = nullptr;
+    int32_t* jk = nullptr;
+    int64_t* iters = nullptr;
+    uint8_t* run = nullptr;
   } adj_;
   static constexpr int kAdjSplit = 16;  // at most this many CTAs per instance in the adjoint's dot products
   void setup_adjoint(int mr);
@@ -2645,7 +2651,18 @@ void BatchSolver::setup_adjoint(int mr) {
     adj_.mask = A.alloc<uint8_t>(K_);
   }
   for (double** v : {&adj_.coef, &adj_.dots1, &adj_.dots2, &adj_.dotsn}) *v = A.alloc<double>((size_t)K_ * (mr + 1));
-  if (!adj_.dpart) adj_.dpart = A.alloc<double>((size_t)K_ * kAdjSplit * 8);
+  adj_.H = A.alloc<double>((size_t)K_ * (mr + 1) * mr);
+  adj_.cs = A.alloc<double>((size_t)K_ * mr);
+  adj_.sn = A.alloc<double>((size_t)K_ * mr);
+  adj_.gam = A.alloc<double>((size_t)K_ * (mr + 1));
+  if (!adj_.dpart) {
+    adj_.dpart = A.alloc<double>((size_t)K_ * kAdjSplit * 8);
+    adj_.beta0 = A.alloc<double>(K_);
+    adj_.res = A.alloc<double>(K_);
+    adj_.jk = A.alloc<int32_t>(K_);
+    adj_.iters = A.alloc<int64_t>(K_);
+    adj_.run = A.alloc<uint8_t>(K_);
+  }
 }
 
 // out = (I - M') u on the masked instances
@@ -2743,13 +2760,17 @@ int BatchSolver::grad(const double* const* dldx, const double* const* dldy, doub
       beta0[k] = std::sqrt(h[k * ld]);
       conv[k] = beta0[k] > 0 ? 0 : 1;
     }
+    double* hb = stage<double>(K);
+    for (int64_t k = 0; k < K; ++k) hb[k] = beta0[k] > 0 ? beta0[k] : 1.0;
+    PDCS_CUDA(cudaMemcpyAsync(adj_.beta0, hb, sizeof(double) * K, cudaMemcpyHostToDevice, s_));
+    PDCS_CUDA(cudaMemsetAsync(adj_.iters, 0, sizeof(int64_t) * K, s_));
   }
   // restarted GMRES: one Arnoldi process per instance, all instances per launch;
-  // classical Gram-Schmidt twice with the coefficients kept on the device
-  std::vector<double> Hh((size_t)K * (mr + 1) * mr), cs((size_t)K * mr), sn((size_t)K * mr), gam((size_t)K * (mr + 1));
-  std::vector<int> jk(K);
-  std::vector<double> coef((size_t)K * ld);
-  auto Hc = [&](int64_t k, int i, int j) -> double& { return Hh[((size_t)k * (mr + 1) + i) * mr + j]; };
+  // classical Gram-Schmidt twice, the Hessenberg column, Givens rotations and the
+  // back substitution on the device (adj_givens_kernel, adj_backsub_kernel), so a
+  // step needs no host round trip; the host looks at the mask every kCheck steps
+  constexpr int kCheck = 8;
+  const int kg = (int)std::max<int64_t>(1, std::min<int64_t>((K + kThreads - 1) / kThreads, 148));
   double* V = adj_.V;
   int64_t total_it = 0;
   bool first = true;
@@ -2771,24 +2792,35 @@ int BatchSolver::grad(const double* const* dldx, const double* const* dldy, doub
     adj_normalize_kernel<<<grid_for(N), kThreads, 0, s_>>>(N, n_, ix_, iy_, adj_.mask, adj_.dotsn, ld, V);
     kernels_++;
     PDCS_CUDA(cudaStreamSynchronize(s_));
+    double* hg = stage<double>(K);  // gamma = (beta, 0, ..., 0) per instance
     for (int64_t k = 0; k < K; ++k) {
+      hg[k] = 0.0;
       if (!run[k]) continue;
       const double beta = std::sqrt(hb[k * ld]);
       res[k] = beta / beta0[k];
-      jk[k] = 0;
       if (beta <= tol * beta0[k]) {
         conv[k] = 1;
         run[k] = 0;
         continue;
       }
-      gam[(size_t)k * (mr + 1)] = beta;
-      for (int i = 1; i <= mr; ++i) gam[(size_t)k * (mr + 1) + i] = 0.0;
+      hg[k] = beta;
     }
     if (!any(run)) break;
-    std::vector<uint8_t> arn = run;  // instances still extending their Krylov basis this cycle
+    {  // the cycle's instances: the Arnoldi mask and the back substitution's
+      PDCS_CUDA(cudaMemsetAsync(adj_.gam, 0, sizeof(double) * K * (mr + 1), s_));
+      PDCS_CUDA(cudaMemcpy2DAsync(adj_.gam, sizeof(double) * (mr + 1), hg, sizeof(double), sizeof(double), K,
+                                  cudaMemcpyHostToDevice, s_));
+      upload_mask8(run);
+      PDCS_CUDA(cudaMemcpyAsync(adj_.run, adj_.mask, K, cudaMemcpyDeviceToDevice, s_));
+      PDCS_CUDA(cudaMemsetAsync(adj_.jk, 0, sizeof(int32_t) * K, s_));
+    }
     for (int j = 0; j < mr && total_it < maxit; ++j) {
-      if (!any(arn)) break;
-      upload_mask8(arn);
+      if (j > 0 && j % kCheck == 0) {  // every instance done extending its basis: end the cycle
+        uint8_t* hm = stage<uint8_t>(K);
+        PDCS_CUDA(cudaMemcpyAsync(hm, adj_.mask, K, cudaMemcpyDeviceToHost, s_));
+        PDCS_CUDA(cudaStreamSynchronize(s_));
+        if (!std::any_of(hm, hm + K, [](uint8_t v) { return v != 0; })) break;
+      }
       double* W = V + (size_t)(j + 1) * N;
       apply_AT(V + (size_t)j * N, W, adj_.mask);
       dots(adj_.mask, V, j + 1, W, adj_.dots1);
@@ -2799,61 +2831,32 @@ int BatchSolver::grad(const double* const* dldx, const double* const* dldy, doub
                                                           -1.0, W);
       dots(adj_.mask, W, 1, W, adj_.dotsn);
       adj_normalize_kernel<<<grid_for(N), kThreads, 0, s_>>>(N, n_, ix_, iy_, adj_.mask, adj_.dotsn, ld, W);
-      kernels_ += 3;
-      const double* h1 = fetch(adj_.dots1);
-      const double* h2 = fetch(adj_.dots2);
-      const double* hn = fetch(adj_.dotsn);
-      PDCS_CUDA(cudaStreamSynchronize(s_));
+      adj_givens_kernel<<<kg, kThreads, 0, s_>>>(K, j, mr, ld, adj_.mask, adj_.dots1, adj_.dots2, adj_.dotsn, adj_.H,
+                                                 adj_.cs, adj_.sn, adj_.gam, adj_.beta0, tol, adj_.jk, adj_.iters,
+                                                 adj_.res);
+      kernels_ += 4;
       total_it++;
-      for (int64_t k = 0; k < K; ++k) {
-        if (!arn[k]) continue;
-        const double hnk = std::sqrt(hn[k * ld]);
-        for (int i = 0; i <= j; ++i) Hc(k, i, j) = h1[k * ld + i] + h2[k * ld + i];
-        Hc(k, j + 1, j) = hnk;
-        // previous rotations, then a new one that zeroes H(j+1, j)
-        for (int i = 0; i < j; ++i) {
-          const double a0 = Hc(k, i, j), a1 = Hc(k, i + 1, j);
-          Hc(k, i, j) = cs[k * mr + i] * a0 + sn[k * mr + i] * a1;
-          Hc(k, i + 1, j) = -sn[k * mr + i] * a0 + cs[k * mr + i] * a1;
-        }
-        const double a0 = Hc(k, j, j), a1 = Hc(k, j + 1, j);
-        const double rr = std::hypot(a0, a1);
-        const double c = rr > 0 ? a0 / rr : 1.0, sv = rr > 0 ? a1 / rr : 0.0;
-        cs[k * mr + j] = c;
-        sn[k * mr + j] = sv;
-        Hc(k, j, j) = rr;
-        Hc(k, j + 1, j) = 0.0;
-        double& gj = gam[(size_t)k * (mr + 1) + j];
-        gam[(size_t)k * (mr + 1) + j + 1] = -sv * gj;
-        gj = c * gj;
-        jk[k] = j + 1;
-        iters[k]++;
-        res[k] = std::fabs(gam[(size_t)k * (mr + 1) + j + 1]) / beta0[k];
-        if (res[k] <= tol || hnk <= 1e-300) arn[k] = 0;  // converged (or breakdown: exact solution)
-      }
     }
-    // u += V y, y = H^{-1} gamma (back substitution per instance)
-    std::fill(coef.begin(), coef.end(), 0.0);
+    // u += V y, y = H^{-1} gamma (back substitution per instance on the device)
+    adj_backsub_kernel<<<kg, kThreads, 0, s_>>>(K, mr, ld, adj_.run, adj_.jk, adj_.H, adj_.gam, adj_.coef);
+    kernels_++;
+    int32_t* hj = stage<int32_t>(K);
+    PDCS_CUDA(cudaMemcpyAsync(hj, adj_.jk, sizeof(int32_t) * K, cudaMemcpyDeviceToHost, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
     int jmax = 0;
-    for (int64_t k = 0; k < K; ++k) {
-      if (!run[k] || jk[k] == 0) continue;
-      const int J = jk[k];
-      jmax = std::max(jmax, J);
-      for (int i = J - 1; i >= 0; --i) {
-        double v = gam[(size_t)k * (mr + 1) + i];
-        for (int q = i + 1; q < J; ++q) v -= Hc(k, i, q) * coef[k * ld + q];
-        coef[k * ld + i] = v / Hc(k, i, i);
-      }
-    }
+    for (int64_t k = 0; k < K; ++k)
+      if (run[k]) jmax = std::max(jmax, (int)hj[k]);
     if (jmax > 0) {
-      upload_mask8(run);
-      double* h = stage<double>((size_t)K * ld);
-      std::memcpy(h, coef.data(), sizeof(double) * K * ld);
-      PDCS_CUDA(cudaMemcpyAsync(adj_.coef, h, sizeof(double) * K * ld, cudaMemcpyHostToDevice, s_));
-      adj_combine_kernel<<<grid_for(N), kThreads, 0, s_>>>(N, n_, ix_, iy_, adj_.mask, V, N, jmax, adj_.coef, ld, 1.0,
+      adj_combine_kernel<<<grid_for(N), kThreads, 0, s_>>>(N, n_, ix_, iy_, adj_.run, V, N, jmax, adj_.coef, ld, 1.0,
                                                           adj_.u);
       kernels_++;
     }
+  }
+  {
+    int64_t* hi = stage<int64_t>(K);
+    PDCS_CUDA(cudaMemcpyAsync(hi, adj_.iters, sizeof(int64_t) * K, cudaMemcpyDeviceToHost, s_));
+    PDCS_CUDA(cudaStreamSynchronize(s_));
+    for (int64_t k = 0; k < K; ++k) iters[k] = hi[k];
   }
   // true relative residuals |g - A u| / |g|
   {
