@@ -710,23 +710,114 @@ void BatchSolver::merge() {
   P = mp;
 }
 
+// Host -> device copy of many pageable host segments into one contiguous
+// device range.  A copy from pageable memory is staged by the driver one
+// buffer at a time; here host threads gather the segments into pinned chunks
+// while the copy engine moves the chunks filled before them.  Every thread
+// owns two pinned chunks of a per-device ring, kept for the life of the
+// process (kStageThreads x 2 x kStageChunk bytes, allocated on the first
+// batch upload of a device) and guarded by a mutex, so concurrent batch
+// setups on one device take turns.  The copies run on stream s; a chunk is
+// refilled only after the event of its previous copy has completed.
+struct HostSeg {
+  const void* p;
+  size_t bytes;
+};
+constexpr int kStageThreads = 8;
+constexpr size_t kStageChunk = size_t(8) << 20;
+
+class StageRing {
+ public:
+  static StageRing& of_current_device() {
+    static std::mutex mu;
+    static std::map<int, StageRing*> rings;
+    int dev = 0;
+    PDCS_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    StageRing*& r = rings[dev];
+    if (!r) r = new StageRing();  // kept until exit: pinned buffers are process-wide
+    return *r;
+  }
+  // Copies the concatenation of segs (total bytes) to dst.
+  void upload(void* dst, const std::vector<HostSeg>& segs, cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(mu_);
+    std::vector<size_t> pre(segs.size() + 1, 0);
+    for (size_t i = 0; i < segs.size(); ++i) pre[i + 1] = pre[i] + segs[i].bytes;
+    const size_t total = pre.back();
+    if (total == 0) return;
+    const size_t nchunks = (total + kStageChunk - 1) / kStageChunk;
+    const int nth = (int)std::min<size_t>(kStageThreads, nchunks);
+    if (!buf_[0]) {
+      for (int i = 0; i < 2 * kStageThreads; ++i) {
+        PDCS_CUDA(cudaHostAlloc(&buf_[i], kStageChunk, cudaHostAllocPortable));
+        PDCS_CUDA(cudaEventCreateWithFlags(&ev_[i], cudaEventDisableTiming));
+        PDCS_CUDA(cudaEventRecord(ev_[i], s));
+      }
+    }
+    int dev = 0;
+    PDCS_CUDA(cudaGetDevice(&dev));
+    std::exception_ptr err = nullptr;
+    std::mutex emu;
+    auto work = [&](int t) {
+      try {
+        PDCS_CUDA(cudaSetDevice(dev));
+        for (size_t c = (size_t)t, it = 0; c < nchunks; c += (size_t)nth, ++it) {
+          const int slot = 2 * t + (int)(it & 1);
+          PDCS_CUDA(cudaEventSynchronize(ev_[slot]));  // its previous copy has left the chunk
+          const size_t a = c * kStageChunk, b = std::min(total, a + kStageChunk);
+          size_t i = (size_t)(std::upper_bound(pre.begin(), pre.end(), a) - pre.begin()) - 1;
+          unsigned char* out = static_cast<unsigned char*>(buf_[slot]);
+          for (size_t pos = a; pos < b; ++i) {
+            const size_t s0 = pos - pre[i], len = std::min(b, pre[i + 1]) - pos;
+            if (len) std::memcpy(out + (pos - a), static_cast<const unsigned char*>(segs[i].p) + s0, len);
+            pos += len;
+          }
+          PDCS_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(dst) + a, out, b - a, cudaMemcpyHostToDevice, s));
+          PDCS_CUDA(cudaEventRecord(ev_[slot], s));
+        }
+      } catch (...) {
+        std::lock_guard<std::mutex> lk(emu);
+        err = std::current_exception();
+      }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nth; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+    if (err) std::rethrow_exception(err);
+  }
+
+ private:
+  std::mutex mu_;
+  void* buf_[2 * kStageThreads] = {};
+  cudaEvent_t ev_[2 * kStageThreads] = {};
+};
+
 // The merged CSR of G, assembled on the device: every instance's column
 // indices and values are uploaded as they are (concatenated in instance
-// order), then merge_cols_kernel moves each merged row's nonzeros into place
-// with the columns mapped to their merged positions (and checked against the
-// instance's column count).
+// order, through the pinned staging ring), then merge_cols_kernel moves each
+// merged row's nonzeros into place with the columns mapped to their merged
+// positions (and checked against the instance's column count).
 void BatchSolver::upload_matrix(int32_t* g_rp, int32_t* g_ci, double* g_v) {
   const int64_t K = K_;
   PDCS_CUDA(cudaMemcpyAsync(g_rp, h_rp_.data(), sizeof(int32_t) * (m_ + 1), cudaMemcpyHostToDevice, s_));
   if (nnz_ == 0) return;
   int32_t* ci_in = A.alloc<int32_t>(nnz_);
   double* v_in = A.alloc<double>(nnz_);
-  for (int64_t k = 0; k < K; ++k) {
-    const pdcs_problem& q = probs_[k];
-    if (!q.nnz) continue;
-    const int64_t o = q.G_rowptr[0];
-    PDCS_CUDA(cudaMemcpyAsync(ci_in + nnz_off_[k], q.G_colind + o, sizeof(int32_t) * q.nnz, cudaMemcpyHostToDevice, s_));
-    PDCS_CUDA(cudaMemcpyAsync(v_in + nnz_off_[k], q.G_val + o, sizeof(double) * q.nnz, cudaMemcpyHostToDevice, s_));
+  {
+    std::vector<HostSeg> sci, sv;
+    sci.reserve(K);
+    sv.reserve(K);
+    for (int64_t k = 0; k < K; ++k) {
+      const pdcs_problem& q = probs_[k];
+      if (!q.nnz) continue;
+      const int64_t o = q.G_rowptr[0];
+      sci.push_back({q.G_colind + o, sizeof(int32_t) * (size_t)q.nnz});
+      sv.push_back({q.G_val + o, sizeof(double) * (size_t)q.nnz});
+    }
+    StageRing& ring = StageRing::of_current_device();
+    ring.upload(ci_in, sci, s_);  // nnz_off_ is the running sum of the instances' nnz in this order
+    ring.upload(v_in, sv, s_);
   }
   std::vector<int64_t> ncol(K);
   for (int64_t k = 0; k < K; ++k) ncol[k] = probs_[k].n;

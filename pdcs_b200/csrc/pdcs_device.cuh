@@ -128,7 +128,15 @@ __device__ __forceinline__ double grp_bcast(double v, int g) { return __shfl_syn
 // projection, NaN = none; NULL = no warm start).  Q is concave increasing, so
 // from a start above the root one Newton step lands at or below it; from
 // there the iterates climb monotonically as in warp_soc_reg.
+__device__ inline void group_soc_reg_w(double& v, double w, int d, bool weighted, int g, double ws_in, double* ws);
 __device__ inline void group_soc_reg(double& v, double w, int d, bool weighted, int g, double* ws) {
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  group_soc_reg_w(v, w, d, weighted, g, (ws && (threadIdx.x & (g - 1)) == 0) ? *ws : nan, ws);
+}
+// The same with the warm start already loaded (ws_in: lane 0 of the group's
+// value, NaN for none; ws: where to store the new root, NULL for nowhere), so a
+// caller can issue that load together with its other loads.
+__device__ inline void group_soc_reg_w(double& v, double w, int d, bool weighted, int g, double ws_in, double* ws) {
   const int gl = threadIdx.x & (g - 1);
   const bool act = gl < d;
   const double scale = grp_max(act ? fabs(v) : 0.0, g);
@@ -151,7 +159,7 @@ __device__ inline void group_soc_reg(double& v, double w, int d, bool weighted, 
   const double a = 1.0 + D * D;
   const double s_lo = fmax(t, 0.0);
   double s = s_lo;
-  double sw = (newton && ws && gl == 0) ? *ws : __longlong_as_double(0x7ff8000000000000ll);
+  double sw = (newton && gl == 0) ? ws_in : __longlong_as_double(0x7ff8000000000000ll);
   sw = grp_bcast(sw, g) / sc;
   bool first = newton && isfinite(sw) && sw > s_lo;
   if (first) s = sw;

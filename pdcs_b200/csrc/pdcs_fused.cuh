@@ -31,6 +31,9 @@ constexpr int kFusedWarps = kFusedThreads / 32;
 // SOC / RSOC tables, 2 (128) when the exponential-cone root solve is compiled in
 constexpr int kFusedMinCtas = 4, kFusedMinCtasExp = 2;
 constexpr int kSellC = 32;  // rows per slice
+// rows a thread updates at once in the step, their loads in flight together (2 spills
+// registers under the 64-register budget and measured slower)
+constexpr int kFusedRows = 1;
 
 struct FusedTile {
   int32_t inst;    // instance
@@ -61,10 +64,11 @@ struct FusedCsr {
   int32_t max_rows;       // largest tile's rows (products in shared memory)
 };
 
-// ---- fused ops: z(j, a, b) is the value before the projection given the
-// row's products (a, b: G'y for the primal step; G x, G x_lag for the dual
-// one); fin(j, p, a, b, acc) stores the projection's result and adds the
-// control step's terms.
+// ---- fused ops.  In is what the update reads of row j (load), z(q, a, b)
+// the value before the projection given the row's products (a, b: G'y for
+// the primal step; G x, G x_lag for the dual one); Fin is what the store of
+// the result reads (load_fin, or fin_of an In), fin(j, f, p, a, b, acc)
+// stores the projection's result p and adds the control step's terms.
 
 // FP32 bulk, primal: z = xa + dx_lag + tau_k (qa + G' dy_lag), dx = P(z) - xa;
 // acc0 += (dx - dx_lag)^2
@@ -76,12 +80,23 @@ struct FusedPrimal32 {
   const double* ps;
   const uint8_t* mask;
   double sk = 0.0;
+  struct In {
+    double xa, qa;
+    float dxl;
+  };
+  struct Fin {
+    double xa;
+    float dxl;
+  };
   __device__ void begin(int64_t k) { sk = ps[k]; }
-  __device__ double z(int64_t j, float a, float) const { return xa[j] + (double)dxp[j].y + sk * (qa[j] + (double)a); }
-  __device__ void fin(int64_t j, double p, float, float, double* acc) const {
-    const float d = (float)(p - xa[j]);
+  __device__ In load(int64_t j) const { return {xa[j], qa[j], dxp[j].y}; }
+  __device__ double z(const In& q, float a, float) const { return q.xa + (double)q.dxl + sk * (q.qa + (double)a); }
+  __device__ Fin load_fin(int64_t j) const { return {xa[j], dxp[j].y}; }
+  __device__ static Fin fin_of(const In& q) { return {q.xa, q.dxl}; }
+  __device__ void fin(int64_t j, const Fin& f, double p, float, float, double* acc) const {
+    const float d = (float)(p - f.xa);
     dxp[j].x = d;
-    const double s = (double)d - (double)dxp[j].y;
+    const double s = (double)d - (double)f.dxl;
     acc[0] += s * s;
   }
 };
@@ -97,14 +112,25 @@ struct FusedDual32 {
   const double* ds;
   const uint8_t* mask;
   double sk = 0.0;
+  struct In {
+    double ya, ra;
+    float dyl;
+  };
+  struct Fin {
+    double ya;
+    float dyl;
+  };
   __device__ void begin(int64_t k) { sk = ds[k]; }
-  __device__ double z(int64_t i, float g, float gl) const {
-    return ya[i] + (double)dyl[i] - sk * (ra[i] + (2.0 * (double)g - (double)gl));
+  __device__ In load(int64_t i) const { return {ya[i], ra[i], dyl[i]}; }
+  __device__ double z(const In& q, float g, float gl) const {
+    return q.ya + (double)q.dyl - sk * (q.ra + (2.0 * (double)g - (double)gl));
   }
-  __device__ void fin(int64_t i, double p, float g, float gl, double* acc) const {
-    const float d = (float)(p - ya[i]);
+  __device__ Fin load_fin(int64_t i) const { return {ya[i], dyl[i]}; }
+  __device__ static Fin fin_of(const In& q) { return {q.ya, q.dyl}; }
+  __device__ void fin(int64_t i, const Fin& f, double p, float g, float gl, double* acc) const {
+    const float d = (float)(p - f.ya);
     dy[i] = d;
-    const double s = (double)d - (double)dyl[i];
+    const double s = (double)d - (double)f.dyl;
     acc[0] += s * s;
     acc[1] += s * ((double)g - (double)gl);
   }
@@ -119,11 +145,20 @@ struct FusedPrimal64 {
   const double* ps;
   const uint8_t* mask;
   double sk = 0.0;
+  struct In {
+    double xl, c;
+  };
+  struct Fin {
+    double xl;
+  };
   __device__ void begin(int64_t k) { sk = ps[k]; }
-  __device__ double z(int64_t j, double a, double) const { return xl[j] + sk * (a - c[j]); }
-  __device__ void fin(int64_t j, double p, double, double, double* acc) const {
+  __device__ In load(int64_t j) const { return {xl[j], c[j]}; }
+  __device__ double z(const In& q, double a, double) const { return q.xl + sk * (a - q.c); }
+  __device__ Fin load_fin(int64_t j) const { return {xl[j]}; }
+  __device__ static Fin fin_of(const In& q) { return {q.xl}; }
+  __device__ void fin(int64_t j, const Fin& f, double p, double, double, double* acc) const {
     out[j] = p;
-    const double d = p - xl[j];
+    const double d = p - f.xl;
     acc[0] += d * d;
   }
 };
@@ -138,15 +173,46 @@ struct FusedDual64 {
   const double* ds;
   const uint8_t* mask;
   double sk = 0.0;
+  struct In {
+    double yl, h;
+  };
+  struct Fin {
+    double yl;
+  };
   __device__ void begin(int64_t k) { sk = ds[k]; }
-  __device__ double z(int64_t i, double g, double gl) const { return yl[i] - sk * ((2.0 * g - gl) - h[i]); }
-  __device__ void fin(int64_t i, double p, double g, double gl, double* acc) const {
+  __device__ In load(int64_t i) const { return {yl[i], h[i]}; }
+  __device__ double z(const In& q, double g, double gl) const { return q.yl - sk * ((2.0 * g - gl) - q.h); }
+  __device__ Fin load_fin(int64_t i) const { return {yl[i]}; }
+  __device__ static Fin fin_of(const In& q) { return {q.yl}; }
+  __device__ void fin(int64_t i, const Fin& f, double p, double g, double gl, double* acc) const {
     out[i] = p;
-    const double d = p - yl[i];
+    const double d = p - f.yl;
     acc[0] += d * d;
     acc[1] += d * (g - gl);
   }
 };
+
+// Asynchronous global -> shared copy of B = 4, 8 or 16 bytes (cp.async, cached
+// in L1), both addresses aligned to B; cp_async_wait_all waits for this thread's
+// copies (a barrier then makes every thread's visible).
+template <int B>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  static_assert(B == 4 || B == 8 || B == 16, "cp.async size");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Shared memory before the products: the staged column segment, or (after the
+// row pass) two doubles per tile row, whichever is larger.
+template <class T, int NV>
+__host__ __device__ inline size_t fused_stage_bytes(const FusedCsr& A) {
+  const size_t a = sizeof(TileVal<T, NV>) * (size_t)(A.max_cols > 1 ? A.max_cols : 1);
+  const size_t b = 2 * sizeof(double) * (size_t)(A.max_rows > 1 ? A.max_rows : 1);
+  return ((a > b ? a : b) + 15) & ~size_t(15);
+}
 
 // The fused tile kernel.  T: matrix / product type; NV: 1 (G' y) or kPair /
 // 2 (G applied to two vectors); EXP: compile the exponential-cone path.
@@ -160,8 +226,12 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
   using V = TileVal<T, NV>;
   constexpr int NP = NV == 1 ? 1 : 2;
   extern __shared__ __align__(16) unsigned char fused_smem[];
-  const size_t stage = (sizeof(V) * (size_t)A.max_cols + 15) & ~size_t(15);
+  const size_t stage = fused_stage_bytes<T, NV>(A);
   V* sx = reinterpret_cast<V*>(fused_smem);
+  // after the row pass the staged segment is dead: the step keeps each row's value
+  // before / after the projection (zs) and its cone scaling (ss) there
+  double* zs = reinterpret_cast<double*>(fused_smem);
+  double* ss = zs + A.max_rows;
   T* pr0 = reinterpret_cast<T*>(fused_smem + stage);
   T* pr1 = pr0 + A.max_rows;
   __shared__ int64_t run_row[kMaxRuns];
@@ -179,11 +249,22 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
       run_row[threadIdx.x] = A.rows.start[k * kMaxRuns + threadIdx.x];
       run_ord[threadIdx.x] = A.rloc[k * kMaxRuns + threadIdx.x];
     }
+    // the instance's column segment, copied to shared memory asynchronously (every copy
+    // in flight at once, no registers held)
     for (int r = 0; r < kMaxRuns; ++r) {
       const int64_t s0 = A.cols.start[k * kMaxRuns + r], L = A.cols.len[k * kMaxRuns + r];
       V* dst = sx + A.cloc[k * kMaxRuns + r];
-      for (int64_t i = threadIdx.x; i < L; i += kFusedThreads) dst[i] = tile_load<T, NV>(x0, x1, s0 + i);
+      if constexpr (NV == 2) {
+        for (int64_t i = threadIdx.x; i < L; i += kFusedThreads) {
+          cp_async<sizeof(T)>(&dst[i].x, x0 + s0 + i);
+          cp_async<sizeof(T)>(&dst[i].y, x1 + s0 + i);
+        }
+      } else {
+        const V* src = reinterpret_cast<const V*>(x0) + s0;
+        for (int64_t i = threadIdx.x; i < L; i += kFusedThreads) cp_async<sizeof(V)>(dst + i, src + i);
+      }
     }
+    cp_async_wait_all();
     __syncthreads();
     // ---- the tile's rows, SELL-32: lane = row, one coalesced load per column ----
     for (int64_t s = tl.s0 + warp; s < tl.s1; s += kFusedWarps) {
@@ -218,7 +299,7 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
       }
     }
     __syncthreads();
-    // ---- the step of the tile's rows ----
+    // ---- the step of the tile's rows, in three passes over shared memory ----
     op.begin(k);
     double acc[Op::NACC];
 #pragma unroll
@@ -229,73 +310,132 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
         if (o >= run_ord[t]) r = t;
       return run_row[r] + (o - run_ord[r]);
     };
-    for (int i = threadIdx.x; i < tl.ew; i += kFusedThreads) {  // elementwise rows
-      const int64_t j = merged(tl.o0 + i);
-      int32_t kind = CT.seg_kind[0];
-      for (int s = 1; s < CT.nseg; ++s)
-        if (j >= CT.seg_start[s]) kind = CT.seg_kind[s];
-      const T a = pr0[i], b = NP == 2 ? pr1[i] : T(0);
-      const double p = elem_proj(kind, op.z(j, a, b), j, CT);
-      op.fin(j, p, a, b, acc);
+    const int nr = tl.o1 - tl.o0;
+    // (a) every row's update in row order, kFusedRows rows per thread with their loads
+    // issued together: elementwise rows are projected and stored here; a cone row's
+    // value before the projection (and its scaling) goes to shared memory
+    for (int i0 = threadIdx.x; i0 < nr; i0 += kFusedRows * kFusedThreads) {
+      int64_t jj[kFusedRows];
+      typename Op::In q[kFusedRows];
+      double l[kFusedRows], h[kFusedRows];
+      int32_t kd[kFusedRows];
+#pragma unroll
+      for (int u = 0; u < kFusedRows; ++u) {
+        const int i = i0 + u * kFusedThreads;
+        jj[u] = i < nr ? merged(tl.o0 + i) : -1;
+        kd[u] = -1;
+        l[u] = 1.0;
+        h[u] = 1.0;
+        if (jj[u] < 0) continue;
+        q[u] = op.load(jj[u]);
+        if (i < tl.ew) {
+          kd[u] = CT.seg_kind[0];
+          for (int g = 1; g < CT.nseg; ++g)
+            if (jj[u] >= CT.seg_start[g]) kd[u] = CT.seg_kind[g];
+          if (kd[u] == PK_BOX) {
+            l[u] = CT.lo[jj[u]];
+            h[u] = CT.hi[jj[u]];
+          }
+        } else if (CT.S) {
+          l[u] = CT.S[jj[u]];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kFusedRows; ++u) {
+        const int i = i0 + u * kFusedThreads;
+        if (jj[u] < 0) continue;
+        const T a = pr0[i], b = NP == 2 ? pr1[i] : T(0);
+        const double z = op.z(q[u], a, b);
+        if (kd[u] >= 0) {
+          const double p = kd[u] == PK_ZERO ? 0.0 : kd[u] == PK_NONNEG ? fmax(z, 0.0)
+                           : kd[u] == PK_BOX ? fmin(fmax(z, l[u]), h[u]) : z;
+          op.fin(jj[u], Op::fin_of(q[u]), p, a, b, acc);
+        } else {
+          zs[i] = z;
+          ss[i] = l[u];
+        }
+      }
     }
-    for (int64_t t = tl.t0 + warp; t < tl.t1; t += kFusedWarps) {  // SOC / RSOC blocks, lane groups
-      const int4 tk = A.task[t];
-      const int g = tk.z, gl = lane & (g - 1);
-      const bool have = lane / g < tk.y;
-      int4 rc = make_int4(0, 0, 0, 0);
-      if (have) rc = A.crec[tk.x + lane / g];
-      const int64_t st = rc.x;
-      const int d = have ? (rc.y & 0x3fffffff) : 0;
-      const bool rsoc = have && (rc.y >> 30) != 0;
-      const int li = rc.w + gl;
-      const T a = gl < d ? pr0[li] : T(0), b = (gl < d && NP == 2) ? pr1[li] : T(0);
-      double v = gl < d ? op.z(st + gl, a, b) : 0.0;
-      double w = 1.0;
-      if (CT.S && gl < d) {
-        const double* S = CT.S + st;
-        if (rsoc) w = (gl >= 2) ? sqrt(S[0] * S[1]) / S[gl] : 1.0;
-        else w = (gl >= 1) ? S[0] / S[gl] : 1.0;
+    __syncthreads();
+    // (b) SOC / RSOC blocks in lane groups, on the values in shared memory; the next
+    // task's descriptor and record are in flight while a task is projected
+    {
+      int64_t t = tl.t0 + warp;
+      int4 tkn = make_int4(0, 0, 2, 0);
+      if (t < tl.t1) tkn = A.task[t];
+      for (; t < tl.t1; t += kFusedWarps) {
+        const int4 tk = tkn;
+        const int g = tk.z, gl = lane & (g - 1);
+        const bool have = lane / g < tk.y;
+        int4 rc = make_int4(0, 0, 0, 0);
+        if (have) rc = A.crec[tk.x + lane / g];
+        if (t + kFusedWarps < tl.t1) tkn = A.task[t + kFusedWarps];
+        const int d = have ? (rc.y & 0x3fffffff) : 0;
+        const bool rsoc = have && (rc.y >> 30) != 0;
+        const int li = rc.w + gl;
+        double* wsp = (have && CT.soc_ws) ? CT.soc_ws + rc.z : nullptr;
+        const double wsv = (wsp && gl == 0) ? *wsp : __longlong_as_double(0x7ff8000000000000ll);
+        double v = gl < d ? zs[li] : 0.0;
+        double w = 1.0;
+        if (CT.S && gl < d) {
+          if (rsoc) w = (gl >= 2) ? sqrt(ss[rc.w] * ss[rc.w + 1]) / ss[li] : 1.0;
+          else w = (gl >= 1) ? ss[rc.w] / ss[li] : 1.0;
+        }
+        const bool weighted = grp_max(w != 1.0 ? 1.0 : 0.0, g) != 0.0;
+        {  // RSOC: rotate the first two elements to the SOC form (every lane shuffles)
+          const double p0 = __shfl_sync(kFull, v, 0, g), q0 = __shfl_sync(kFull, v, 1, g);
+          if (rsoc && gl == 0) v = (p0 + q0) * r2;
+          if (rsoc && gl == 1) v = (p0 - q0) * r2;
+        }
+        group_soc_reg_w(v, w, d, weighted, g, wsv, wsp);
+        {
+          const double a0 = __shfl_sync(kFull, v, 0, g), b0 = __shfl_sync(kFull, v, 1, g);
+          if (rsoc && gl == 0) v = (a0 + b0) * r2;
+          if (rsoc && gl == 1) v = (a0 - b0) * r2;
+        }
+        if (gl < d) zs[li] = v;
       }
-      const bool weighted = grp_max(w != 1.0 ? 1.0 : 0.0, g) != 0.0;
-      {  // RSOC: rotate the first two elements to the SOC form (every lane shuffles)
-        const double p0 = __shfl_sync(kFull, v, 0, g), q0 = __shfl_sync(kFull, v, 1, g);
-        if (rsoc && gl == 0) v = (p0 + q0) * r2;
-        if (rsoc && gl == 1) v = (p0 - q0) * r2;
-      }
-      group_soc_reg(v, w, d, weighted, g, (have && CT.soc_ws) ? CT.soc_ws + rc.z : nullptr);
-      {
-        const double a0 = __shfl_sync(kFull, v, 0, g), b0 = __shfl_sync(kFull, v, 1, g);
-        if (rsoc && gl == 0) v = (a0 + b0) * r2;
-        if (rsoc && gl == 1) v = (a0 - b0) * r2;
-      }
-      if (gl < d) op.fin(st + gl, v, a, b, acc);
     }
     if constexpr (EXP) {
       for (int64_t e = tl.x0 + threadIdx.x; e < tl.x1; e += kFusedThreads) {  // exponential cones
         const int4 xr = A.xrec[e];
-        const int64_t j = xr.x, kk = xr.y;
+        const int64_t kk = xr.y;
         const int li = xr.z;
         const bool first = kk < CT.exp_count;
         const int32_t kind = first ? CT.exp_kind : CT.dexp_kind;
-        T pa[3], pb[3];
         double zz[3];
 #pragma unroll
-        for (int u = 0; u < 3; ++u) {
-          pa[u] = pr0[li + u];
-          pb[u] = NP == 2 ? pr1[li + u] : T(0);
-          zz[u] = op.z(j + u, pa[u], pb[u]);
-        }
+        for (int u = 0; u < 3; ++u) zz[u] = zs[li + u];
         double S0 = 1.0, S1 = 1.0, S2 = 1.0;
         if (CT.S) {
-          S0 = CT.S[j];
-          S1 = CT.S[j + 1];
-          S2 = CT.S[j + 2];
+          S0 = ss[li];
+          S1 = ss[li + 1];
+          S2 = ss[li + 2];
         }
         double* ws = CT.rho_ws ? CT.rho_ws + kk : nullptr;
         if (kind == PK_EXP) proj_exp_scaled_dev(zz[0], zz[1], zz[2], S0, S1, S2, ws);
         else proj_dexp_scaled_dev(zz[0], zz[1], zz[2], S0, S1, S2, ws);
 #pragma unroll
-        for (int u = 0; u < 3; ++u) op.fin(j + u, zz[u], pa[u], pb[u], acc);
+        for (int u = 0; u < 3; ++u) zs[li + u] = zz[u];
+      }
+    }
+    __syncthreads();
+    // (c) the cone rows' results, stored in row order with the control step's terms
+    for (int i0 = tl.ew + threadIdx.x; i0 < nr; i0 += kFusedRows * kFusedThreads) {
+      int64_t jj[kFusedRows];
+      typename Op::Fin f[kFusedRows];
+#pragma unroll
+      for (int u = 0; u < kFusedRows; ++u) {
+        const int i = i0 + u * kFusedThreads;
+        jj[u] = i < nr ? merged(tl.o0 + i) : -1;
+        if (jj[u] >= 0) f[u] = op.load_fin(jj[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < kFusedRows; ++u) {
+        const int i = i0 + u * kFusedThreads;
+        if (jj[u] < 0) continue;
+        const T a = pr0[i], b = NP == 2 ? pr1[i] : T(0);
+        op.fin(jj[u], f[u], zs[i], a, b, acc);
       }
     }
     // ---- the tile's partial sums, in a fixed order ----
@@ -342,8 +482,7 @@ __global__ void sell_fill_kernel(int64_t nslices, const int64_t* __restrict__ sb
 
 template <class T, int NV>
 inline size_t fused_smem_bytes(const FusedCsr& A) {
-  const size_t stage = (sizeof(TileVal<T, NV>) * (size_t)std::max(A.max_cols, 1) + 15) & ~size_t(15);
-  return stage + sizeof(T) * (NV == 1 ? 1 : 2) * (size_t)std::max(A.max_rows, 1);
+  return fused_stage_bytes<T, NV>(A) + sizeof(T) * (NV == 1 ? 1 : 2) * (size_t)std::max(A.max_rows, 1);
 }
 
 // Raise the kernel's dynamic shared memory limit to what A needs (per device,

@@ -104,7 +104,7 @@ class _Holder:
         return a.ctypes.data if a.size else None
 
     def i64(self, a):
-        a = np.ascontiguousarray(np.asarray(list(a), dtype=np.int64))
+        a = np.ascontiguousarray(np.asarray(a if isinstance(a, np.ndarray) else list(a), dtype=np.int64).reshape(-1))
         self.keep.append(a)
         return a.ctypes.data if a.size else None
 
@@ -137,15 +137,14 @@ def _problem_struct(hold: _Holder, *, n, m, nb, c, G, h, mGzero, mGnonnegative, 
     else:
         rowptr, colind, val = G  # (crow_indices, col_indices, values) tensors on the device
         nnz = int(val.numel())
-    if m != mGzero + mGnonnegative + sum(socG) + sum(rsocG) + (expG + dual_expG) * 3:
+    socG, rsocG, soc_x, rsoc_x = (np.asarray(d, dtype=np.int64).reshape(-1) for d in (socG, rsocG, soc_x, rsoc_x))
+    if m != mGzero + mGnonnegative + int(socG.sum()) + int(rsocG.sum()) + (expG + dual_expG) * 3:
         raise ValueError("m does not match the sum of mGzero, mGnonnegative, socG, rsocG, "
                          "and (expG + dual_expG) * 3")
-    for q in list(socG) + list(soc_x):
-        if q < 2:
-            raise ValueError("The size of the SOC must be greater than 1")
-    for q in list(rsocG) + list(rsoc_x):
-        if q < 3:
-            raise ValueError("The size of the rotated SOC must be greater than 2")
+    if (socG.size and socG.min() < 2) or (soc_x.size and soc_x.min() < 2):
+        raise ValueError("The size of the SOC must be greater than 1")
+    if (rsocG.size and rsocG.min() < 3) or (rsoc_x.size and rsoc_x.min() < 3):
+        raise ValueError("The size of the rotated SOC must be greater than 2")
     P = capi.PdcsProblem()
     P.n, P.m, P.nb, P.nnz = n, m, nb, nnz
     P.G_rowptr, P.G_colind, P.G_val = hold.i32(rowptr), hold.i32(colind), hold.f64(val)
