@@ -560,6 +560,8 @@ def run_ours(args):
                 "batched_fp64": {"time_to_1e-6_ms": 1e3 * t64, "instances_per_s": units / t64,
                                  "optimal": sum(1 for s in s64 if s.info.exit_status == "optimal")},
                 "plain_fp64": plain, "speedup_vs_plain_fp64": value / plain["instances_per_s"] / world,
+                # like for like: both sides include upload, preprocessing and solve
+                "speedup_e2e_vs_plain_fp64": (e2e["value"] / plain["instances_per_s"] / world) if e2e else None,
                 "spmv_schedule": schedule,
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
                 "cpu_baseline": cpu, "single_instance": single, "portfolio": portfolio,

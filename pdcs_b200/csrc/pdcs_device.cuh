@@ -142,8 +142,9 @@ __device__ inline void group_soc_reg_w(double& v, double w, int d, bool weighted
   const double scale = grp_max(act ? fabs(v) : 0.0, g);
   const bool trivial = scale == 0.0 || !isfinite(scale);
   const double sc = trivial ? 1.0 : scale;
-  const double t = grp_bcast(v, g) / sc;
-  const double xi = (act && gl >= 1) ? v / sc : 0.0;
+  const double vs = act ? v / sc : 0.0;  // one division per lane: t is lane 0's
+  const double t = grp_bcast(vs, g);
+  const double xi = gl >= 1 ? vs : 0.0;
   const double D = (act && gl >= 1) ? w : 1.0;
   const double nDx = sqrt(grp_sum((D * xi) * (D * xi), g));
   const double nxD = sqrt(grp_sum((xi / D) * (xi / D), g));
@@ -152,9 +153,12 @@ __device__ inline void group_soc_reg_w(double& v, double w, int d, bool weighted
   const bool rest = !inside && !polar;
   const bool zero_t = rest && weighted && t == 0.0;
   const bool newton = rest && weighted && t != 0.0;
-  // t == 0: closed form (every lane computes it; only zero_t groups use it)
-  const double y0 = xi / (1.0 + D * D);
-  const double s_zero = sqrt(grp_sum((D * y0) * (D * y0), g));
+  // t == 0: closed form (computed by every lane of a warp in which some group needs it)
+  double s_zero = 0.0;
+  if (__any_sync(kFull, zero_t)) {
+    const double y0 = xi / (1.0 + D * D);
+    s_zero = sqrt(grp_sum((D * y0) * (D * y0), g));
+  }
   const double c = D * D * xi * xi;
   const double a = 1.0 + D * D;
   const double s_lo = fmax(t, 0.0);
@@ -168,14 +172,14 @@ __device__ inline void group_soc_reg_w(double& v, double w, int d, bool weighted
     if (!__any_sync(kFull, !done)) break;
     double S1 = 0.0, S2 = 0.0;
     if (!done && c != 0.0) {
-      const double iu = 1.0 / (s * a - t * D * D);
+      const double iu = __drcp_rn(s * a - t * D * D);  // = 1.0 / x, correctly rounded
       S1 = c * iu * iu;
       S2 = c * a * iu * iu * iu;
     }
     S1 = grp_sum(S1, g);
     S2 = grp_sum(S2, g);
     if (done) continue;
-    const double Q = 1.0 / sqrt(S1);
+    const double Q = __drcp_rn(sqrt(S1));
     const double dQ = Q * Q * Q * S2;
     const double step = (1.0 - Q) / dQ;
     if (first) {

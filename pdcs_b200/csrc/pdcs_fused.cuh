@@ -381,14 +381,17 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
           if (rsoc) w = (gl >= 2) ? sqrt(ss[rc.w] * ss[rc.w + 1]) / ss[li] : 1.0;
           else w = (gl >= 1) ? ss[rc.w] / ss[li] : 1.0;
         }
-        const bool weighted = grp_max(w != 1.0 ? 1.0 : 0.0, g) != 0.0;
-        {  // RSOC: rotate the first two elements to the SOC form (every lane shuffles)
+        // the group is weighted when any of its lanes has w != 1 (a vote instead of a reduction)
+        const unsigned gmask = g == 32 ? kFull : ((1u << g) - 1u) << (lane & ~(g - 1));
+        const bool weighted = (__ballot_sync(kFull, w != 1.0) & gmask) != 0u;
+        const bool any_rsoc = __any_sync(kFull, rsoc);
+        if (any_rsoc) {  // RSOC: rotate the first two elements to the SOC form (every lane shuffles)
           const double p0 = __shfl_sync(kFull, v, 0, g), q0 = __shfl_sync(kFull, v, 1, g);
           if (rsoc && gl == 0) v = (p0 + q0) * r2;
           if (rsoc && gl == 1) v = (p0 - q0) * r2;
         }
         group_soc_reg_w(v, w, d, weighted, g, wsv, wsp);
-        {
+        if (any_rsoc) {
           const double a0 = __shfl_sync(kFull, v, 0, g), b0 = __shfl_sync(kFull, v, 1, g);
           if (rsoc && gl == 0) v = (a0 + b0) * r2;
           if (rsoc && gl == 1) v = (a0 - b0) * r2;
