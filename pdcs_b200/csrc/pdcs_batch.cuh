@@ -1183,8 +1183,8 @@ void BatchSolver::setup_fused() {
             recs[cone_cls_[cs][at[a].id]].push_back(
                 make_int4((int32_t)at[a].j, at[a].flags, at[a].id, (int32_t)(at[a].ord - T.o0)));
         T.t0 = (int32_t)P.task.size();
-        for (int cls = 0; cls < kCls - 1; ++cls) {
-          const int g = 2 << cls, per = 32 / g;
+        for (int cls = 0; cls < kCls - 1; ++cls) {  // blocks of <= 2 << cls elements
+          const int g = std::max(1, (2 << cls) / kFusedEPL), per = 32 / g;
           for (size_t r = 0; r < recs[cls].size(); r += per) {
             const int cnt = (int)std::min<size_t>(per, recs[cls].size() - r);
             P.task.push_back(make_int4((int32_t)P.crec.size(), cnt, g, 0));
@@ -1293,7 +1293,9 @@ void BatchSolver::setup_fused() {
           for (int32_t q = T.t0; q < T.t1; ++q)
             for (int r = 0; r < task[q].y; ++r) {
               const int4 cr = crec[task[q].x + r];
-              if (cr.w < T.ew || cr.w + (cr.y & 0x3fffffff) > nr || (cr.y & 0x3fffffff) > task[q].z) bad("cone records");
+              if (cr.w < T.ew || cr.w + (cr.y & 0x3fffffff) > nr || (cr.y & 0x3fffffff) > task[q].z * kFusedEPL ||
+                  (cr.y & 0x3fffffff) < (((cr.y >> 30) & 1) ? 3 : 2))
+                bad("cone records");
             }
           for (int32_t q = T.x0; q < T.x1; ++q)
             if (xrec[q].z < T.ew || xrec[q].z + 3 > nr) bad("exp records");

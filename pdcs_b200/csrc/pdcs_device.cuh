@@ -107,19 +107,21 @@ __device__ inline void warp_soc_reg(double& v, double w, int d, bool weighted) {
 }
 
 // ---------------------------------------------------------------------------
-// Lane groups: g lanes (g = 2..32, a power of two) per block, 32 / g blocks per
+// Lane groups: g lanes (g = 1..32, a power of two) per block, 32 / g blocks per
 // warp.  Reductions are xor butterflies within the group followed by a
 // broadcast from the group's lane 0 (identical values in every lane).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double grp_sum(double v, int g) {
+  if (g == 1) return v;
   for (int o = g >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o, g);
   return __shfl_sync(kFull, v, 0, g);
 }
 __device__ __forceinline__ double grp_max(double v, int g) {
+  if (g == 1) return v;
   for (int o = g >> 1; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o, g));
   return __shfl_sync(kFull, v, 0, g);
 }
-__device__ __forceinline__ double grp_bcast(double v, int g) { return __shfl_sync(kFull, v, 0, g); }
+__device__ __forceinline__ double grp_bcast(double v, int g) { return g == 1 ? v : __shfl_sync(kFull, v, 0, g); }
 
 // warp_soc_reg for a lane group (block of d <= g elements, element i in group
 // lane i).  Every lane runs the same shuffles: groups whose block is inside,
@@ -219,6 +221,129 @@ __device__ inline void group_soc_reg_w(double& v, double w, int d, bool weighted
     if (newton && ws) *ws = s * sc;
   } else if (act) {
     v = v / (1.0 + mu * D * D);
+  }
+}
+
+// The same projection with E elements per lane: block element e lives in group
+// lane e % g, slot e / g (g = 1: a whole block of up to E elements in one lane, no
+// shuffles).  Every scalar of group_soc_reg_w is formed the same way from per-lane
+// sums over the slots followed by the group's butterflies, so a warp projects 32 / g
+// blocks at once with fewer lanes idle and fewer shuffles per block.  w holds the
+// slots' weights on entry (1 for element 0 and empty slots).
+template <int E>
+__device__ inline void group_soc_multi(double (&v)[E], double (&w)[E], int d, bool weighted, int g, double ws_in,
+                                       double* ws) {
+  const int gl = threadIdx.x & (g - 1);
+  double amax = 0.0;
+#pragma unroll
+  for (int q = 0; q < E; ++q)
+    if (gl + g * q < d) amax = fmax(amax, fabs(v[q]));
+  const double scale = grp_max(amax, g);
+  const bool trivial = scale == 0.0 || !isfinite(scale);
+  const double sc = trivial ? 1.0 : scale;
+  double xi[E];
+  double t0 = 0.0, sdx = 0.0, sxd = 0.0;
+#pragma unroll
+  for (int q = 0; q < E; ++q) {
+    const bool act = gl + g * q < d, head = q == 0 && gl == 0;
+    const double vs = act ? v[q] / sc : 0.0;
+    if (q == 0) t0 = vs;
+    xi[q] = head ? 0.0 : vs;
+    if (!act || head) w[q] = 1.0;  // w is D from here on
+    sdx += (w[q] * xi[q]) * (w[q] * xi[q]);
+    sxd += (xi[q] / w[q]) * (xi[q] / w[q]);
+  }
+  const double t = grp_bcast(t0, g);
+  const double nDx = sqrt(grp_sum(sdx, g));
+  const double nxD = sqrt(grp_sum(sxd, g));
+  const bool inside = trivial || nDx <= t;
+  const bool polar = !inside && nxD <= -t;
+  const bool rest = !inside && !polar;
+  const bool zero_t = rest && weighted && t == 0.0;
+  const bool newton = rest && weighted && t != 0.0;
+  double s_zero = 0.0;  // t == 0: closed form
+  if (__any_sync(kFull, zero_t)) {
+    double acc = 0.0;
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      const double y0 = xi[q] / (1.0 + w[q] * w[q]);
+      acc += (w[q] * y0) * (w[q] * y0);
+    }
+    s_zero = sqrt(grp_sum(acc, g));
+  }
+  const double s_lo = fmax(t, 0.0);
+  double s = s_lo;
+  double sw = (newton && gl == 0) ? ws_in : __longlong_as_double(0x7ff8000000000000ll);
+  sw = grp_bcast(sw, g) / sc;
+  bool first = newton && isfinite(sw) && sw > s_lo;
+  if (first) s = sw;
+  bool done = !newton;
+  for (int it = 0; it < 200; ++it) {
+    if (!__any_sync(kFull, !done)) break;
+    double S1 = 0.0, S2 = 0.0;
+    if (!done) {
+#pragma unroll
+      for (int q = 0; q < E; ++q) {
+        const double c = w[q] * w[q] * xi[q] * xi[q];
+        if (c != 0.0) {
+          const double a = 1.0 + w[q] * w[q];
+          const double iu = __drcp_rn(s * a - t * w[q] * w[q]);
+          S1 += c * iu * iu;
+          S2 += c * a * iu * iu * iu;
+        }
+      }
+    }
+    S1 = grp_sum(S1, g);
+    S2 = grp_sum(S2, g);
+    if (done) continue;
+    const double Q = __drcp_rn(sqrt(S1));
+    const double dQ = Q * Q * Q * S2;
+    const double step = (1.0 - Q) / dQ;
+    if (first) {
+      first = false;
+      if (step < 0.0) {  // warm start above the root
+        s = fmax(s + step, s_lo);
+        continue;
+      }
+    }
+    if (!(step > 0.0)) {
+      done = true;
+      continue;
+    }
+    const double sn = s + step;
+    if (!(sn > s)) {
+      done = true;
+      continue;
+    }
+    s = sn;
+    if (step <= 1e-17 * s) done = true;
+  }
+  if (inside) return;
+  if (polar) {
+#pragma unroll
+    for (int q = 0; q < E; ++q)
+      if (gl + g * q < d) v[q] = 0.0;
+    return;
+  }
+  if (!weighted) {
+    const double cc = 0.5 * (1.0 + t / nDx);
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+      if (q == 0 && gl == 0) v[q] = cc * nDx * sc;
+      else if (gl + g * q < d) v[q] *= cc;
+    }
+    return;
+  }
+  const double sf = zero_t ? s_zero : s;
+  const double mu = zero_t ? 1.0 : 1.0 - t / s;
+#pragma unroll
+  for (int q = 0; q < E; ++q) {
+    if (q == 0 && gl == 0) {
+      v[q] = sf * sc;
+      if (newton && ws) *ws = s * sc;
+    } else if (gl + g * q < d) {
+      v[q] = v[q] / (1.0 + mu * w[q] * w[q]);
+    }
   }
 }
 

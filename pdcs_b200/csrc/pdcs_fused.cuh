@@ -31,6 +31,9 @@ constexpr int kFusedWarps = kFusedThreads / 32;
 // SOC / RSOC tables, 2 (128) when the exponential-cone root solve is compiled in
 constexpr int kFusedMinCtas = 4, kFusedMinCtasExp = 2;
 constexpr int kSellC = 32;  // rows per slice
+// elements per lane of the lane-group cone projections: a block of d elements takes
+// g = d / kFusedEPL lanes (rounded up to a power of two), 32 / g blocks per warp
+constexpr int kFusedEPL = 2;
 // rows a thread updates at once in the step, their loads in flight together (2 spills
 // registers under the 64-register budget and measured slower)
 constexpr int kFusedRows = 1;
@@ -357,8 +360,9 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
       }
     }
     __syncthreads();
-    // (b) SOC / RSOC blocks in lane groups, on the values in shared memory; the next
-    // task's descriptor and record are in flight while a task is projected
+    // (b) SOC / RSOC blocks in lane groups of g lanes with kFusedEPL elements per lane,
+    // on the values in shared memory; the next task's descriptor is in flight while a
+    // task is projected
     {
       int64_t t = tl.t0 + warp;
       int4 tkn = make_int4(0, 0, 2, 0);
@@ -372,31 +376,45 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
         if (t + kFusedWarps < tl.t1) tkn = A.task[t + kFusedWarps];
         const int d = have ? (rc.y & 0x3fffffff) : 0;
         const bool rsoc = have && (rc.y >> 30) != 0;
-        const int li = rc.w + gl;
+        const int l0 = rc.w;
         double* wsp = (have && CT.soc_ws) ? CT.soc_ws + rc.z : nullptr;
         const double wsv = (wsp && gl == 0) ? *wsp : __longlong_as_double(0x7ff8000000000000ll);
-        double v = gl < d ? zs[li] : 0.0;
-        double w = 1.0;
-        if (CT.S && gl < d) {
-          if (rsoc) w = (gl >= 2) ? sqrt(ss[rc.w] * ss[rc.w + 1]) / ss[li] : 1.0;
-          else w = (gl >= 1) ? ss[rc.w] / ss[li] : 1.0;
+        // weights: S_0 / S_e (SOC), sqrt(S_0 S_1) / S_e for e >= 2 (RSOC); ss holds 1 when unscaled
+        const double num = d > 0 ? (rsoc ? sqrt(ss[l0] * ss[l0 + 1]) : ss[l0]) : 1.0;
+        double v[kFusedEPL], w[kFusedEPL];
+        bool wne = false;
+#pragma unroll
+        for (int q = 0; q < kFusedEPL; ++q) {
+          const int e = gl + g * q;
+          v[q] = e < d ? zs[l0 + e] : 0.0;
+          w[q] = (e < d && e >= (rsoc ? 2 : 1)) ? num / ss[l0 + e] : 1.0;
+          wne |= w[q] != 1.0;
         }
-        // the group is weighted when any of its lanes has w != 1 (a vote instead of a reduction)
+        // the group is weighted when any of its elements has a weight != 1 (a vote)
         const unsigned gmask = g == 32 ? kFull : ((1u << g) - 1u) << (lane & ~(g - 1));
-        const bool weighted = (__ballot_sync(kFull, w != 1.0) & gmask) != 0u;
+        const bool weighted = (__ballot_sync(kFull, wne) & gmask) != 0u;
         const bool any_rsoc = __any_sync(kFull, rsoc);
-        if (any_rsoc) {  // RSOC: rotate the first two elements to the SOC form (every lane shuffles)
-          const double p0 = __shfl_sync(kFull, v, 0, g), q0 = __shfl_sync(kFull, v, 1, g);
-          if (rsoc && gl == 0) v = (p0 + q0) * r2;
-          if (rsoc && gl == 1) v = (p0 - q0) * r2;
+        auto rotate = [&]() {  // RSOC: the first two elements <-> the SOC form (an involution)
+          if (g == 1) {
+            const double p0 = v[0], q0 = v[1];
+            if (rsoc) {
+              v[0] = (p0 + q0) * r2;
+              v[1] = (p0 - q0) * r2;
+            }
+          } else {
+            const double p0 = __shfl_sync(kFull, v[0], 0, g), q0 = __shfl_sync(kFull, v[0], 1, g);
+            if (rsoc && gl == 0) v[0] = (p0 + q0) * r2;
+            if (rsoc && gl == 1) v[0] = (p0 - q0) * r2;
+          }
+        };
+        if (any_rsoc) rotate();
+        group_soc_multi<kFusedEPL>(v, w, d, weighted, g, wsv, wsp);
+        if (any_rsoc) rotate();
+#pragma unroll
+        for (int q = 0; q < kFusedEPL; ++q) {
+          const int e = gl + g * q;
+          if (e < d) zs[l0 + e] = v[q];
         }
-        group_soc_reg_w(v, w, d, weighted, g, wsv, wsp);
-        if (any_rsoc) {
-          const double a0 = __shfl_sync(kFull, v, 0, g), b0 = __shfl_sync(kFull, v, 1, g);
-          if (rsoc && gl == 0) v = (a0 + b0) * r2;
-          if (rsoc && gl == 1) v = (a0 - b0) * r2;
-        }
-        if (gl < d) zs[li] = v;
       }
     }
     if constexpr (EXP) {
