@@ -1327,6 +1327,8 @@ void BatchSolver::setup_fused() {
     F.cloc = tl_[w].T.cloc;
     F.max_cols = tl_[w].T.max_cols;
     F.max_rows = max_rows;
+    F.sched = A.alloc<int32_t>(2);
+    PDCS_CUDA(cudaMemsetAsync(F.sched, 0, 2 * sizeof(int32_t), s_));
     fu.first_dev = up(fu.first);
     fu.tpart = A.alloc<double>(std::max<size_t>(tiles.size(), 1) * (w == 0 ? 2 : 1));
     int32_t* d_srow = up(srow);

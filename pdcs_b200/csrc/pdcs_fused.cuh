@@ -65,6 +65,7 @@ struct FusedCsr {
   const int32_t* cloc;    // K * kMaxRuns: instance-local first column of each column run
   int32_t max_cols;       // staged elements (largest instance's column count)
   int32_t max_rows;       // largest tile's rows (products in shared memory)
+  int32_t* sched;         // [0] next tile to hand out, [1] CTAs finished; both 0 between launches
 };
 
 // ---- fused ops.  In is what the update reads of row j (load), z(q, a, b)
@@ -243,11 +244,23 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
   const int64_t nt = A.act ? *A.n_act : A.ntiles;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const double r2 = 0.7071067811865476;
-  for (int64_t q = blockIdx.x; q < nt; q += gridDim.x) {
+  // Tiles are handed out one at a time from a counter, largest first (the order of
+  // the active list), so a CTA that drew short tiles takes more of them.
+  __shared__ int32_t s_next;
+  if (threadIdx.x == 0) s_next = atomicAdd(&A.sched[0], 1);
+  __syncthreads();
+  for (;;) {
+    const int64_t q = s_next;
+    if (q >= nt) break;
     const int64_t tid = A.act ? (int64_t)A.act[q] : q;
     const FusedTile tl = A.tiles[tid];
     const int64_t k = tl.inst;
-    if (!op.mask[k]) continue;  // CTA-uniform: the instance does not iterate
+    if (!op.mask[k]) {  // CTA-uniform: the instance does not iterate
+      __syncthreads();  // every thread has read s_next
+      if (threadIdx.x == 0) s_next = atomicAdd(&A.sched[0], 1);
+      __syncthreads();
+      continue;
+    }
     if (threadIdx.x < kMaxRuns) {
       run_row[threadIdx.x] = A.rows.start[k * kMaxRuns + threadIdx.x];
       run_ord[threadIdx.x] = A.rloc[k * kMaxRuns + threadIdx.x];
@@ -472,7 +485,18 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
       for (int w = 1; w < kFusedWarps; ++w) v += red[threadIdx.x][w];
       tpart[tid * Op::NACC + threadIdx.x] = v;
     }
+    if (threadIdx.x == 0) s_next = atomicAdd(&A.sched[0], 1);
     __syncthreads();  // the next tile restages sx, the products and the run tables
+  }
+  // the last CTA to finish resets the counters for the next launch (every other CTA
+  // is past its last read of them)
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&A.sched[1], 1) == (int32_t)gridDim.x - 1) {
+      A.sched[0] = 0;
+      A.sched[1] = 0;
+      __threadfence();
+    }
   }
 }
 
