@@ -1491,7 +1491,7 @@ void BatchSolver::build_act_lists(const std::vector<Inst*>& its) {
       meta[kCls + 2 + c] = off;
       std::memcpy(sched + off, bycls[c].data(), bycls[c].size() * sizeof(int64_t));
       for (size_t q = 0; q < bycls[c].size(); ++q) desc[off + q] = cone_desc_[w][bycls[c][q]];
-      const int64_t per = (c < kCls - 1) ? 32 / (2 << c) : 1;
+      const int64_t per = (c < kCls - 1) ? 32 / cls_lanes(c) : 1;
       task += ((int64_t)bycls[c].size() + per - 1) / per;
       off += (int64_t)bycls[c].size();
     }

@@ -137,6 +137,50 @@ __device__ void bs_wcone(const Op& op, const ConeTable& T, int64_t k, int lane, 
 
 // Project the instance's elements of one side (runs r0 .. r1 - 1 elementwise,
 // its warp cones and exp cones) with op; CTA-collective, ends with a barrier.
+// Two blocks of at most 32 elements per warp: block ka in lanes 0-15, kb (-1: none) in
+// lanes 16-31, two elements per lane (group_soc_multi; the weights and the RSOC
+// rotation as in bs_wcone).
+template <class Op>
+__device__ void bs_wcone_pair(const Op& op, const ConeTable& T, int64_t ka, int64_t kb, int lane, double* acc) {
+  constexpr int g = 16;
+  const double r2 = 0.7071067811865476;
+  const int gl = lane & (g - 1);
+  const int64_t k = lane < g ? ka : kb;
+  const bool have = k >= 0;
+  const int64_t st = have ? T.wc_start[k] : 0;
+  const int d = have ? T.wc_len[k] : 0;
+  const bool rsoc = have && T.wc_kind[k] == PK_RSOC;
+  const double* S = (T.S && have) ? T.S + st : nullptr;
+  const double num = S ? (rsoc ? sqrt(S[0] * S[1]) : S[0]) : 1.0;
+  double* wsp = (have && T.soc_ws) ? T.soc_ws + k : nullptr;
+  const double wsv = (wsp && gl == 0) ? *wsp : __longlong_as_double(0x7ff8000000000000ll);
+  double z[2], v[2], w[2];
+  bool wne = false;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int e = gl + g * q;
+    z[q] = e < d ? op.z(st + e) : 0.0;
+    v[q] = z[q];
+    w[q] = (S && e < d && e >= (rsoc ? 2 : 1)) ? num / S[e] : 1.0;
+    wne |= w[q] != 1.0;
+  }
+  const unsigned gmask = 0xffffu << (lane & g);
+  const bool weighted = (__ballot_sync(kFull, wne) & gmask) != 0u;
+  auto rotate = [&]() {  // RSOC: the first two elements <-> the SOC form (an involution)
+    const double p0 = __shfl_sync(kFull, v[0], 0, g), q0 = __shfl_sync(kFull, v[0], 1, g);
+    if (rsoc && gl == 0) v[0] = (p0 + q0) * r2;
+    if (rsoc && gl == 1) v[0] = (p0 - q0) * r2;
+  };
+  rotate();
+  group_soc_multi<2>(v, w, d, weighted, g, wsv, wsp);
+  rotate();
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int e = gl + g * q;
+    if (e < d) op.fin(st + e, z[q], v[q], acc);
+  }
+}
+
 template <class Op>
 __device__ void bs_project(const Op& op, const ConeTable& T, const RunTable& R, int r0, int r1, const int64_t* cr,
                            int64_t k, double* acc) {
@@ -151,8 +195,18 @@ __device__ void bs_project(const Op& op, const ConeTable& T, const RunTable& R, 
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int part = 0; part < 2; ++part)
-    for (int64_t w = cr[2 * part] + warp; w < cr[2 * part + 1]; w += kWarps) bs_wcone(op, T, w, lane, acc);
+  for (int part = 0; part < 2; ++part) {  // two blocks per warp when both have at most 32 elements
+    const int64_t c1 = cr[2 * part + 1];
+    for (int64_t w = cr[2 * part] + 2 * warp; w < c1; w += 2 * kWarps) {
+      const bool hb = w + 1 < c1;
+      if (T.wc_len[w] <= 32 && (!hb || T.wc_len[w + 1] <= 32)) {
+        bs_wcone_pair(op, T, w, hb ? w + 1 : -1, lane, acc);
+      } else {
+        bs_wcone(op, T, w, lane, acc);
+        if (hb) bs_wcone(op, T, w + 1, lane, acc);
+      }
+    }
+  }
   for (int part = 0; part < 2; ++part) {
     for (int64_t e = cr[4 + 2 * part] + threadIdx.x; e < cr[5 + 2 * part]; e += kThreads) {
       const bool first = e < T.exp_count;

@@ -373,6 +373,11 @@ inline void launch_spmv(const CsrT<T>& A, const std::type_identity_t<T>* x0, con
 // Block structure of one vector for projections.
 // ---------------------------------------------------------------------------
 constexpr int kCls = 6;
+// Lane groups of the cone schedule: class c < kCls - 1 holds blocks of at most
+// 2 << c elements, projected by cls_lanes(c) lanes with kClsEPL elements per lane
+// (32 / cls_lanes(c) blocks per warp); the last class takes a warp per block.
+constexpr int kClsEPL = 2;
+__host__ __device__ constexpr int cls_lanes(int c) { return (2 << c) / kClsEPL < 1 ? 1 : (2 << c) / kClsEPL; }
 
 struct ConeTable {
   int64_t len;
@@ -392,7 +397,7 @@ struct ConeTable {
   const double* S;           // scaling (NULL: unscaled)
   double* rho_ws;            // per exp/dual-exp cone warm start of the root (NULL: none)
   // warp-cone schedule by size class: class c < kCls - 1 packs blocks of at
-  // most g = 2 << c elements, 32 / g per warp; the last class (> 32) takes a
+  // most 2 << c elements, 32 / cls_lanes(c) per warp; the last class (> 32) takes a
   // warp per block.  sched lists warp-cone indices class by class.
   const int64_t* sched;
   int64_t cls_off[kCls + 1];  // ranges of sched per class
@@ -792,7 +797,7 @@ concept MaskedOp = requires(const Op& o) { o.live(int64_t(0)); };
 // HUGE: compile part D (tables with huge blocks only: its code raises the
 // register count of the whole kernel, 64 -> 80 without EXP).
 template <class Op, bool EXP = true, bool HUGE = false>
-__global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTable T, double* partials,
+__global__ void __launch_bounds__(kThreads, HUGE ? 2 : 1) update_project_kernel(Op op, ConeTable T, double* partials,
                                                                  const int32_t* active) {
   if (active && !*active) return;
   op.load();
@@ -855,8 +860,8 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
       for (int q = 1; q < kCls; ++q)
         if (task >= task0[q]) c = q;
       if (c < kCls - 1) {
-        // 32 / g blocks of at most g elements, one per lane group
-        const int g = 2 << c;
+        // 32 / g blocks of at most 2 g elements, one per lane group, two elements per lane
+        const int g = cls_lanes(c);
         const int gl = lane & (g - 1);
         const int64_t idx = cls_off[c] + (task - task0[c]) * (32 / g) + lane / g;
         bool have = idx < cls_off[c + 1];
@@ -882,26 +887,43 @@ __global__ void __launch_bounds__(kThreads) update_project_kernel(Op op, ConeTab
           rsoc = have && T.wc_kind[k] == PK_RSOC;
         }
         const double* S = (T.S && have) ? T.S + st : nullptr;
-        const double z = (gl < d) ? op.z(st + gl) : 0.0;
-        double v = z;
-        double w = 1.0;
-        if (S && gl < d) {
-          if (rsoc) w = (gl >= 2) ? sqrt(S[0] * S[1]) / S[gl] : 1.0;
-          else w = (gl >= 1) ? S[0] / S[gl] : 1.0;
+        const double num = (S && d > 0) ? (rsoc ? sqrt(S[0] * S[1]) : S[0]) : 1.0;
+        double* wsp = (have && T.soc_ws) ? T.soc_ws + k : nullptr;
+        const double wsv = (wsp && gl == 0) ? *wsp : __longlong_as_double(0x7ff8000000000000ll);
+        double z[kClsEPL], v[kClsEPL], w[kClsEPL];
+        bool wne = false;
+#pragma unroll
+        for (int q = 0; q < kClsEPL; ++q) {
+          const int e = gl + g * q;
+          z[q] = e < d ? op.z(st + e) : 0.0;
+          v[q] = z[q];
+          w[q] = (S && e < d && e >= (rsoc ? 2 : 1)) ? num / S[e] : 1.0;
+          wne |= w[q] != 1.0;
         }
-        const bool weighted = grp_max(w != 1.0 ? 1.0 : 0.0, g) != 0.0;
-        {  // RSOC: rotate the first two elements to the SOC form (all lanes shuffle)
-          const double p0 = __shfl_sync(kFull, v, 0, g), q0 = __shfl_sync(kFull, v, 1, g);
-          if (rsoc && gl == 0) v = (p0 + q0) * r2;
-          if (rsoc && gl == 1) v = (p0 - q0) * r2;
+        // the group is weighted when any of its elements has a weight != 1 (a vote)
+        const unsigned gmask = g == 32 ? kFull : ((1u << g) - 1u) << (lane & ~(g - 1));
+        const bool weighted = (__ballot_sync(kFull, wne) & gmask) != 0u;
+        auto rotate = [&]() {  // RSOC: the first two elements <-> the SOC form (an involution)
+          if (g == 1) {
+            const double p0 = v[0], q0 = v[1];
+            if (rsoc) {
+              v[0] = (p0 + q0) * r2;
+              v[1] = (p0 - q0) * r2;
+            }
+          } else {
+            const double p0 = __shfl_sync(kFull, v[0], 0, g), q0 = __shfl_sync(kFull, v[0], 1, g);
+            if (rsoc && gl == 0) v[0] = (p0 + q0) * r2;
+            if (rsoc && gl == 1) v[0] = (p0 - q0) * r2;
+          }
+        };
+        rotate();
+        group_soc_multi<kClsEPL>(v, w, d, weighted, g, wsv, wsp);
+        rotate();
+#pragma unroll
+        for (int q = 0; q < kClsEPL; ++q) {
+          const int e = gl + g * q;
+          if (e < d) op.fin(st + e, z[q], v[q], acc);
         }
-        group_soc_reg(v, w, d, weighted, g, (have && T.soc_ws) ? T.soc_ws + k : nullptr);
-        {
-          const double a0 = __shfl_sync(kFull, v, 0, g), b0 = __shfl_sync(kFull, v, 1, g);
-          if (rsoc && gl == 0) v = (a0 + b0) * r2;
-          if (rsoc && gl == 1) v = (a0 - b0) * r2;
-        }
-        if (gl < d) op.fin(st + gl, z, v, acc);
       } else {
         // blocks of more than 32 elements: a warp each, values staged in op.out
         int64_t k, st;

@@ -918,7 +918,7 @@ void Solver::size_table(ConeTable& T) {
 void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<int64_t>& rsoc_x,
                           const std::vector<int64_t>& socG, const std::vector<int64_t>& rsocG) {
   // warp-cone lists (shared by the iteration and KKT tables of each vector)
-  // warp-cone lists and their size-class schedule (lane groups of g = 2 << c lanes)
+  // warp-cone lists and their size-class schedule (lane groups of cls_lanes(c) lanes)
   auto upload_wc = [&](const std::vector<int64_t>& soc, const std::vector<int64_t>& rsoc, int64_t start0,
                        ConeTable& T) {
     std::vector<int64_t> stv;
@@ -950,7 +950,7 @@ void Solver::build_tables(const std::vector<int64_t>& soc_x, const std::vector<i
       T.cls_off[c] = (int64_t)sched.size();
       T.task0[c] = task;
       sched.insert(sched.end(), cls[c].begin(), cls[c].end());
-      const int64_t per = (c < kCls - 1) ? 32 / (2 << c) : 1;
+      const int64_t per = (c < kCls - 1) ? 32 / cls_lanes(c) : 1;
       task += ((int64_t)cls[c].size() + per - 1) / per;
     }
     T.cls_off[kCls] = (int64_t)sched.size();
