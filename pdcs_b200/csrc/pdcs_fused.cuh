@@ -454,6 +454,9 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
       }
     }
     __syncthreads();
+    // the next tile, published by the barrier of the partial sums below (every thread
+    // read this tile's index at the top of the loop, several barriers ago)
+    if (threadIdx.x == 0) s_next = atomicAdd(&A.sched[0], 1);
     // (c) the cone rows' results, stored in row order with the control step's terms
     for (int i0 = tl.ew + threadIdx.x; i0 < nr; i0 += kFusedRows * kFusedThreads) {
       int64_t jj[kFusedRows];
@@ -485,8 +488,9 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
       for (int w = 1; w < kFusedWarps; ++w) v += red[threadIdx.x][w];
       tpart[tid * Op::NACC + threadIdx.x] = v;
     }
-    if (threadIdx.x == 0) s_next = atomicAdd(&A.sched[0], 1);
-    __syncthreads();  // the next tile restages sx, the products and the run tables
+    // no barrier here: the next tile's first writes to shared memory (run tables, staged
+    // segment) touch nothing read after the barrier above, and red is rewritten only
+    // after the next tile's own barriers
   }
   // the last CTA to finish resets the counters for the next launch (every other CTA
   // is past its last read of them)
