@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
   const double r2 = 0.7071067811865476;
   // Tiles are handed out one at a time from a counter, largest first (the order of
   // the active list), so a CTA that drew short tiles takes more of them.
-  __shared__ int32_t s_next;
+  __shared__ int32_t s_next, s_slice, s_task;
   if (threadIdx.x == 0) s_next = atomicAdd(&A.sched[0], 1);
   __syncthreads();
   for (;;) {
@@ -264,6 +264,10 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
     if (threadIdx.x < kMaxRuns) {
       run_row[threadIdx.x] = A.rows.start[k * kMaxRuns + threadIdx.x];
       run_ord[threadIdx.x] = A.rloc[k * kMaxRuns + threadIdx.x];
+    }
+    if (threadIdx.x == 0) {  // the tile's slices and cone tasks are taken by the warps one at a time
+      s_slice = 0;
+      s_task = 0;
     }
     // the instance's column segment, copied to shared memory asynchronously (every copy
     // in flight at once, no registers held)
@@ -283,7 +287,12 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
     cp_async_wait_all();
     __syncthreads();
     // ---- the tile's rows, SELL-32: lane = row, one coalesced load per column ----
-    for (int64_t s = tl.s0 + warp; s < tl.s1; s += kFusedWarps) {
+    for (;;) {
+      int32_t si = 0;
+      if (lane == 0) si = atomicAdd(&s_slice, 1);
+      si = __shfl_sync(kFull, si, 0);
+      if (si >= tl.s1 - tl.s0) break;
+      const int64_t s = tl.s0 + si;
       const int64_t base = A.sb[s] + lane;
       const int32_t len = A.sl[s];
       const int32_t slot = A.so[s * kSellC + lane];
@@ -374,19 +383,27 @@ __global__ void __launch_bounds__(kFusedThreads, EXP ? kFusedMinCtasExp : kFused
     }
     __syncthreads();
     // (b) SOC / RSOC blocks in lane groups of g lanes with kFusedEPL elements per lane,
-    // on the values in shared memory; the next task's descriptor is in flight while a
-    // task is projected
+    // on the values in shared memory; a warp takes the next task when it finishes one
+    // (tasks cost different numbers of Newton steps), its descriptor in flight while the
+    // current task is projected
     {
-      int64_t t = tl.t0 + warp;
+      const int32_t ntask = tl.t1 - tl.t0;
+      int32_t t = 0;
+      if (lane == 0) t = atomicAdd(&s_task, 1);
+      t = __shfl_sync(kFull, t, 0);
       int4 tkn = make_int4(0, 0, 2, 0);
-      if (t < tl.t1) tkn = A.task[t];
-      for (; t < tl.t1; t += kFusedWarps) {
+      if (t < ntask) tkn = A.task[tl.t0 + t];
+      while (t < ntask) {
         const int4 tk = tkn;
         const int g = tk.z, gl = lane & (g - 1);
         const bool have = lane / g < tk.y;
         int4 rc = make_int4(0, 0, 0, 0);
         if (have) rc = A.crec[tk.x + lane / g];
-        if (t + kFusedWarps < tl.t1) tkn = A.task[t + kFusedWarps];
+        int32_t tn = 0;  // the warp's next task, its descriptor in flight during this one
+        if (lane == 0) tn = atomicAdd(&s_task, 1);
+        tn = __shfl_sync(kFull, tn, 0);
+        if (tn < ntask) tkn = A.task[tl.t0 + tn];
+        t = tn;
         const int d = have ? (rc.y & 0x3fffffff) : 0;
         const bool rsoc = have && (rc.y >> 30) != 0;
         const int l0 = rc.w;
