@@ -179,14 +179,51 @@ __global__ void __launch_bounds__(kThreads) batch_reflect32_kernel(const int32_t
   const int64_t nch = *n_rchunk;
   const int lane = threadIdx.x & 31;
   const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  constexpr int R = 4;  // elements per lane with their loads in flight together
   for (int64_t q = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nch; q += wstride) {
     const int4 ch = rchunk[q];  // {first element, length, 0 = x / 1 = y, instance}
-    const PdhgState& s = sts[ch.w];
-    if (!s.do_reflect) continue;
-    for (int i = lane; i < ch.y; i += 32) {
-      const int64_t j = (int64_t)ch.x + i;
-      if (ch.z == 0) reflect32_x(s, dxp, dxm, j);
-      else reflect32_y(s, dy, dyl, dym, j);
+    const PdhgState& st = sts[ch.w];
+    if (!st.do_reflect) continue;
+    PdhgState s;  // the reflection's scalars only
+    s.refl_tmp = st.refl_tmp;
+    s.refl_inv = st.refl_inv;
+    s.refl_extra = st.refl_extra;
+    s.refl_eta = st.refl_eta;
+    s.refl_cum = st.refl_cum;
+    for (int i0 = lane; i0 < ch.y; i0 += 32 * R) {
+      float d[R], dl[R];
+      double dm[R];
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int i = i0 + 32 * u;
+        if (i >= ch.y) continue;
+        const int64_t j = (int64_t)ch.x + i;
+        if (ch.z == 0) {
+          const float2 p = dxp[j];
+          d[u] = p.x;
+          dl[u] = p.y;
+          dm[u] = dxm[j];
+        } else {
+          d[u] = dy[j];
+          dl[u] = dyl[j];
+          dm[u] = dym[j];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int i = i0 + 32 * u;
+        if (i >= ch.y) continue;
+        const int64_t j = (int64_t)ch.x + i;
+        const float nv = reflect32_value(s, d[u], dl[u], dm[u]);
+        if (ch.z == 0) {
+          dxp[j] = make_float2(nv, nv);
+          dxm[j] = dm[u];
+        } else {
+          dy[j] = nv;
+          dyl[j] = nv;
+          dym[j] = dm[u];
+        }
+      }
     }
   }
 }
