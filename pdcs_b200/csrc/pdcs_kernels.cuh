@@ -739,13 +739,13 @@ __device__ void huge_block_proj(const Op& op, const ConeTable& T, int h, int cta
             const double c = e[k].x, D = e[k].y;
             if (c == 0.0) continue;
             const double a = 1.0 + D * D;
-            const double iu = 1.0 / (s * a - t * D * D);
+            const double iu = __drcp_rn(s * a - t * D * D);  // = 1.0 / x, correctly rounded
             q[0] += c * iu * iu;
             q[1] += c * a * iu * iu * iu;
           }
         }
         if (!huge_allreduce<2>(T, cta, round, q, ksum2)) return;
-        const double Q = 1.0 / sqrt(q[0]);
+        const double Q = __drcp_rn(sqrt(q[0]));
         const double dQ = Q * Q * Q * q[1];
         const double step = (1.0 - Q) / dQ;
         if (first) {
